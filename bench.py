@@ -1,0 +1,321 @@
+#!/usr/bin/env python
+"""Throughput of the fused Model C step on B200 (Gcell-updates/s).
+
+Workload (default): Karma-Rappel Model C on 4096^2 cells as 16x16 blocks of
+256^2, ghost 1, h = 0.4, dt = 0.008, D = 2, lambda = D/0.6267, eps4 = 0.05,
+u0 = -0.55, 16 seeded grains of radius 8, zero-flux boundaries, Gaussian
+noise b = 0.01, Euler-Maruyama, FP64.  A step is one time step over the whole
+grid (16.8M cell-updates).  The state (2 fields x 2 buffers, 0.54 GB) is
+larger than L2, so no flush is needed between steps.
+
+Arms:
+  default          this library on N GPUs (N independent replicas, one per
+                   rank, weak scaling; the path has no cross-replica exchange)
+  --impl reference the reference's CPU path (the oracle restatement, all host
+                   threads) on rank 0, same config and metric.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+CONFIGS = {
+    # Model C 2D, 4096^2 as 16x16 blocks of 256^2
+    "c2": dict(workload="model_c_4096sq", cells=4096, block=256, h=0.4, dt=0.008, d_thermal=2.0,
+               lam=2.0 / 0.6267, eps4=0.05, u0=0.55, grains=16, radius=8.0, noise=0.01, seed=42,
+               full_steps=20000),
+    # Model C 2D at full scale, 10080^2 as 80x80 blocks of 126^2
+    "c3": dict(workload="model_c_10080sq", cells=10080, block=126, h=0.4, dt=0.008, d_thermal=2.0,
+               lam=2.0 / 0.6267, eps4=0.05, u0=0.5, grains=64, radius=8.0, noise=0.01, seed=42,
+               full_steps=10000),
+}
+
+BYTES_PER_CELL = {"f64": 32, "f32": 16}  # read phi, u; write phi, u
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi sampled every 200 ms while the timed region runs."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "200", "-f", self.path], stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"], "samples": 0}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        for line in Path(self.path).read_text().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({n for r in rows for n, v in zip(names, r[5:9]) if v.lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def dist_setup(n_gpus: int):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    import torch
+
+    torch.cuda.set_device(local)
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        pg = dist
+    return rank, world, local, pg
+
+
+def barrier(pg):
+    if pg is not None:
+        pg.barrier()
+
+
+def max_over_ranks(pg, value: float) -> float:
+    if pg is None:
+        return value
+    import torch
+
+    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def make_sim(cfg, dtype, sched, seed_offset=0):
+    import legendre_b200 as L
+
+    n, b, h = cfg["cells"], cfg["block"], cfg["h"]
+    grid = L.CartesianGrid([n, n], [b, b], [0.0, 0.0], [h, h])
+    model = L.ModelC(cfg["eps4"], cfg["lam"], cfg["noise"])
+    model.d_thermal = cfg["d_thermal"]
+    sim = L.Simulation(grid, L.FiniteVolume(), model, L.EulerMaruyama(cfg["seed"] + seed_offset), sched,
+                       L.CudaAllocator(dtype))
+    grains = L.seed_positions(n, h, cfg["grains"], cfg["seed"], radius=cfg["radius"])
+    return sim, grid, model, grains
+
+
+def initialize(sim, grid, model, grains, cfg, dtype, sched):
+    import numpy as np
+
+    import legendre_b200 as L
+
+    if dtype == "f64":
+        model.initialize_grains(grid, sim.state, grains, cfg["u0"])
+        return
+    tmp = L.DeviceState(grid, sched, L.CudaAllocator("f64"), sim.state.specs)
+    model.initialize_grains(grid, tmp, grains, cfg["u0"])
+    for f in ("phi", "u"):
+        sim.state.upload(f, tmp.download(f).astype(np.float32))
+    tmp._destroy()
+
+
+def cpu_oracle_rate(cfg, steps_budget_s: float, max_steps: int):
+    """Oracle (C++ restatement of the reference's CPU path), all host threads,
+    on the full grid; returns (Gcell/s, steps run, threads)."""
+    sys.path.insert(0, str(ROOT / "tests"))
+    import oracle_bind as orc
+
+    from legendre_b200 import seed_positions
+
+    n, b, h = cfg["cells"], cfg["block"], cfg["h"]
+    og = orc.Grid([n, n], [b, b], [0.0, 0.0], [h, h])
+    st = orc.State(og, [1, 1])
+    grains = seed_positions(n, h, cfg["grains"], cfg["seed"], radius=cfg["radius"])
+    st.initialize_grains([(g.center[0], g.center[1], g.radius) for g in grains], cfg["u0"])
+    p = orc.modelc_params(eps4=cfg["eps4"], lam=cfg["lam"], d_thermal=cfg["d_thermal"], noise=cfg["noise"])
+    threads = int(orc.lib.orc_num_threads_available())
+    t0 = time.perf_counter()
+    t = st.modelc_run(p, 0.0, cfg["dt"], cfg["seed"], 1, True, threads)
+    one = time.perf_counter() - t0
+    steps = max(1, min(max_steps, int(steps_budget_s / max(one, 1e-6))))
+    t0 = time.perf_counter()
+    st.modelc_run(p, t, cfg["dt"], cfg["seed"], steps, True, threads)
+    el = time.perf_counter() - t0
+    return n * n * steps / el / 1e9, steps, threads
+
+
+def run_reference(args, cfg):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    rate, steps, threads = cpu_oracle_rate(cfg, steps_budget_s=60.0, max_steps=args.steps)
+    line = {
+        "metric": "Gcell-updates/s", "value": rate, "unit": "Gcell-updates/s", "impl": "reference",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+        "dtype": "f64", "data": "synthetic",
+        "config": {"workload": cfg["workload"], "cells": cfg["cells"], "block": cfg["block"], "noise": cfg["noise"]},
+        "cpu_baseline": {"value": rate, "unit": "Gcell-updates/s", "cores": threads, "kind": "port",
+                         "sample": f"{steps} of {args.steps} steps on the full {cfg['cells']}^2 grid (plus 1 warm-up)"},
+        "e2e": {"value": rate, "unit": "Gcell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "the reference (Rust) cannot be built here; this arm times the C++ restatement of its "
+                "SerialScheduler path with OpenMP over blocks (RayonScheduler's parallelism)",
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="own", choices=["own", "reference"])
+    ap.add_argument("--config", default="c2", choices=sorted(CONFIGS))
+    ap.add_argument("--dtype", default="f64", choices=["f64", "f32"])
+    ap.add_argument("--variant", type=int, default=0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    cfg = CONFIGS[args.config]
+    if args.impl == "reference":
+        run_reference(args, cfg)
+        return
+
+    import torch
+
+    import legendre_b200 as L
+
+    rank, world, local, pg = dist_setup(args.gpus)
+    stream = torch.cuda.current_stream()
+    sched = L.CudaScheduler(local, stream.cuda_stream)
+    sim, grid, model, grains = make_sim(cfg, args.dtype, sched, seed_offset=rank)
+    initialize(sim, grid, model, grains, cfg, args.dtype, sched)
+    dt = cfg["dt"]
+    cells = cfg["cells"] ** 2
+
+    # warm-up (also captures the step graph)
+    sim.run(dt, args.warmup, graph=True, variant=args.variant)
+    torch.cuda.synchronize()
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    barrier(pg)
+    torch.cuda.synchronize()
+    launches0 = sched.kernel_launches
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    sim.run(dt, args.steps, graph=True, variant=args.variant)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier(pg)
+    clk = clocks.stop()
+    launches = sched.kernel_launches - launches0
+    ms = max_over_ranks(pg, e0.elapsed_time(e1))
+    ms_per_step = ms / args.steps
+    value = world * cells * args.steps / (ms / 1e3) / 1e9
+
+    # end to end through the public API: pinned host state in, K steps, state out
+    e2e = None
+    sdtype = torch.float64 if args.dtype == "f64" else torch.float32
+    n_el = grid.num_blocks() * grid.block_len(1)
+    host_in = [torch.from_numpy(sim.state.download(f).reshape(-1)).pin_memory() for f in ("phi", "u")]
+    host_out = [torch.empty(n_el, dtype=sdtype).pin_memory() for _ in range(2)]
+    import ctypes as C
+
+    barrier(pg)
+    torch.cuda.synchronize()
+    e2 = torch.cuda.Event(enable_timing=True)
+    e3 = torch.cuda.Event(enable_timing=True)
+    e2.record(stream)
+    for f, buf in enumerate(host_in):
+        L._native.check(L._native.lib.lg_state_upload_field(sim.state.handle, f, C.c_void_p(buf.data_ptr()), n_el),
+                        sched.handle)
+    sim.run(dt, args.steps, graph=True, variant=args.variant)
+    for f, buf in enumerate(host_out):
+        L._native.check(L._native.lib.lg_state_download_field(sim.state.handle, f, C.c_void_p(buf.data_ptr()), n_el),
+                        sched.handle)
+    e3.record(stream)
+    torch.cuda.synchronize()
+    barrier(pg)
+    ms_e2e = max_over_ranks(pg, e2.elapsed_time(e3))
+    esz = 8 if args.dtype == "f64" else 4
+    e2e = {"value": world * cells * args.steps / (ms_e2e / 1e3) / 1e9, "unit": "Gcell-updates/s",
+           "h2d_bytes_per_step": 2 * n_el * esz / args.steps, "d2h_bytes_per_step": 2 * n_el * esz / args.steps,
+           "what": f"lg_state_upload_field x2 from pinned host + {args.steps} steps + lg_state_download_field x2, "
+                   "bytes amortised per step"}
+
+    if rank == 0:
+        peak, peak_kind = peaks()
+        algo = BYTES_PER_CELL[args.dtype] * cells
+        achieved = algo / (ms_per_step / 1e3) / 1e9
+        cpu = None
+        if not args.no_cpu_baseline and world == 1:
+            rate, steps_run, threads = cpu_oracle_rate(cfg, steps_budget_s=15.0, max_steps=1000)
+            cpu = {"value": rate, "unit": "Gcell-updates/s", "cores": threads, "kind": "port",
+                   "sample": f"{steps_run} steps of the same {cfg['cells']}^2 grid after 1 warm-up step, "
+                             "OpenMP over blocks"}
+        line = {
+            "metric": "Gcell-updates/s", "value": value, "unit": "Gcell-updates/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": args.dtype, "data": "synthetic",
+            "config": {"workload": cfg["workload"], "cells": cfg["cells"], "block": cfg["block"],
+                       "noise": cfg["noise"], "parallelism": f"replicas{world}",
+                       "l2": "state 2 fields x 2 buffers larger than L2; no flush",
+                       "graph": True, "variant": args.variant},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
+                         "algorithmic_bytes_per_cell": BYTES_PER_CELL[args.dtype]},
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": launches,
+            "clocks": {"sm_mhz": clk["sm_mhz"], "sm_max_mhz": clk["sm_max_mhz"], "reasons": clk["reasons"],
+                       "samples": clk["samples"]},
+        }
+        print(json.dumps(line), flush=True)
+    sched.close()
+    if pg is not None:
+        pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,162 @@
+/* legendre_b200 -- C ABI of the B200 block-stepping library.
+ *
+ * The reference (trbritt/legendre 0.1.4, Rust) has no FFI of its own: its
+ * device seam is two traits, `Scheduler` (src/core/scheduler.rs:25-38) and
+ * `Allocator`/`StorageBackend` (src/core/storage.rs:126-154).  A
+ * `CudaScheduler` cannot carry device work through `for_each_block_mut`
+ * (its closure is opaque host code), so the device path enters at
+ * integrator-step granularity and at the storage seam.  The entry points
+ * below are exactly what a Rust `CudaScheduler` / `CudaAllocator` /
+ * device-integrator wrapper binds; each comment names the reference
+ * interface it replaces.
+ *
+ * Conventions
+ *  - Every function returns an int status: LG_OK (0) or a negative LG_ERR_*;
+ *    lg_last_error(ctx) gives the text of the last failure on that context.
+ *  - All device work of a context runs in order on its one stream; calls on
+ *    one context are not re-entrant (one host thread per context).
+ *  - Host arrays are plain pointers + element counts; nothing here takes
+ *    PyTorch or CUDA-runtime C++ types.
+ *  - Field data crosses the boundary in the reference's layout: for each
+ *    block in BlockId order, the field's ghost-inclusive slab, dimension 0
+ *    fastest (src/geometry/cartesian.rs:8-11).
+ */
+#ifndef LEGENDRE_B200_H
+#define LEGENDRE_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LG_ABI_VERSION 1
+
+enum lg_status {
+    LG_OK = 0,
+    LG_ERR_INVALID = -1,   /* bad argument (the reference panics or returns GridError) */
+    LG_ERR_CUDA = -2,      /* a CUDA runtime call failed */
+    LG_ERR_NOMEM = -3,     /* device allocation failed */
+    LG_ERR_TIMEOUT = -4,   /* lg_sync gave up waiting */
+    LG_ERR_STATE = -5,     /* call out of order (e.g. wrong dtype or field) */
+    LG_ERR_DEVICE = -6     /* a kernel reported a device-side error flag */
+};
+
+enum lg_dtype { LG_F64 = 0, LG_F32 = 1 };
+
+/* Run flags. */
+#define LG_RUN_GRAPH 1u      /* capture the step sequence once in a CUDA graph and replay it */
+
+typedef struct lg_ctx lg_ctx;
+typedef struct lg_grid lg_grid;
+typedef struct lg_state lg_state;
+
+/* ---------------------------------------------------------------- context
+ * The `CudaScheduler` itself: device, stream, error text.  Replaces
+ * `SerialScheduler`/`RayonScheduler` (src/core/scheduler.rs:39-84) as the
+ * type-level selector of the device path.  `stream` may be NULL (the
+ * context creates its own) or an existing cudaStream_t to run on. */
+int lg_abi_version(void);
+int lg_ctx_create(int device, void* stream, lg_ctx** out);
+int lg_ctx_destroy(lg_ctx* ctx);
+const char* lg_last_error(const lg_ctx* ctx);
+/* Wait for all work of the context; LG_ERR_TIMEOUT after timeout_ms (< 0: no limit). */
+int lg_sync(lg_ctx* ctx, int64_t timeout_ms);
+/* Number of kernels this context has launched (its own kernels only). */
+int64_t lg_ctx_kernel_launches(const lg_ctx* ctx);
+
+/* ------------------------------------------------------------------- grid
+ * Device block-topology table of a `CartesianGrid<D>`
+ * (src/geometry/cartesian.rs:48-97): D <= 3, cells[d] % block[d] == 0,
+ * spacing > 0 (CartesianGrid::new errors -> LG_ERR_INVALID); periodic[d]
+ * is `with_periodic`.  Face neighbours follow `face_neighbor`
+ * (cartesian.rs:162-181). */
+int lg_grid_create_cartesian(lg_ctx* ctx, int D, const int64_t* cells, const int64_t* block_cells,
+                             const double* origin, const double* spacing, const int* periodic, lg_grid** out);
+int lg_grid_destroy(lg_grid* grid);
+int64_t lg_grid_num_blocks(const lg_grid* grid);
+/* Neighbour of `block` across face (dim, dir = -1/+1); *out = -1 at a physical boundary. */
+int lg_grid_face_neighbor(const lg_grid* grid, int64_t block, int dim, int dir, int64_t* out);
+
+/* ------------------------------------------------------------------ state
+ * The `CudaAllocator`: one device arena per state, block-major slabs, zero
+ * initialised (replaces StateBuilder::build / BlockStorage::allocate,
+ * src/core/state.rs:207-264, and SystemAllocator, storage.rs:560-572).
+ * Field f has ghost width ghosts[f] <= every block extent
+ * (cartesian.rs:456-462).  The arena is double-buffered: steps read one
+ * copy and write the other, which stands in for the reference's stage
+ * buffers (simulation.rs:187-202). */
+int lg_state_create(lg_ctx* ctx, const lg_grid* grid, int dtype, int nfields, const int* ghosts, lg_state** out);
+int lg_state_destroy(lg_state* st);
+/* Host <-> device copies of one field, every block, ghost-inclusive slabs in
+ * BlockId order (`State::slab`/`slab_mut`, state.rs:413-424).  `nelem` must
+ * equal num_blocks * block_len(ghost).  Uploading marks ghosts stale; the
+ * next step refills them first. */
+int lg_state_upload_field(lg_state* st, int field, const void* host, int64_t nelem);
+int lg_state_download_field(lg_state* st, int field, void* host, int64_t nelem);
+/* Device address and length of one slab of the current buffer
+ * (`StorageBackend::as_slice`, storage.rs:126-138, on device memory). */
+int lg_state_slab(lg_state* st, int64_t block, int field, void** dev, int64_t* len);
+/* `Simulation::time` / its step counter (simulation.rs:225-233). */
+int lg_state_get_time(const lg_state* st, double* t, int64_t* step_index);
+int lg_state_set_time(lg_state* st, double t, int64_t step_index);
+
+/* -------------------------------------------------------------- kernels */
+
+/* (b) Ghost fill of one field: halo exchange, periodic wrap and mirror
+ * (no-flux) boundaries -- `fill_ghosts_mirror` (cartesian.rs:392-401,
+ * 439-526; FaceBc::Mirror, boundary.rs:63-66).  Result identical to the
+ * reference's dimension sweep, corners included. */
+int lg_fill_ghosts(lg_state* st, int field);
+
+/* (d) `nsteps` forward-Euler steps of the heat model `Heat<D>`
+ * (examples/heat3d.rs:41-85, tests/heat3d.rs:33-80): u += dt * (kappa *
+ * CentralLaplacian(u)) (finite_difference.rs:49-67, euler.rs:28-54).  The
+ * field must have ghost width 1.  Advances the state's time by dt per step. */
+int lg_heat_fe_run(lg_state* st, int field, double kappa, double dt, int64_t nsteps, uint32_t flags);
+
+/* Model C parameters: the public fields of `ModelC`
+ * (src/physics/phasefield.rs:55-66) and `FiniteVolume::tol`
+ * (finite_volume.rs:41-50).  noise_amplitude != 0 selects
+ * `ModelC<Wiener<1>>`, 0 selects `ModelC<NoNoise>`. */
+typedef struct lg_modelc_params {
+    double eps4;
+    double lambda;
+    double d_thermal;
+    double noise_amplitude;
+    double anisotropy_tol;
+    double flux_tol;
+} lg_modelc_params;
+
+/* (a) `nsteps` Euler-Maruyama steps of Model C on a 2-D Cartesian state with
+ * fields phi (0) and u (1), ghost 1 -- EulerMaruyama::step
+ * (src/integrators/euler_maruyama.rs:34-75) with
+ * ModelC::vector_field_block (phasefield.rs:353-422), fill_ghosts
+ * (phasefield.rs:431-439) and State::apply_step_with (state.rs:656-699) in
+ * one fused kernel per step.  The noise salt of each step is the bit
+ * pattern of the state's time before the step; `seed` is
+ * `EulerMaruyama::seed`.  FP64 states are bit-identical to the reference
+ * without noise; with noise the integer key stream is exact and the
+ * Gaussian is within 1e-12 relative.  `variant` selects a kernel shape
+ * (0 = library default). */
+int lg_modelc_em_run(lg_state* st, const lg_modelc_params* p, double dt, uint64_t seed, int64_t nsteps,
+                     int variant, uint32_t flags);
+
+/* Initial conditions, computed on the host exactly as the reference does and
+ * uploaded.  `ModelC::initialize_grains` without orientations
+ * (phasefield.rs:227-314): grains = n x (cx, cy, radius, orientation). */
+int lg_modelc_initialize_grains(lg_state* st, const double* grains, int64_t n, double u0);
+/* Heat initial condition of the 96^3 benchmark: sin(2 pi x) sin(2 pi y)
+ * sin(2 pi z) + amp * (2 * unit_open(mix_key(seed, [gx, gy, gz])) - 1) at
+ * cell centres (gx.. = global cell index); the reference has no such
+ * helper, it is a `fill_from_fn` closure (cartesian.rs:546-559). */
+int lg_heat_initialize_sine_noise(lg_state* st, int field, uint64_t seed, double amp);
+
+/* Standard normals of n keys on the device (`rng::standard_normal`,
+ * src/util/rng.rs:43-49); host arrays in and out. */
+int lg_standard_normal(lg_ctx* ctx, const uint64_t* keys, int64_t n, double* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

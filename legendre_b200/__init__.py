@@ -1,0 +1,16 @@
+"""legendre_b200: the B200 device path of legendre's block-stepping hot path.
+
+Importing the package loads ``liblegendre_b200.so`` (built in-tree by
+``python -m legendre_b200.build``) and fails if it is missing.
+"""
+from ._native import LegendreError, exported_symbols  # noqa: F401  (loads the library)
+from .core import CudaAllocator, CudaScheduler, DeviceState, FieldSpec, Simulation, StateBuilder, TIME, wiener
+from .geometry import CartesianGrid, GridError
+from .integrators import EulerMaruyama, FiniteDifference, FiniteVolume, ForwardEuler
+from .physics import A1, A2, Grain, Heat, ModelC, seed_positions
+
+__all__ = [
+    "A1", "A2", "CartesianGrid", "CudaAllocator", "CudaScheduler", "DeviceState", "EulerMaruyama", "FieldSpec",
+    "FiniteDifference", "FiniteVolume", "ForwardEuler", "Grain", "GridError", "Heat", "LegendreError", "ModelC",
+    "Simulation", "StateBuilder", "TIME", "seed_positions", "wiener",
+]

@@ -1,0 +1,94 @@
+"""Build the native pieces in-tree.
+
+``build_library()`` compiles the CUDA sources under ``csrc/`` for sm_100a into
+``legendre_b200/liblegendre_b200.so`` (plain ``nvcc``; no PyTorch extension
+machinery, the library exports a C ABI only).  ``build_oracle()`` compiles
+the CPU restatement used by the tests into ``oracle/liblegendre_oracle.so``.
+
+Run ``python -m legendre_b200.build`` to build both.
+"""
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+from pathlib import Path
+
+PKG = Path(__file__).resolve().parent
+ROOT = PKG.parent
+CSRC = PKG / "csrc"
+LIB = PKG / "liblegendre_b200.so"
+ORACLE_DIR = ROOT / "oracle"
+ORACLE_LIB = ORACLE_DIR / "liblegendre_oracle.so"
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+# Translation units and their floating-point contraction policy.  The FP64
+# reference-order kernels must not contract a*b+c (the reference is Rust,
+# which never does); units holding only freely restructured FP32 kernels may.
+SOURCES = [
+    ("lg_kernels.cu", ["-fmad=false"]),
+    ("lg_abi.cu", ["-fmad=false"]),
+]
+
+
+def _nvcc() -> str:
+    for cand in (os.environ.get("NVCC"), shutil.which("nvcc"), "/usr/local/cuda/bin/nvcc"):
+        if cand and Path(cand).exists():
+            return cand
+    raise RuntimeError("nvcc not found; the CUDA toolkit is required to build legendre_b200")
+
+
+def _stale(target: Path, deps) -> bool:
+    if not target.exists():
+        return True
+    t = target.stat().st_mtime
+    return any(Path(d).stat().st_mtime > t for d in deps)
+
+
+def build_library(force: bool = False, verbose: bool = False) -> Path:
+    deps = [CSRC / s for s, _ in SOURCES] + list(CSRC.glob("*.h")) + list(CSRC.glob("*.cuh"))
+    deps.append(ROOT / "include" / "legendre_b200.h")
+    if not force and not _stale(LIB, deps):
+        return LIB
+    nvcc = _nvcc()
+    objdir = PKG / "_build"
+    objdir.mkdir(exist_ok=True)
+    objs = []
+    for src, flags in SOURCES:
+        obj = objdir / (Path(src).stem + ".o")
+        cmd = [nvcc, "-O3", "-std=c++17", *ARCH, "-lineinfo", "-Xcompiler", "-fPIC", *flags,
+               "-I", str(ROOT / "include"), "-c", str(CSRC / src), "-o", str(obj)]
+        if verbose:
+            cmd.insert(1, "-Xptxas=-v")
+        _run(cmd)
+        objs.append(str(obj))
+    _run([nvcc, "-shared", *ARCH, *objs, "-o", str(LIB)])
+    return LIB
+
+
+def build_oracle(force: bool = False) -> Path:
+    src = ORACLE_DIR / "legendre_oracle.cpp"
+    deps = [src, ORACLE_DIR / "legendre_oracle.h"]
+    if not force and not _stale(ORACLE_LIB, deps):
+        return ORACLE_LIB
+    cxx = shutil.which("g++") or "g++"
+    _run([cxx, "-O2", "-std=c++17", "-ffp-contract=off", "-fopenmp", "-fPIC", "-shared", str(src),
+          "-o", str(ORACLE_LIB)])
+    return ORACLE_LIB
+
+
+def _run(cmd):
+    proc = subprocess.run(cmd, capture_output=True, text=True)
+    if proc.returncode != 0:
+        sys.stderr.write(proc.stdout + proc.stderr)
+        raise RuntimeError("build step failed: " + " ".join(cmd))
+    if proc.stderr.strip():
+        sys.stderr.write(proc.stderr)
+
+
+if __name__ == "__main__":
+    force = "--force" in sys.argv
+    print(build_library(force=force, verbose="-v" in sys.argv))
+    print(build_oracle(force=force))

@@ -1,0 +1,675 @@
+// C ABI of the legendre B200 library: contexts (the CudaScheduler), device
+// block-topology tables, state arenas (the CudaAllocator), run loops and
+// CUDA-graph capture of step sequences.  Declarations and contracts live in
+// include/legendre_b200.h.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "../../include/legendre_b200.h"
+#include "lg_kernels.h"
+
+struct lg_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    std::string err;
+    int64_t launches = 0;
+};
+
+struct lg_grid {
+    lg_ctx* ctx = nullptr;
+    int D = 0;
+    int64_t cells[3] = {1, 1, 1}, block[3] = {1, 1, 1}, nb[3] = {1, 1, 1};
+    double origin[3] = {0, 0, 0}, spacing[3] = {1, 1, 1};
+    int periodic[3] = {0, 0, 0};
+    int64_t nblocks = 0;
+    std::vector<int> h_nbr;  // nblocks * 3 * 2
+    int* d_nbr = nullptr;
+};
+
+struct GraphEntry {
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    int64_t steps = 0;
+    int64_t launches = 0;
+};
+
+struct lg_state {
+    lg_ctx* ctx = nullptr;
+    const lg_grid* grid = nullptr;
+    int dtype = LG_F64;
+    int esize = 8;
+    int nfields = 0;
+    std::vector<int> ghosts;
+    int64_t slab_stride = 0;  // elements
+    void* arena[2] = {nullptr, nullptr};
+    int cur = 0;
+    double* d_t = nullptr;    // two time slots
+    int tslot = 0;
+    double t = 0.0;
+    int64_t step_index = 0;
+    bool ghosts_valid = false;
+    std::map<std::string, GraphEntry> graphs;
+};
+
+namespace {
+
+int fail(lg_ctx* ctx, int code, const std::string& msg) {
+    if (ctx) ctx->err = msg;
+    return code;
+}
+
+int cuda_fail(lg_ctx* ctx, cudaError_t e, const char* what) {
+    return fail(ctx, LG_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define LG_CUDA(ctx, call)                                        \
+    do {                                                          \
+        cudaError_t e_ = (call);                                  \
+        if (e_ != cudaSuccess) return cuda_fail((ctx), e_, #call); \
+    } while (0)
+
+int64_t block_len(const lg_grid* g, int ghost) {
+    int64_t n = 1;
+    for (int d = 0; d < g->D; ++d) n *= g->block[d] + 2 * ghost;
+    return n;
+}
+
+lg::CartTopo topo_of(const lg_grid* g) {
+    lg::CartTopo t{};
+    t.D = g->D;
+    for (int d = 0; d < 3; ++d) {
+        t.n[d] = (int)g->block[d];
+        t.nb[d] = (int)g->nb[d];
+    }
+    t.nblocks = (int)g->nblocks;
+    t.nbr = g->d_nbr;
+    return t;
+}
+
+lg::SlabLayout layout_of(const lg_state* st, int field) {
+    lg::SlabLayout L{};
+    L.nfields = st->nfields;
+    L.ghost = st->ghosts[field];
+    L.slab_stride = st->slab_stride;
+    L.len = block_len(st->grid, L.ghost);
+    for (int d = 0; d < 3; ++d) L.gdim[d] = d < st->grid->D ? (int)st->grid->block[d] + 2 * L.ghost : 1;
+    return L;
+}
+
+// face_neighbor (cartesian.rs:162-181)
+int64_t face_neighbor(const lg_grid* g, int64_t b, int dim, int dir) {
+    int64_t c[3] = {0, 0, 0}, rem = b;
+    for (int d = 0; d < g->D; ++d) {
+        c[d] = rem % g->nb[d];
+        rem /= g->nb[d];
+    }
+    int64_t stepped = c[dim] + (dir < 0 ? -1 : 1), next;
+    if (stepped >= 0 && stepped < g->nb[dim]) next = stepped;
+    else if (g->periodic[dim]) next = ((stepped % g->nb[dim]) + g->nb[dim]) % g->nb[dim];
+    else return -1;
+    int64_t id = 0, stride = 1;
+    for (int d = 0; d < g->D; ++d) {
+        id += (d == dim ? next : c[d]) * stride;
+        stride *= g->nb[d];
+    }
+    return id;
+}
+
+int fill_all_ghosts(lg_state* st) {
+    lg_ctx* ctx = st->ctx;
+    for (int f = 0; f < st->nfields; ++f) {
+        if (st->ghosts[f] == 0) continue;
+        cudaError_t e = lg::launch_halo_fill(st->arena[st->cur], st->esize, topo_of(st->grid), layout_of(st, f), f,
+                                             ctx->stream);
+        ctx->launches++;
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "halo fill launch");
+    }
+    st->ghosts_valid = true;
+    return LG_OK;
+}
+
+// Run `nsteps` of a step functor, optionally through a cached CUDA graph of
+// an even number of steps (so the ping-pong buffer and time slot return to
+// their starting parity after every replay).
+template <class StepFn>
+int run_steps(lg_state* st, const std::string& key, int64_t nsteps, uint32_t flags, StepFn step) {
+    lg_ctx* ctx = st->ctx;
+    int64_t done = 0;
+    if ((flags & LG_RUN_GRAPH) && nsteps >= 2) {
+        const int64_t chunk = std::min<int64_t>(nsteps - (nsteps & 1), 64);
+        std::string gk = key + "|chunk=" + std::to_string(chunk) + "|cur=" + std::to_string(st->cur) +
+                         "|slot=" + std::to_string(st->tslot);
+        auto it = st->graphs.find(gk);
+        if (it == st->graphs.end()) {
+            GraphEntry ge;
+            ge.steps = chunk;
+            int64_t before = ctx->launches;
+            LG_CUDA(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+            int cur0 = st->cur, slot0 = st->tslot;
+            int rc = LG_OK;
+            for (int64_t s = 0; s < chunk && rc == LG_OK; ++s) rc = step();
+            cudaError_t ec = cudaStreamEndCapture(ctx->stream, &ge.graph);
+            st->cur = cur0;
+            st->tslot = slot0;
+            ge.launches = ctx->launches - before;
+            ctx->launches = before;
+            if (rc != LG_OK) {
+                if (ge.graph) cudaGraphDestroy(ge.graph);
+                return rc;
+            }
+            if (ec != cudaSuccess) return cuda_fail(ctx, ec, "cudaStreamEndCapture");
+            LG_CUDA(ctx, cudaGraphInstantiate(&ge.exec, ge.graph, 0));
+            it = st->graphs.emplace(gk, ge).first;
+        }
+        const GraphEntry& ge = it->second;
+        while (nsteps - done >= ge.steps) {
+            LG_CUDA(ctx, cudaGraphLaunch(ge.exec, ctx->stream));
+            ctx->launches += ge.launches;
+            done += ge.steps;
+        }
+    }
+    for (; done < nsteps; ++done) {
+        int rc = step();
+        if (rc != LG_OK) return rc;
+    }
+    return LG_OK;
+}
+
+// Host-side time bookkeeping of `steps` steps: t += dt each
+// (simulation.rs:285-286), the same IEEE additions the kernels perform.
+void advance_time(lg_state* st, double dt, int64_t steps) {
+    for (int64_t s = 0; s < steps; ++s) st->t += dt;
+    st->step_index += steps;
+}
+
+}  // namespace
+
+extern "C" {
+
+int lg_abi_version(void) { return LG_ABI_VERSION; }
+
+int lg_ctx_create(int device, void* stream, lg_ctx** out) {
+    if (!out) return LG_ERR_INVALID;
+    *out = nullptr;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || device < 0 || device >= n) return LG_ERR_CUDA;
+    if (cudaSetDevice(device) != cudaSuccess) return LG_ERR_CUDA;
+    lg_ctx* ctx = new lg_ctx();
+    ctx->device = device;
+    if (stream) {
+        ctx->stream = static_cast<cudaStream_t>(stream);
+    } else {
+        if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
+            delete ctx;
+            return LG_ERR_CUDA;
+        }
+        ctx->own_stream = true;
+    }
+    *out = ctx;
+    return LG_OK;
+}
+
+int lg_ctx_destroy(lg_ctx* ctx) {
+    if (!ctx) return LG_ERR_INVALID;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+    return LG_OK;
+}
+
+const char* lg_last_error(const lg_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+int64_t lg_ctx_kernel_launches(const lg_ctx* ctx) { return ctx ? ctx->launches : -1; }
+
+int lg_sync(lg_ctx* ctx, int64_t timeout_ms) {
+    if (!ctx) return LG_ERR_INVALID;
+    auto t0 = std::chrono::steady_clock::now();
+    for (;;) {
+        cudaError_t e = cudaStreamQuery(ctx->stream);
+        if (e == cudaSuccess) return LG_OK;
+        if (e != cudaErrorNotReady) return cuda_fail(ctx, e, "stream");
+        if (timeout_ms >= 0) {
+            auto ms = std::chrono::duration_cast<std::chrono::milliseconds>(std::chrono::steady_clock::now() - t0);
+            if (ms.count() > timeout_ms) return fail(ctx, LG_ERR_TIMEOUT, "lg_sync timed out");
+        }
+        std::this_thread::sleep_for(std::chrono::microseconds(50));
+    }
+}
+
+int lg_grid_create_cartesian(lg_ctx* ctx, int D, const int64_t* cells, const int64_t* block_cells,
+                             const double* origin, const double* spacing, const int* periodic, lg_grid** out) {
+    if (!ctx || !out || !cells || !block_cells || !origin || !spacing || !periodic)
+        return fail(ctx, LG_ERR_INVALID, "null argument");
+    *out = nullptr;
+    if (D < 1 || D > 3) return fail(ctx, LG_ERR_INVALID, "dimension must be 1, 2 or 3");
+    lg_grid* g = new lg_grid();
+    g->ctx = ctx;
+    g->D = D;
+    g->nblocks = 1;
+    for (int d = 0; d < D; ++d) {
+        // CartesianGrid::new (cartesian.rs:48-82)
+        if (!(cells[d] > 0 && block_cells[d] > 0)) {
+            delete g;
+            return fail(ctx, LG_ERR_INVALID, "empty dimension " + std::to_string(d));
+        }
+        if (cells[d] % block_cells[d] != 0) {
+            delete g;
+            return fail(ctx, LG_ERR_INVALID, "cells not divisible by block cells in dimension " + std::to_string(d));
+        }
+        if (!(spacing[d] > 0.0) || !std::isfinite(spacing[d])) {
+            delete g;
+            return fail(ctx, LG_ERR_INVALID, "invalid spacing in dimension " + std::to_string(d));
+        }
+        g->cells[d] = cells[d];
+        g->block[d] = block_cells[d];
+        g->nb[d] = cells[d] / block_cells[d];
+        g->origin[d] = origin[d];
+        g->spacing[d] = spacing[d];
+        g->periodic[d] = periodic[d] ? 1 : 0;
+        g->nblocks *= g->nb[d];
+    }
+    if (g->nblocks > (int64_t)1 << 30) {
+        delete g;
+        return fail(ctx, LG_ERR_INVALID, "too many blocks");
+    }
+    g->h_nbr.assign(g->nblocks * 6, -1);
+    for (int64_t b = 0; b < g->nblocks; ++b)
+        for (int d = 0; d < D; ++d)
+            for (int s = 0; s < 2; ++s) g->h_nbr[(b * 3 + d) * 2 + s] = (int)face_neighbor(g, b, d, s ? 1 : -1);
+    cudaSetDevice(ctx->device);
+    cudaError_t e = cudaMalloc(&g->d_nbr, g->h_nbr.size() * sizeof(int));
+    if (e != cudaSuccess) {
+        delete g;
+        return fail(ctx, LG_ERR_NOMEM, "topology table allocation failed");
+    }
+    e = cudaMemcpy(g->d_nbr, g->h_nbr.data(), g->h_nbr.size() * sizeof(int), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        cudaFree(g->d_nbr);
+        delete g;
+        return cuda_fail(ctx, e, "topology upload");
+    }
+    *out = g;
+    return LG_OK;
+}
+
+int lg_grid_destroy(lg_grid* g) {
+    if (!g) return LG_ERR_INVALID;
+    cudaSetDevice(g->ctx->device);
+    cudaStreamSynchronize(g->ctx->stream);
+    cudaFree(g->d_nbr);
+    delete g;
+    return LG_OK;
+}
+
+int64_t lg_grid_num_blocks(const lg_grid* g) { return g ? g->nblocks : -1; }
+
+int lg_grid_face_neighbor(const lg_grid* g, int64_t block, int dim, int dir, int64_t* out) {
+    if (!g || !out || block < 0 || block >= g->nblocks || dim < 0 || dim >= g->D || (dir != 1 && dir != -1))
+        return LG_ERR_INVALID;
+    *out = face_neighbor(g, block, dim, dir);
+    return LG_OK;
+}
+
+int lg_state_create(lg_ctx* ctx, const lg_grid* grid, int dtype, int nfields, const int* ghosts, lg_state** out) {
+    if (!ctx || !grid || !out || nfields < 1 || !ghosts) return fail(ctx, LG_ERR_INVALID, "bad state arguments");
+    *out = nullptr;
+    if (dtype != LG_F64 && dtype != LG_F32) return fail(ctx, LG_ERR_INVALID, "dtype must be LG_F64 or LG_F32");
+    int64_t maxlen = 0;
+    for (int f = 0; f < nfields; ++f) {
+        for (int d = 0; d < grid->D; ++d)
+            if (ghosts[f] < 0 || ghosts[f] > grid->block[d])
+                return fail(ctx, LG_ERR_INVALID,
+                            "ghost width " + std::to_string(ghosts[f]) + " exceeds block extent in dimension " +
+                                std::to_string(d));
+        maxlen = std::max(maxlen, block_len(grid, ghosts[f]));
+    }
+    lg_state* st = new lg_state();
+    st->ctx = ctx;
+    st->grid = grid;
+    st->dtype = dtype;
+    st->esize = dtype == LG_F64 ? 8 : 4;
+    st->nfields = nfields;
+    st->ghosts.assign(ghosts, ghosts + nfields);
+    const int64_t align = 256 / st->esize;
+    st->slab_stride = (maxlen + align - 1) / align * align;
+    const size_t bytes = (size_t)grid->nblocks * nfields * st->slab_stride * st->esize;
+    cudaSetDevice(ctx->device);
+    for (int k = 0; k < 2; ++k) {
+        if (cudaMalloc(&st->arena[k], bytes) != cudaSuccess) {
+            cudaGetLastError();
+            for (int j = 0; j < k; ++j) cudaFree(st->arena[j]);
+            delete st;
+            return fail(ctx, LG_ERR_NOMEM, "state arena allocation of " + std::to_string(bytes) + " bytes failed");
+        }
+        cudaMemsetAsync(st->arena[k], 0, bytes, ctx->stream);
+    }
+    if (cudaMalloc(&st->d_t, 2 * sizeof(double)) != cudaSuccess) {
+        cudaFree(st->arena[0]);
+        cudaFree(st->arena[1]);
+        delete st;
+        return fail(ctx, LG_ERR_NOMEM, "time slot allocation failed");
+    }
+    cudaMemsetAsync(st->d_t, 0, 2 * sizeof(double), ctx->stream);
+    cudaError_t e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) {
+        lg_state_destroy(st);
+        return cuda_fail(ctx, e, "state initialisation");
+    }
+    *out = st;
+    return LG_OK;
+}
+
+int lg_state_destroy(lg_state* st) {
+    if (!st) return LG_ERR_INVALID;
+    cudaSetDevice(st->ctx->device);
+    cudaStreamSynchronize(st->ctx->stream);
+    for (auto& kv : st->graphs) {
+        if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+        if (kv.second.graph) cudaGraphDestroy(kv.second.graph);
+    }
+    cudaFree(st->arena[0]);
+    cudaFree(st->arena[1]);
+    cudaFree(st->d_t);
+    delete st;
+    return LG_OK;
+}
+
+static int field_copy(lg_state* st, int field, void* host, int64_t nelem, bool upload) {
+    lg_ctx* ctx = st->ctx;
+    if (field < 0 || field >= st->nfields) return fail(ctx, LG_ERR_INVALID, "field index out of range");
+    const int64_t len = block_len(st->grid, st->ghosts[field]);
+    if (!host || nelem != len * st->grid->nblocks)
+        return fail(ctx, LG_ERR_INVALID, "element count must be num_blocks * block_len(ghost)");
+    char* dev = static_cast<char*>(st->arena[st->cur]) + (size_t)field * st->slab_stride * st->esize;
+    const size_t dpitch = (size_t)st->nfields * st->slab_stride * st->esize;
+    const size_t width = (size_t)len * st->esize;
+    cudaSetDevice(ctx->device);
+    if (upload) {
+        LG_CUDA(ctx, cudaMemcpy2DAsync(dev, dpitch, host, width, width, st->grid->nblocks, cudaMemcpyHostToDevice,
+                                       ctx->stream));
+        st->ghosts_valid = false;
+    } else {
+        LG_CUDA(ctx, cudaMemcpy2DAsync(host, width, dev, dpitch, width, st->grid->nblocks, cudaMemcpyDeviceToHost,
+                                       ctx->stream));
+    }
+    LG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return LG_OK;
+}
+
+int lg_state_upload_field(lg_state* st, int field, const void* host, int64_t nelem) {
+    if (!st) return LG_ERR_INVALID;
+    return field_copy(st, field, const_cast<void*>(host), nelem, true);
+}
+
+int lg_state_download_field(lg_state* st, int field, void* host, int64_t nelem) {
+    if (!st) return LG_ERR_INVALID;
+    return field_copy(st, field, host, nelem, false);
+}
+
+int lg_state_slab(lg_state* st, int64_t block, int field, void** dev, int64_t* len) {
+    if (!st || !dev || !len) return LG_ERR_INVALID;
+    if (block < 0 || block >= st->grid->nblocks || field < 0 || field >= st->nfields)
+        return fail(st->ctx, LG_ERR_INVALID, "block or field out of range");
+    *dev = static_cast<char*>(st->arena[st->cur]) + ((size_t)block * st->nfields + field) * st->slab_stride * st->esize;
+    *len = block_len(st->grid, st->ghosts[field]);
+    return LG_OK;
+}
+
+int lg_state_get_time(const lg_state* st, double* t, int64_t* step_index) {
+    if (!st || !t || !step_index) return LG_ERR_INVALID;
+    *t = st->t;
+    *step_index = st->step_index;
+    return LG_OK;
+}
+
+int lg_state_set_time(lg_state* st, double t, int64_t step_index) {
+    if (!st) return LG_ERR_INVALID;
+    st->t = t;
+    st->step_index = step_index;
+    return LG_OK;
+}
+
+int lg_fill_ghosts(lg_state* st, int field) {
+    if (!st) return LG_ERR_INVALID;
+    lg_ctx* ctx = st->ctx;
+    if (field < 0 || field >= st->nfields) return fail(ctx, LG_ERR_INVALID, "field index out of range");
+    cudaSetDevice(ctx->device);
+    cudaError_t e = lg::launch_halo_fill(st->arena[st->cur], st->esize, topo_of(st->grid), layout_of(st, field),
+                                         field, ctx->stream);
+    ctx->launches++;
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "halo fill launch");
+    return LG_OK;
+}
+
+int lg_heat_fe_run(lg_state* st, int field, double kappa, double dt, int64_t nsteps, uint32_t flags) {
+    if (!st) return LG_ERR_INVALID;
+    lg_ctx* ctx = st->ctx;
+    if (st->dtype != LG_F64) return fail(ctx, LG_ERR_STATE, "the heat path is FP64");
+    if (field < 0 || field >= st->nfields || st->ghosts[field] != 1)
+        return fail(ctx, LG_ERR_STATE, "heat field must exist and have ghost width 1");
+    if (nsteps < 0) return fail(ctx, LG_ERR_INVALID, "negative step count");
+    cudaSetDevice(ctx->device);
+    if (!st->ghosts_valid) {
+        int rc = fill_all_ghosts(st);
+        if (rc != LG_OK) return rc;
+    }
+    double inv_h2[3] = {0, 0, 0};
+    for (int d = 0; d < st->grid->D; ++d) inv_h2[d] = 1.0 / (st->grid->spacing[d] * st->grid->spacing[d]);
+    const lg::CartTopo topo = topo_of(st->grid);
+    const lg::SlabLayout L = layout_of(st, field);
+    char key[256];
+    snprintf(key, sizeof key, "heat|f=%d|k=%a|dt=%a", field, kappa, dt);
+    auto step = [&]() -> int {
+        const double* in = static_cast<const double*>(st->arena[st->cur]);
+        double* out = static_cast<double*>(st->arena[st->cur ^ 1]);
+        cudaError_t e = lg::launch_heat_step(in, out, topo, L, field, kappa, dt, inv_h2, ctx->stream);
+        ctx->launches++;
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "heat step launch");
+        st->cur ^= 1;
+        st->tslot ^= 1;
+        return LG_OK;
+    };
+    int rc = run_steps(st, key, nsteps, flags, step);
+    if (rc != LG_OK) return rc;
+    if (nsteps & 1) {
+        // graph replays keep parity; the remainder steps already flipped it
+    }
+    advance_time(st, dt, nsteps);
+    return LG_OK;
+}
+
+int lg_modelc_em_run(lg_state* st, const lg_modelc_params* p, double dt, uint64_t seed, int64_t nsteps,
+                     int variant, uint32_t flags) {
+    if (!st || !p) return LG_ERR_INVALID;
+    lg_ctx* ctx = st->ctx;
+    if (st->grid->D != 2 || st->nfields < 2 || st->ghosts[0] != 1 || st->ghosts[1] != 1)
+        return fail(ctx, LG_ERR_STATE, "Model C needs a 2-D state with phi and u of ghost width 1");
+    if (nsteps < 0) return fail(ctx, LG_ERR_INVALID, "negative step count");
+    cudaSetDevice(ctx->device);
+    if (!st->ghosts_valid) {
+        int rc = fill_all_ghosts(st);
+        if (rc != LG_OK) return rc;
+    }
+    lg::ModelCDev m{};
+    m.lambda = p->lambda;
+    m.d_thermal = p->d_thermal;
+    m.a_bar = std::fma(3.0, -p->eps4, 1.0);            // phasefield.rs:101
+    m.eps_prime = 3.0 * p->eps4 / m.a_bar;             // phasefield.rs:109
+    m.tol = p->anisotropy_tol;
+    m.f_a_bar = std::fma(3.0, -p->eps4, 1.0);          // finite_volume.rs:114
+    m.f_eps_prime = 3.0 * p->eps4 / m.f_a_bar;         // finite_volume.rs:115
+    m.f_a12 = 4.0 * m.f_a_bar * m.f_eps_prime;         // finite_volume.rs:119
+    m.f_tol = p->flux_tol;
+    m.inv_h2_flux = 1.0 / (st->grid->spacing[0] * st->grid->spacing[1]);
+    m.inv_h2[0] = 1.0 / (st->grid->spacing[0] * st->grid->spacing[0]);
+    m.inv_h2[1] = 1.0 / (st->grid->spacing[1] * st->grid->spacing[1]);
+    lg::NoiseDev nz{};
+    nz.on = p->noise_amplitude != 0.0 ? 1 : 0;
+    nz.seed = seed;
+    nz.amp = p->noise_amplitude;
+    // the device time slot starts from the host's time
+    LG_CUDA(ctx, cudaMemcpyAsync(st->d_t + st->tslot, &st->t, sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    const lg::CartTopo topo = topo_of(st->grid);
+    const lg::SlabLayout L = layout_of(st, 0);
+    char key[512];
+    snprintf(key, sizeof key, "modelc|%a|%a|%a|%a|%a|%a|dt=%a|seed=%llu|v=%d", p->eps4, p->lambda, p->d_thermal,
+             p->noise_amplitude, p->anisotropy_tol, p->flux_tol, dt, (unsigned long long)seed, variant);
+    auto step = [&]() -> int {
+        cudaError_t e;
+        if (st->dtype == LG_F64)
+            e = lg::launch_modelc_step_f64(static_cast<const double*>(st->arena[st->cur]),
+                                           static_cast<double*>(st->arena[st->cur ^ 1]), topo, L, m, dt, nz, st->d_t,
+                                           st->tslot, variant, ctx->stream);
+        else
+            e = lg::launch_modelc_step_f32(static_cast<const float*>(st->arena[st->cur]),
+                                           static_cast<float*>(st->arena[st->cur ^ 1]), topo, L, m, dt, nz, st->d_t,
+                                           st->tslot, variant, ctx->stream);
+        ctx->launches++;
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "Model C step launch");
+        st->cur ^= 1;
+        st->tslot ^= 1;
+        return LG_OK;
+    };
+    int rc = run_steps(st, key, nsteps, flags, step);
+    if (rc != LG_OK) return rc;
+    advance_time(st, dt, nsteps);
+    return LG_OK;
+}
+
+int lg_modelc_initialize_grains(lg_state* st, const double* grains, int64_t n, double u0) {
+    if (!st || (n > 0 && !grains)) return LG_ERR_INVALID;
+    lg_ctx* ctx = st->ctx;
+    const lg_grid* g = st->grid;
+    if (g->D != 2 || st->nfields < 2 || st->ghosts[0] != 1 || st->ghosts[1] != 1)
+        return fail(ctx, LG_ERR_STATE, "Model C needs a 2-D state with phi and u of ghost width 1");
+    const int64_t nx = g->block[0], ny = g->block[1];
+    const int64_t len = block_len(g, 1), sy = nx + 2;
+    std::vector<double> phi(len * g->nblocks, 0.0), u(len * g->nblocks, 0.0);
+    auto center = [&](int64_t b, int64_t i, int64_t j, double* out) {
+        // CartesianGrid::cell_center (cartesian.rs:588-597)
+        int64_t c0 = b % g->nb[0], c1 = b / g->nb[0];
+        out[0] = std::fma(((double)(c0 * nx) + (double)i) + 0.5, g->spacing[0], g->origin[0]);
+        out[1] = std::fma(((double)(c1 * ny) + (double)j) + 0.5, g->spacing[1], g->origin[1]);
+    };
+    const double CUTOFF = 27.0;
+    auto work = [&](int64_t b0, int64_t b1) {
+        for (int64_t b = b0; b < b1; ++b) {
+            // ModelC::initialize_grains (phasefield.rs:238-286)
+            double hx = g->spacing[0], hy = g->spacing[1], c0[2], c1[2];
+            center(b, 0, 0, c0);
+            center(b, nx - 1, ny - 1, c1);
+            double lo[2] = {std::fma(0.5, -hx, c0[0]), std::fma(0.5, -hy, c0[1])};
+            double hi[2] = {std::fma(0.5, hx, c1[0]), std::fma(0.5, hy, c1[1])};
+            std::vector<int64_t> near;
+            for (int64_t k = 0; k < n; ++k) {
+                double cx = grains[4 * k], cy = grains[4 * k + 1];
+                double dx = std::max(std::max(lo[0] - cx, cx - hi[0]), 0.0);
+                double dy = std::max(std::max(lo[1] - cy, cy - hi[1]), 0.0);
+                if (std::hypot(dx, dy) <= grains[4 * k + 2] + CUTOFF) near.push_back(k);
+            }
+            double* ph = phi.data() + b * len;
+            double* uu = u.data() + b * len;
+            for (int64_t j = 0; j < ny; ++j)
+                for (int64_t i = 0; i < nx; ++i) {
+                    double v = -1.0;
+                    if (!near.empty()) {
+                        double xy[2];
+                        center(b, i, j, xy);
+                        for (int64_t k : near) {
+                            double r = std::hypot(xy[0] - grains[4 * k], xy[1] - grains[4 * k + 1]);
+                            v = std::fmax(v, -std::tanh((r - grains[4 * k + 2]) / std::sqrt(2.0)));
+                        }
+                    }
+                    ph[(i + 1) + (j + 1) * sy] = v;
+                    uu[(i + 1) + (j + 1) * sy] = -u0;
+                }
+        }
+    };
+    unsigned nt = std::max(1u, std::min(64u, std::thread::hardware_concurrency()));
+    if (g->nblocks < 4) nt = 1;
+    std::vector<std::thread> pool;
+    int64_t per = (g->nblocks + nt - 1) / nt;
+    for (unsigned k = 0; k < nt; ++k) {
+        int64_t b0 = k * per, b1 = std::min<int64_t>(g->nblocks, b0 + per);
+        if (b0 < b1) pool.emplace_back(work, b0, b1);
+    }
+    for (auto& th : pool) th.join();
+    int rc = lg_state_upload_field(st, 0, phi.data(), (int64_t)phi.size());
+    if (rc != LG_OK) return rc;
+    return lg_state_upload_field(st, 1, u.data(), (int64_t)u.size());
+}
+
+int lg_heat_initialize_sine_noise(lg_state* st, int field, uint64_t seed, double amp) {
+    if (!st) return LG_ERR_INVALID;
+    lg_ctx* ctx = st->ctx;
+    const lg_grid* g = st->grid;
+    if (st->dtype != LG_F64 || field < 0 || field >= st->nfields)
+        return fail(ctx, LG_ERR_STATE, "heat initial condition needs an FP64 field");
+    const int gh = st->ghosts[field];
+    const int64_t len = block_len(g, gh);
+    std::vector<double> host(len * g->nblocks, 0.0);
+    const double two_pi = 2.0 * 3.14159265358979323846;
+    for (int64_t b = 0; b < g->nblocks; ++b) {
+        int64_t c[3] = {0, 0, 0}, rem = b;
+        for (int d = 0; d < g->D; ++d) {
+            c[d] = rem % g->nb[d];
+            rem /= g->nb[d];
+        }
+        int64_t n[3] = {g->block[0], g->D > 1 ? g->block[1] : 1, g->D > 2 ? g->block[2] : 1};
+        for (int64_t k = 0; k < n[2]; ++k)
+            for (int64_t j = 0; j < n[1]; ++j)
+                for (int64_t i = 0; i < n[0]; ++i) {
+                    int64_t idx[3] = {i, j, k};
+                    uint64_t parts_key = lg::splitmix64(seed);
+                    double s = 1.0;
+                    int64_t off = 0, stride = 1;
+                    for (int d = 0; d < g->D; ++d) {
+                        int64_t global = c[d] * g->block[d] + idx[d];
+                        double x = std::fma(((double)(c[d] * g->block[d]) + (double)idx[d]) + 0.5, g->spacing[d],
+                                            g->origin[d]);
+                        s = s * std::sin(two_pi * x);
+                        parts_key = lg::splitmix64(parts_key ^ (uint64_t)global);
+                        off += (idx[d] + gh) * stride;
+                        stride *= g->block[d] + 2 * gh;
+                    }
+                    host[b * len + off] = s + amp * (2.0 * lg::unit_open(parts_key) - 1.0);
+                }
+    }
+    return lg_state_upload_field(st, field, host.data(), (int64_t)host.size());
+}
+
+int lg_standard_normal(lg_ctx* ctx, const uint64_t* keys, int64_t n, double* out) {
+    if (!ctx || n < 0 || (n > 0 && (!keys || !out))) return fail(ctx, LG_ERR_INVALID, "bad arguments");
+    if (n == 0) return LG_OK;
+    cudaSetDevice(ctx->device);
+    uint64_t* dk = nullptr;
+    double* dout = nullptr;
+    LG_CUDA(ctx, cudaMalloc(&dk, n * sizeof(uint64_t)));
+    cudaError_t e = cudaMalloc(&dout, n * sizeof(double));
+    if (e != cudaSuccess) {
+        cudaFree(dk);
+        return cuda_fail(ctx, e, "cudaMalloc");
+    }
+    e = cudaMemcpyAsync(dk, keys, n * sizeof(uint64_t), cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess) {
+        e = lg::launch_standard_normal(dk, dout, n, ctx->stream);
+        ctx->launches++;
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out, dout, n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    cudaFree(dk);
+    cudaFree(dout);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "standard normal");
+    return LG_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,395 @@
+// Halo fill, heat and Model C step kernels of the legendre B200 library.
+//
+// This translation unit is compiled with -fmad=false: the reference is Rust,
+// which never contracts a*b+c into a fused multiply-add, so every product
+// and sum below rounds separately and `fma` appears exactly where the
+// reference calls `f64::mul_add`.  That is what makes the FP64 path
+// bit-identical to the reference's SerialScheduler.
+#include <cmath>
+#include <cstdio>
+
+#include "lg_common.cuh"
+#include "lg_kernels.h"
+
+namespace lg {
+namespace {
+
+__device__ __forceinline__ int64_t slab_base(const SlabLayout& L, int b, int field) {
+    return ((int64_t)b * L.nfields + field) * L.slab_stride;
+}
+
+// Offset of interior-relative index l inside a ghost-inclusive slab
+// (cartesian.rs:189-204).
+template <int D>
+__device__ __forceinline__ int64_t lin(const SlabLayout& L, const int* l) {
+    int64_t o = l[0] + L.ghost;
+    if (D > 1) o += (int64_t)(l[1] + L.ghost) * L.gdim[0];
+    if (D > 2) o += (int64_t)(l[2] + L.ghost) * L.gdim[0] * L.gdim[1];
+    return o;
+}
+
+// Write the value of interior cell `l` of block `b` into every ghost entry
+// whose source it is.  The reference fills ghosts by a dimension sweep
+// (cartesian.rs:439-526); its result is separable per dimension -- ghost
+// (x, y, ...) holds the interior value at (map_0(x), map_1(y), ...), each
+// map being the identity inside the block, the face neighbour's interior
+// (wrapped in periodic dimensions) or the mirror image at a physical
+// boundary.  Pushing along the pre-images of that map writes every ghost
+// entry exactly once, with no ordering between blocks.
+template <int D, class T>
+__device__ __forceinline__ void push_ghost_images(T* __restrict__ arena, const CartTopo& topo,
+                                                  const SlabLayout& L, int field, int b, const int* l, T val) {
+    const int g = L.ghost;
+    int step[D][3], cl[D][3], nc[D];
+    bool any = false;
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+        const int n = topo.n[d];
+        nc[d] = 1;
+        step[d][0] = 0;
+        cl[d][0] = l[d];
+        if (l[d] < g) {
+            int nb = topo.nbr[(b * 3 + d) * 2 + 0];
+            step[d][nc[d]] = nb >= 0 ? -1 : 0;
+            cl[d][nc[d]] = nb >= 0 ? n + l[d] : -1 - l[d];
+            ++nc[d];
+            any = true;
+        }
+        if (l[d] >= n - g) {
+            int nb = topo.nbr[(b * 3 + d) * 2 + 1];
+            step[d][nc[d]] = nb >= 0 ? 1 : 0;
+            cl[d][nc[d]] = nb >= 0 ? l[d] - n : 2 * n - 1 - l[d];
+            ++nc[d];
+            any = true;
+        }
+    }
+    if (!any) return;
+    int c[3] = {0, 0, 0};
+    for (;;) {
+        // advance the mixed-radix counter; the all-zero combination is the
+        // cell itself and is skipped
+        int d = 0;
+        while (d < D) {
+            if (++c[d] < nc[d]) break;
+            c[d] = 0;
+            ++d;
+        }
+        if (d == D) break;
+        int blk = b;
+        int tl[3] = {0, 0, 0};
+#pragma unroll
+        for (int e = 0; e < D; ++e) {
+            int st = step[e][c[e]];
+            if (st != 0) blk = topo.nbr[(blk * 3 + e) * 2 + (st > 0 ? 1 : 0)];
+            tl[e] = cl[e][c[e]];
+        }
+        arena[slab_base(L, blk, field) + lin<D>(L, tl)] = val;
+    }
+}
+
+// ------------------------------------------------------------- halo (b) --
+struct RingShape {
+    int64_t strip[LG_MAX_DIM];  // cells in one strip normal to dimension d
+    int64_t total;              // all ring cells of one block
+};
+
+// One thread per ghost entry.  Ring cells are enumerated as in the
+// reference's for_each_ring_cell (src/geometry/amr/intergrid.rs:73-86): per
+// dimension d, a low and a high strip of width g, spanning the grown range
+// in earlier dimensions and the interior range in later ones.
+template <class T>
+__global__ void halo_fill_kernel(T* __restrict__ arena, CartTopo topo, SlabLayout L, int field, RingShape rs) {
+    const int g = L.ghost;
+    for (int b = blockIdx.y; b < topo.nblocks; b += gridDim.y)
+    for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < rs.total;
+         r += (int64_t)gridDim.x * blockDim.x) {
+        int64_t rem = r;
+        int d = 0;
+        while (rem >= 2 * rs.strip[d]) {
+            rem -= 2 * rs.strip[d];
+            ++d;
+        }
+        const int side = rem >= rs.strip[d] ? 1 : 0;
+        int64_t pos = rem - side * rs.strip[d];
+        int idx[3] = {0, 0, 0};
+        for (int e = 0; e < topo.D; ++e) {
+            int64_t ext = e < d ? topo.n[e] + 2 * g : (e == d ? g : topo.n[e]);
+            int p = (int)(pos % ext);
+            pos /= ext;
+            if (e < d) idx[e] = p - g;
+            else if (e == d) idx[e] = side ? topo.n[e] + p : p - g;
+            else idx[e] = p;
+        }
+        // source of this ghost entry, dimension by dimension
+        int src = b;
+        int sl[3] = {idx[0], idx[1], idx[2]};
+        for (int e = 0; e < topo.D; ++e) {
+            const int n = topo.n[e];
+            if (idx[e] < 0) {
+                int nb = topo.nbr[(src * 3 + e) * 2 + 0];
+                if (nb >= 0) { src = nb; sl[e] = n + idx[e]; }
+                else sl[e] = -1 - idx[e];
+            } else if (idx[e] >= n) {
+                int nb = topo.nbr[(src * 3 + e) * 2 + 1];
+                if (nb >= 0) { src = nb; sl[e] = idx[e] - n; }
+                else sl[e] = 2 * n - 1 - idx[e];
+            }
+        }
+        int64_t to = idx[0] + g, so = sl[0] + g, stride = L.gdim[0];
+        for (int e = 1; e < topo.D; ++e) {
+            to += (int64_t)(idx[e] + g) * stride;
+            so += (int64_t)(sl[e] + g) * stride;
+            stride *= L.gdim[e];
+        }
+        arena[slab_base(L, b, field) + to] = arena[slab_base(L, src, field) + so];
+    }
+}
+
+// ------------------------------------------------------------- heat (d) --
+// Heat<D>::vector_field_block (examples/heat3d.rs:63-79): the central
+// Laplacian (finite_difference.rs:49-67) times kappa, then ForwardEuler's
+// axpy (integrators/euler.rs:51-53).  One thread per interior cell.
+template <int D>
+__global__ void __launch_bounds__(256) heat_step_kernel(const double* __restrict__ in, double* __restrict__ out,
+                                                        CartTopo topo, SlabLayout L, int field, double kappa,
+                                                        double dt, double ih0, double ih1, double ih2) {
+    const int64_t cells = (int64_t)topo.n[0] * (D > 1 ? topo.n[1] : 1) * (D > 2 ? topo.n[2] : 1);
+    const int64_t st1 = L.gdim[0];
+    const int64_t st2 = (int64_t)L.gdim[0] * (D > 1 ? L.gdim[1] : 1);
+    for (int b = blockIdx.y; b < topo.nblocks; b += gridDim.y) {
+    const double* s = in + slab_base(L, b, field);
+    double* o_slab = out + slab_base(L, b, field);
+    for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < cells;
+         c += (int64_t)gridDim.x * blockDim.x) {
+        int l[3] = {0, 0, 0};
+        int64_t rem = c;
+        l[0] = (int)(rem % topo.n[0]);
+        rem /= topo.n[0];
+        if (D > 1) { l[1] = (int)(rem % topo.n[1]); rem /= topo.n[1]; }
+        if (D > 2) l[2] = (int)rem;
+        const int64_t o = lin<D>(L, l);
+        const double center = s[o];
+        double acc = 0.0;
+        acc += ((s[o + 1] - (center + center)) + s[o - 1]) * ih0;
+        if (D > 1) acc += ((s[o + st1] - (center + center)) + s[o - st1]) * ih1;
+        if (D > 2) acc += ((s[o + st2] - (center + center)) + s[o - st2]) * ih2;
+        const double k = acc * kappa;
+        const double v = center + dt * k;
+        o_slab[o] = v;
+        push_ghost_images<D, double>(out, topo, L, field, b, l, v);
+    }
+    }
+}
+
+// ----------------------------------------------------------- Model C (a) --
+template <class T>
+struct MC {
+    T lambda, d_thermal, a_bar, eps_prime, tol, f_a_bar, f_eps_prime, f_a12, f_tol, inv_h2_flux, ih0, ih1;
+};
+
+template <class T>
+MC<T> to_mc(const ModelCDev& m) {
+    MC<T> r;
+    r.lambda = (T)m.lambda;
+    r.d_thermal = (T)m.d_thermal;
+    r.a_bar = (T)m.a_bar;
+    r.eps_prime = (T)m.eps_prime;
+    r.tol = (T)m.tol;
+    r.f_a_bar = (T)m.f_a_bar;
+    r.f_eps_prime = (T)m.f_eps_prime;
+    r.f_a12 = (T)m.f_a12;
+    r.f_tol = (T)m.f_tol;
+    r.inv_h2_flux = (T)m.inv_h2_flux;
+    r.ih0 = (T)m.inv_h2[0];
+    r.ih1 = (T)m.inv_h2[1];
+    return r;
+}
+
+// KarmaRappelFlux::face (finite_volume.rs:129-142)
+template <class T>
+__device__ __forceinline__ void kr_face(const MC<T>& m, T dx, T dy, T& a, T& da) {
+    T dx2 = dx * dx;
+    T dy2 = dy * dy;
+    T sum = dx2 + dy2;
+    T mag2 = sum * sum;
+    if (mag2 <= m.f_tol) {
+        a = m.f_a_bar;
+        da = T(0);
+    } else {
+        a = m.f_a_bar * (T(1) + m.f_eps_prime * (dx2 * dx2 + dy2 * dy2) / mag2);
+        da = -(m.f_a12) * dx * dy * (dx2 - dy2) / mag2;
+    }
+}
+
+__device__ __forceinline__ double fma_t(double a, double b, double c) { return fma(a, b, c); }
+__device__ __forceinline__ float fma_t(float a, float b, float c) { return fmaf(a, b, c); }
+
+__device__ __forceinline__ double normal_t(uint64_t key, double) { return standard_normal(key); }
+__device__ __forceinline__ float normal_t(uint64_t key, float) { return standard_normal_f32(key); }
+
+// Reference-order Model C step, one thread per interior cell: the flux
+// kernel (finite_volume.rs:258-283), the local terms (phasefield.rs:395-404),
+// the u Laplacian and coupling (phasefield.rs:412-421), the Time driver
+// axpy (driver.rs:210-216) and the Wiener increment (driver.rs:218-236).
+template <class T>
+__global__ void __launch_bounds__(256) modelc_step_ref_kernel(const T* __restrict__ in, T* __restrict__ out,
+                                                              CartTopo topo, SlabLayout L, MC<T> m, T dt,
+                                                              double dt64, NoiseDev nz, T scale_amp, double* tdev,
+                                                              int slot) {
+    const int n0 = topo.n[0], n1 = topo.n[1];
+    const int64_t sy = L.gdim[0];
+    // Simulation::t lives on the device in two slots: this step reads
+    // tdev[slot] (its bits are the Wiener salt, euler_maruyama.rs:128) and
+    // writes t + dt to the other slot (simulation.rs:285), so a captured
+    // sequence of steps needs no host-side time.
+    const double t = tdev[slot];
+    if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) tdev[slot ^ 1] = t + dt64;
+    for (int b = blockIdx.y; b < topo.nblocks; b += gridDim.y) {
+    const T* ph = in + slab_base(L, b, 0);
+    const T* uu = in + slab_base(L, b, 1);
+    T* phi_out = out + slab_base(L, b, 0);
+    T* u_out = out + slab_base(L, b, 1);
+    uint64_t block_key = 0;
+    if (nz.on) block_key = wiener_block_key(nz.seed, (uint64_t)__double_as_longlong(t), kWienerStream0, (uint64_t)b);
+    const T quarter = T(0.25), half = T(0.5);
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n0 * n1; c += gridDim.x * blockDim.x) {
+        const int i = c % n0, j = c / n0;
+        const int64_t o = (int64_t)(i + 1) + (int64_t)(j + 1) * sy;
+        auto P = [&](int di, int dj) { return ph[o + di + dj * sy]; };
+        T derx_r = P(1, 0) - P(0, 0);
+        T derx_l = P(0, 0) - P(-1, 0);
+        T derx_t = quarter * (P(1, 1) - P(-1, 1) + P(1, 0) - P(-1, 0));
+        T derx_b = quarter * (P(1, 0) - P(-1, 0) + P(1, -1) - P(-1, -1));
+        T dery_t = P(0, 1) - P(0, 0);
+        T dery_b = P(0, 0) - P(0, -1);
+        T dery_r = quarter * (P(1, 1) - P(1, -1) + P(0, 1) - P(0, -1));
+        T dery_l = quarter * (P(0, 1) - P(0, -1) + P(-1, 1) - P(-1, -1));
+        T a_r, da_r, a_l, da_l, a_t, da_t, a_b, da_b;
+        kr_face(m, derx_r, dery_r, a_r, da_r);
+        kr_face(m, derx_l, dery_l, a_l, da_l);
+        kr_face(m, derx_t, dery_t, a_t, da_t);
+        kr_face(m, derx_b, dery_b, a_b, da_b);
+        T j_r = a_r * (a_r * derx_r - da_r * dery_r);
+        T j_l = a_l * (a_l * derx_l - da_l * dery_l);
+        T j_t = a_t * (a_t * dery_t + da_t * derx_t);
+        T j_b = a_b * (a_b * dery_b + da_b * derx_b);
+        T flux = (j_r - j_l + j_t - j_b) * m.inv_h2_flux;
+
+        T p = P(0, 0);
+        T g_prime = fma_t(p * p, p, -p);
+        T one_m_p2 = fma_t(p, -p, T(1));
+        T p_prime = one_m_p2 * one_m_p2;
+        // center_anisotropy (phasefield.rs:159-175)
+        T cdx = half * (P(1, 0) - P(-1, 0));
+        T cdy = half * (P(0, 1) - P(0, -1));
+        T cdx2 = cdx * cdx;
+        T cdy2 = cdy * cdy;
+        T csum = cdx2 + cdy2;
+        T cmag2 = csum * csum;
+        T a = cmag2 <= m.tol ? m.a_bar : m.a_bar * (T(1) + m.eps_prime * (cdx2 * cdx2 + cdy2 * cdy2) / cmag2);
+        T uc = uu[o];
+        T kphi = fma_t(m.lambda * uc, -p_prime, flux - g_prime) / (a * a);
+
+        T acc = T(0);
+        acc += ((uu[o + 1] - (uc + uc)) + uu[o - 1]) * m.ih0;
+        acc += ((uu[o + sy] - (uc + uc)) + uu[o - sy]) * m.ih1;
+        T ku = fma_t(acc, m.d_thermal, half * kphi);
+
+        T phin = p + dt * kphi;
+        if (nz.on) {
+            uint64_t key = splitmix64(block_key ^ (uint64_t)(i + j * n0));
+            phin += scale_amp * normal_t(key, T(0));
+        }
+        T un = uc + dt * ku;
+        phi_out[o] = phin;
+        u_out[o] = un;
+        int l[2] = {i, j};
+        push_ghost_images<2, T>(out, topo, L, 0, b, l, phin);
+        push_ghost_images<2, T>(out, topo, L, 1, b, l, un);
+    }
+    }
+}
+
+__global__ void standard_normal_kernel(const uint64_t* keys, double* out, int64_t n) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = standard_normal(keys[i]);
+}
+
+int grid_x_for(int64_t cells, int threads) {
+    int64_t gx = (cells + threads - 1) / threads;
+    return (int)(gx < 1 ? 1 : (gx > 65535 ? 65535 : gx));
+}
+
+int grid_y_for(int nblocks) { return nblocks < 1 ? 1 : (nblocks > 65535 ? 65535 : nblocks); }
+
+}  // namespace
+
+cudaError_t launch_halo_fill(void* arena, int elem_size, const CartTopo& topo, const SlabLayout& L, int field,
+                             cudaStream_t s) {
+    if (L.ghost == 0) return cudaSuccess;
+    RingShape rs{};
+    rs.total = 0;
+    for (int d = 0; d < topo.D; ++d) {
+        int64_t c = L.ghost;
+        for (int e = 0; e < topo.D; ++e) {
+            if (e < d) c *= topo.n[e] + 2 * L.ghost;
+            else if (e > d) c *= topo.n[e];
+        }
+        rs.strip[d] = c;
+        rs.total += 2 * c;
+    }
+    dim3 grid(grid_x_for(rs.total, 256), grid_y_for(topo.nblocks));
+    if (elem_size == 8)
+        halo_fill_kernel<double><<<grid, 256, 0, s>>>(static_cast<double*>(arena), topo, L, field, rs);
+    else
+        halo_fill_kernel<float><<<grid, 256, 0, s>>>(static_cast<float*>(arena), topo, L, field, rs);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_heat_step(const double* in, double* out, const CartTopo& topo, const SlabLayout& L, int field,
+                             double kappa, double dt, const double inv_h2[3], cudaStream_t s) {
+    int64_t cells = 1;
+    for (int d = 0; d < topo.D; ++d) cells *= topo.n[d];
+    dim3 grid(grid_x_for(cells, 256), grid_y_for(topo.nblocks));
+    switch (topo.D) {
+        case 1:
+            heat_step_kernel<1><<<grid, 256, 0, s>>>(in, out, topo, L, field, kappa, dt, inv_h2[0], 0.0, 0.0);
+            break;
+        case 2:
+            heat_step_kernel<2><<<grid, 256, 0, s>>>(in, out, topo, L, field, kappa, dt, inv_h2[0], inv_h2[1], 0.0);
+            break;
+        default:
+            heat_step_kernel<3><<<grid, 256, 0, s>>>(in, out, topo, L, field, kappa, dt, inv_h2[0], inv_h2[1],
+                                                     inv_h2[2]);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_modelc_step_f64(const double* in, double* out, const CartTopo& topo, const SlabLayout& L,
+                                   const ModelCDev& m, double dt, const NoiseDev& nz, double* tdev, int slot,
+                                   int variant, cudaStream_t s) {
+    (void)variant;
+    dim3 grid(grid_x_for((int64_t)topo.n[0] * topo.n[1], 256), grid_y_for(topo.nblocks));
+    double scale_amp = std::sqrt(dt) * nz.amp;
+    modelc_step_ref_kernel<double><<<grid, 256, 0, s>>>(in, out, topo, L, to_mc<double>(m), dt, dt, nz, scale_amp,
+                                                        tdev, slot);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_modelc_step_f32(const float* in, float* out, const CartTopo& topo, const SlabLayout& L,
+                                   const ModelCDev& m, double dt, const NoiseDev& nz, double* tdev, int slot,
+                                   int variant, cudaStream_t s) {
+    (void)variant;
+    dim3 grid(grid_x_for((int64_t)topo.n[0] * topo.n[1], 256), grid_y_for(topo.nblocks));
+    float scale_amp = (float)std::sqrt(dt) * (float)nz.amp;
+    modelc_step_ref_kernel<float><<<grid, 256, 0, s>>>(in, out, topo, L, to_mc<float>(m), (float)dt, dt, nz,
+                                                       scale_amp, tdev, slot);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_standard_normal(const uint64_t* keys, double* out, int64_t n, cudaStream_t s) {
+    standard_normal_kernel<<<grid_x_for(n, 256), 256, 0, s>>>(keys, out, n);
+    return cudaGetLastError();
+}
+
+}  // namespace lg

@@ -1,0 +1,55 @@
+// Launchers of the legendre B200 kernels (host side, C++ linkage).  Each
+// returns the cudaError_t of its launch; the C-ABI layer turns that into a
+// status code and an error string.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "lg_common.cuh"
+
+namespace lg {
+
+// Model C parameters as the kernels consume them (derived constants are
+// computed on the host exactly as the reference derives them).
+struct ModelCDev {
+    double lambda, d_thermal;
+    double a_bar, eps_prime, tol;                 // ModelC (phasefield.rs:100-116)
+    double f_a_bar, f_eps_prime, f_a12, f_tol;    // KarmaRappelFlux (finite_volume.rs:113-122)
+    double inv_h2_flux;                           // 1/(hx*hy)   (finite_volume.rs:254)
+    double inv_h2[2];                             // 1/(h_d*h_d) (finite_difference.rs:371)
+};
+
+struct NoiseDev {
+    int on;               // Wiener<1> with a non-zero amplitude
+    uint64_t seed;
+    double amp;           // noise amplitude b (the Wiener amplitude field)
+};
+
+// (b) ghost fill of one field (pull form): every ghost entry of every block
+// copies its source interior entry (exchange, periodic wrap or mirror).
+cudaError_t launch_halo_fill(void* arena, int elem_size, const CartTopo& topo, const SlabLayout& L, int field,
+                             cudaStream_t s);
+
+// (d) forward-Euler heat step: out = in + dt * (kappa * lap(in)) on the
+// interiors, plus the ghost ring of `out` filled from the new interiors.
+cudaError_t launch_heat_step(const double* in, double* out, const CartTopo& topo, const SlabLayout& L, int field,
+                             double kappa, double dt, const double inv_h2[3], cudaStream_t s);
+
+// (a) fused Model C Euler-Maruyama step, FP64, bit-exact to the reference.
+// Reads phi (field 0) and u (field 1) from `in`, writes both to `out` with
+// ghosts filled.  `tdev[slot]` holds the step's time (its bits are the noise
+// salt); block 0 writes tdev[slot ^ 1] = t + dt.
+cudaError_t launch_modelc_step_f64(const double* in, double* out, const CartTopo& topo, const SlabLayout& L,
+                                   const ModelCDev& m, double dt, const NoiseDev& nz, double* tdev, int slot,
+                                   int variant, cudaStream_t s);
+
+// FP32 storage and arithmetic variant of the same step.
+cudaError_t launch_modelc_step_f32(const float* in, float* out, const CartTopo& topo, const SlabLayout& L,
+                                   const ModelCDev& m, double dt, const NoiseDev& nz, double* tdev, int slot,
+                                   int variant, cudaStream_t s);
+
+// Standard normals of a key array (tests of the generator).
+cudaError_t launch_standard_normal(const uint64_t* keys, double* out, int64_t n, cudaStream_t s);
+
+}  // namespace lg

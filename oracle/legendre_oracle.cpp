@@ -1,0 +1,594 @@
+// legendre oracle -- TEST INFRASTRUCTURE, NOT PRODUCT CODE.
+//
+// A serial CPU restatement of the reference's `SerialScheduler` path for the
+// block-stepping hot path (trbritt/legendre 0.1.4, Rust).  It exists only to
+// check the CUDA library: the tests, `__graft_entry__.smoke()` and the CPU
+// baseline leg of `bench.py` may call it; nothing in the product links it.
+//
+// Bit-exactness rules (the reference is Rust, which never contracts a*b+c):
+//   * compiled with -ffp-contract=off,
+//   * std::fma exactly where the reference calls `f64::mul_add`,
+//   * the reference's operand order, left-to-right evaluation of a-b+c-d,
+//   * glibc log/cos/sqrt/tanh/hypot (what Rust's f64 methods call on
+//     linux-gnu).
+// Each function names the reference file:line it restates.
+//
+// OpenMP (optional `nthreads`) parallelises only the per-block dispatches,
+// mirroring `RayonScheduler` (src/core/scheduler.rs:65-84): blocks are
+// disjoint, so results are identical for every thread count.
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <vector>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#include "legendre_oracle.h"
+
+namespace {
+
+// ---------------------------------------------------------------- rng ------
+// src/util/rng.rs:13-18
+inline uint64_t splitmix64(uint64_t z) {
+    z += 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+// src/util/rng.rs:23-29
+inline uint64_t mix_key(uint64_t seed, const uint64_t* parts, size_t n) {
+    uint64_t s = splitmix64(seed);
+    for (size_t i = 0; i < n; ++i) s = splitmix64(s ^ parts[i]);
+    return s;
+}
+// src/util/rng.rs:35-37
+inline double unit_open(uint64_t bits) {
+    return (double)((bits >> 11) + 1) * (1.0 / 9007199254740992.0);
+}
+// std::f64::consts::TAU
+constexpr double kTau = 6.283185307179586476925286766559;
+// src/util/rng.rs:43-49
+inline double standard_normal(uint64_t key) {
+    uint64_t a = splitmix64(key);
+    uint64_t b = splitmix64(a ^ 0xD1B54A32D192ED03ull);
+    double u = unit_open(a);
+    double v = unit_open(b);
+    return std::sqrt(-2.0 * std::log(u)) * std::cos(kTau * v);
+}
+
+// --------------------------------------------------------- Cartesian ------
+// src/geometry/cartesian.rs:28-187
+struct Grid {
+    int D;
+    int64_t cells[3], block[3], nb[3];
+    double origin[3], spacing[3];
+    bool periodic[3];
+
+    int64_t num_blocks() const {
+        int64_t n = 1;
+        for (int d = 0; d < D; ++d) n *= nb[d];
+        return n;
+    }
+    int64_t ghosted(int d, int g) const { return block[d] + 2 * g; }
+    int64_t block_len(int g) const {
+        int64_t n = 1;
+        for (int d = 0; d < D; ++d) n *= ghosted(d, g);
+        return n;
+    }
+    // cartesian.rs:145-154
+    void block_coords(int64_t b, int64_t* out) const {
+        int64_t rem = b;
+        for (int d = 0; d < D; ++d) { out[d] = rem % nb[d]; rem /= nb[d]; }
+    }
+    // cartesian.rs:162-181 ; -1 for a non-periodic domain boundary
+    int64_t face_neighbor(int64_t b, int dim, int dir) const {
+        int64_t c[3];
+        block_coords(b, c);
+        int64_t stepped = c[dim] + (dir < 0 ? -1 : 1);
+        int64_t next;
+        if (stepped >= 0 && stepped < nb[dim]) next = stepped;
+        else if (periodic[dim]) next = ((stepped % nb[dim]) + nb[dim]) % nb[dim];
+        else return -1;
+        int64_t id = 0, stride = 1;
+        for (int d = 0; d < D; ++d) {
+            id += (d == dim ? next : c[d]) * stride;
+            stride *= nb[d];
+        }
+        return id;
+    }
+    // cartesian.rs:189-204
+    int64_t linearize(const int64_t* idx, int g) const {
+        int64_t off = 0, stride = 1;
+        for (int d = 0; d < D; ++d) {
+            off += (idx[d] + g) * stride;
+            stride *= block[d] + 2 * g;
+        }
+        return off;
+    }
+    // cartesian.rs:588-597
+    void cell_center(int64_t b, const int64_t* idx, double* out) const {
+        int64_t c[3];
+        block_coords(b, c);
+        for (int d = 0; d < D; ++d) {
+            int64_t global = c[d] * block[d];
+            out[d] = std::fma(((double)global + (double)idx[d]) + 0.5, spacing[d], origin[d]);
+        }
+    }
+    // cartesian.rs:599-619 ; returns false for a ghost entry
+    bool cell_key(int g, int64_t offset, uint64_t* key) const {
+        int64_t rem = offset, k = 0, stride = 1;
+        for (int d = 0; d < D; ++d) {
+            int64_t gh = block[d] + 2 * g;
+            int64_t c = rem % gh;
+            rem /= gh;
+            if (c < g || c >= block[d] + g) return false;
+            k += (c - g) * stride;
+            stride *= block[d];
+        }
+        *key = (uint64_t)k;
+        return true;
+    }
+};
+
+// Visit every index of the half-open box lo..hi, dimension 0 fastest
+// (cartesian.rs:338-358).
+template <class F>
+void for_each_box(int D, const int64_t* lo, const int64_t* hi, F f) {
+    for (int d = 0; d < D; ++d)
+        if (lo[d] >= hi[d]) return;
+    int64_t idx[3] = {lo[0], D > 1 ? lo[1] : 0, D > 2 ? lo[2] : 0};
+    for (;;) {
+        f(idx);
+        int d = 0;
+        for (;;) {
+            idx[d] += 1;
+            if (idx[d] < hi[d]) break;
+            idx[d] = lo[d];
+            if (++d == D) return;
+        }
+    }
+}
+
+template <class F>
+void for_each_interior(const Grid& g, F f) {
+    int64_t lo[3] = {0, 0, 0};
+    for_each_box(g.D, lo, g.block, f);
+}
+
+// Block-major state: blocks x fields, each slab ghost-inclusive
+// (src/core/state.rs:219-296).  A zero-length slab marks a field the buffer
+// does not carry (state.rs:237-264).
+struct State {
+    std::vector<int> ghost;
+    std::vector<std::vector<std::vector<double>>> slab;  // [block][field]
+};
+
+State make_state(const Grid& g, const std::vector<int>& ghosts, const std::vector<bool>& keep) {
+    State s;
+    s.ghost = ghosts;
+    s.slab.resize(g.num_blocks());
+    for (auto& b : s.slab) {
+        b.resize(ghosts.size());
+        for (size_t f = 0; f < ghosts.size(); ++f)
+            if (keep[f]) b[f].assign(g.block_len(ghosts[f]), 0.0);
+    }
+    return s;
+}
+
+// cartesian.rs:439-526 with FaceBc::Mirror (boundary.rs:63-66)
+void fill_ghosts_mirror(const Grid& grid, State& st, int f) {
+    int g = st.ghost[f];
+    if (g == 0) return;
+    const int D = grid.D;
+    for (int d = 0; d < D; ++d) {
+        int64_t n = grid.block[d];
+        int64_t lo[3], hi[3];
+        for (int e = 0; e < D; ++e) { lo[e] = -g; hi[e] = grid.block[e] + g; }
+        for (int64_t b = 0; b < grid.num_blocks(); ++b) {
+            for (int dir : {-1, 1}) {
+                if (dir < 0) { lo[d] = -g; hi[d] = 0; }
+                else { lo[d] = n; hi[d] = n + g; }
+                int64_t nbk = grid.face_neighbor(b, d, dir);
+                std::vector<double>& dst = st.slab[b][f];
+                if (nbk == b) {
+                    for_each_box(D, lo, hi, [&](const int64_t* idx) {
+                        int64_t s[3] = {idx[0], idx[1], idx[2]};
+                        s[d] = dir < 0 ? n + idx[d] : idx[d] - n;
+                        dst[grid.linearize(idx, g)] = dst[grid.linearize(s, g)];
+                    });
+                } else if (nbk >= 0) {
+                    const std::vector<double>& src = st.slab[nbk][f];
+                    for_each_box(D, lo, hi, [&](const int64_t* idx) {
+                        int64_t s[3] = {idx[0], idx[1], idx[2]};
+                        s[d] = dir < 0 ? n + idx[d] : idx[d] - n;
+                        dst[grid.linearize(idx, g)] = src[grid.linearize(s, g)];
+                    });
+                } else {
+                    for_each_box(D, lo, hi, [&](const int64_t* idx) {
+                        int64_t layer = dir < 0 ? -1 - idx[d] : idx[d] - n;
+                        int64_t s[3] = {idx[0], idx[1], idx[2]};
+                        s[d] = dir < 0 ? layer : n - 1 - layer;  // Mirror: interior(k)
+                        dst[grid.linearize(idx, g)] = dst[grid.linearize(s, g)];
+                    });
+                }
+            }
+        }
+    }
+}
+
+// src/discretization/finite_difference.rs:49-67 ; output interior only
+void central_laplacian(const Grid& grid, const std::vector<double>& in, std::vector<double>& out, int g) {
+    double inv_h2[3];
+    for (int d = 0; d < grid.D; ++d) inv_h2[d] = 1.0 / (grid.spacing[d] * grid.spacing[d]);
+    for_each_interior(grid, [&](const int64_t* idx) {
+        double center = in[grid.linearize(idx, g)];
+        double acc = 0.0;
+        for (int d = 0; d < grid.D; ++d) {
+            int64_t p[3] = {idx[0], idx[1], idx[2]}, m[3] = {idx[0], idx[1], idx[2]};
+            p[d] += 1;
+            m[d] -= 1;
+            acc += ((in[grid.linearize(p, g)] - (center + center)) + in[grid.linearize(m, g)]) * inv_h2[d];
+        }
+        out[grid.linearize(idx, g)] = acc;
+    });
+}
+
+template <class F>
+void parallel_blocks(int64_t nblocks, int nthreads, F f) {
+#ifdef _OPENMP
+    if (nthreads > 1) {
+#pragma omp parallel for schedule(dynamic, 1) num_threads(nthreads)
+        for (int64_t b = 0; b < nblocks; ++b) f(b);
+        return;
+    }
+#endif
+    (void)nthreads;
+    for (int64_t b = 0; b < nblocks; ++b) f(b);
+}
+
+// ------------------------------------------------------------- heat -------
+// examples/heat3d.rs:41-85 (Heat3 / tests/heat3d.rs Heat<D>): u registered
+// with ghost 1; drift = CentralLaplacian(u) then *= kappa (heat3d.rs:76-78).
+// ForwardEuler::step (src/integrators/euler.rs:51-53): eval_drift, then
+// state.axpy_with(dt, k) over every slab entry (state.rs:485-498).
+double heat_run(const Grid& grid, State& st, int f, double kappa, double t, double dt, int64_t steps,
+                int nthreads) {
+    int g = st.ghost[f];
+    std::vector<std::vector<double>> k(grid.num_blocks(), std::vector<double>(grid.block_len(g), 0.0));
+    for (int64_t s = 0; s < steps; ++s) {
+        fill_ghosts_mirror(grid, st, f);
+        parallel_blocks(grid.num_blocks(), nthreads, [&](int64_t b) {
+            central_laplacian(grid, st.slab[b][f], k[b], g);
+            for_each_interior(grid, [&](const int64_t* idx) {
+                int64_t o = grid.linearize(idx, g);
+                k[b][o] = k[b][o] * kappa;
+            });
+        });
+        parallel_blocks(grid.num_blocks(), nthreads, [&](int64_t b) {
+            std::vector<double>& x = st.slab[b][f];
+            const std::vector<double>& y = k[b];
+            for (size_t i = 0; i < x.size(); ++i) x[i] += dt * y[i];
+        });
+        t += dt;  // src/core/simulation.rs:285
+    }
+    return t;
+}
+
+// ---------------------------------------------------------- Model C -------
+struct ModelC {
+    double eps4, lambda, d_thermal, noise_amplitude, tol;
+    double a_bar, eps_prime;        // model (phasefield.rs:100-116)
+    double f_a_bar, f_eps_prime, f_a12, f_tol;  // flux (finite_volume.rs:113-122)
+};
+
+ModelC make_model(const orc_modelc_params* p) {
+    ModelC m;
+    m.eps4 = p->eps4;
+    m.lambda = p->lambda;
+    m.d_thermal = p->d_thermal;
+    m.noise_amplitude = p->noise_amplitude;
+    m.tol = p->anisotropy_tol;
+    m.a_bar = std::fma(3.0, -m.eps4, 1.0);
+    m.eps_prime = 3.0 * m.eps4 / m.a_bar;
+    m.f_a_bar = std::fma(3.0, -m.eps4, 1.0);
+    m.f_eps_prime = 3.0 * m.eps4 / m.f_a_bar;
+    m.f_a12 = 4.0 * m.f_a_bar * m.f_eps_prime;
+    m.f_tol = p->flux_tol;
+    return m;
+}
+
+// finite_volume.rs:129-142
+inline void kr_face(const ModelC& m, double dx, double dy, double* a, double* da) {
+    double dx2 = dx * dx;
+    double dy2 = dy * dy;
+    double sum = dx2 + dy2;
+    double mag2 = sum * sum;
+    if (mag2 <= m.f_tol) {
+        *a = m.f_a_bar;
+        *da = 0.0;
+    } else {
+        *a = m.f_a_bar * (1.0 + m.f_eps_prime * (dx2 * dx2 + dy2 * dy2) / mag2);
+        *da = -(m.f_a12) * dx * dy * (dx2 - dy2) / mag2;
+    }
+}
+
+// phasefield.rs:159-175
+inline double center_anisotropy(const ModelC& m, const double* p, int64_t sx, int64_t sy, int64_t o) {
+    double dx = 0.5 * (p[o + sx] - p[o - sx]);
+    double dy = 0.5 * (p[o + sy] - p[o - sy]);
+    double dx2 = dx * dx;
+    double dy2 = dy * dy;
+    double sum = dx2 + dy2;
+    double mag2 = sum * sum;
+    if (mag2 <= m.tol) return m.a_bar;
+    return m.a_bar * (1.0 + m.eps_prime * (dx2 * dx2 + dy2 * dy2) / mag2);
+}
+
+// ModelC::vector_field_block(Driver::Time) on CartesianGrid<2>
+// (phasefield.rs:367-421): KarmaRappelFlux::kernel (finite_volume.rs:248-285)
+// into dphi, the local-term loop (phasefield.rs:393-404), the u Laplacian and
+// the coupling (phasefield.rs:412-421).  Interior entries of kphi/ku only.
+void modelc_drift_block(const Grid& grid, const ModelC& m, const std::vector<double>& phi,
+                        const std::vector<double>& u, std::vector<double>& kphi, std::vector<double>& ku) {
+    const int g = 1;
+    const int64_t sx = 1, sy = grid.block[0] + 2 * g;
+    const double* p = phi.data();
+    double inv_h2 = 1.0 / (grid.spacing[0] * grid.spacing[1]);
+    double quarter = 0.25;
+    for_each_interior(grid, [&](const int64_t* idx) {
+        int64_t o = grid.linearize(idx, g);
+        auto P = [&](int di, int dj) { return p[o + di * sx + dj * sy]; };
+        double derx_r = P(1, 0) - P(0, 0);
+        double derx_l = P(0, 0) - P(-1, 0);
+        double derx_t = quarter * (P(1, 1) - P(-1, 1) + P(1, 0) - P(-1, 0));
+        double derx_b = quarter * (P(1, 0) - P(-1, 0) + P(1, -1) - P(-1, -1));
+        double dery_t = P(0, 1) - P(0, 0);
+        double dery_b = P(0, 0) - P(0, -1);
+        double dery_r = quarter * (P(1, 1) - P(1, -1) + P(0, 1) - P(0, -1));
+        double dery_l = quarter * (P(0, 1) - P(0, -1) + P(-1, 1) - P(-1, -1));
+        double a_r, da_r, a_l, da_l, a_t, da_t, a_b, da_b;
+        kr_face(m, derx_r, dery_r, &a_r, &da_r);
+        kr_face(m, derx_l, dery_l, &a_l, &da_l);
+        kr_face(m, derx_t, dery_t, &a_t, &da_t);
+        kr_face(m, derx_b, dery_b, &a_b, &da_b);
+        double j_r = a_r * (a_r * derx_r - da_r * dery_r);
+        double j_l = a_l * (a_l * derx_l - da_l * dery_l);
+        double j_t = a_t * (a_t * dery_t + da_t * derx_t);
+        double j_b = a_b * (a_b * dery_b + da_b * derx_b);
+        kphi[o] = (j_r - j_l + j_t - j_b) * inv_h2;
+    });
+    for_each_interior(grid, [&](const int64_t* idx) {
+        int64_t o = grid.linearize(idx, g);
+        double pv = p[o];
+        double g_prime = std::fma(pv * pv, pv, -pv);
+        double one_m_p2 = std::fma(pv, -pv, 1.0);
+        double p_prime = one_m_p2 * one_m_p2;
+        double a = center_anisotropy(m, p, sx, sy, o);
+        double val = std::fma(m.lambda * u[o], -p_prime, kphi[o] - g_prime) / (a * a);
+        kphi[o] = val;
+    });
+    central_laplacian(grid, u, ku, g);
+    for_each_interior(grid, [&](const int64_t* idx) {
+        int64_t o = grid.linearize(idx, g);
+        ku[o] = std::fma(ku[o], m.d_thermal, 0.5 * kphi[o]);
+    });
+}
+
+// EulerMaruyama::step (src/integrators/euler_maruyama.rs:34-75) with
+// ModelC<Wiener<1>> (noise != 0) or ModelC<NoNoise>, fields phi=0, u=1.
+double modelc_run(const Grid& grid, State& st, const ModelC& m, double t, double dt, uint64_t seed,
+                  int64_t steps, bool wiener, int nthreads) {
+    const int64_t nb = grid.num_blocks();
+    const int64_t len = grid.block_len(1);
+    // Stage buffers (simulation.rs:187-202): Tendency(Time) carries phi and
+    // u; Tendency(Wiener(0)) carries phi only (phasefield.rs:340-341).
+    std::vector<std::vector<double>> kphi(nb, std::vector<double>(len, 0.0));
+    std::vector<std::vector<double>> ku(nb, std::vector<double>(len, 0.0));
+    std::vector<std::vector<double>> amp(wiener ? nb : 0, std::vector<double>(len, 0.0));
+    for (int64_t s = 0; s < steps; ++s) {
+        // StepCtx::eval_drift (integrators/mod.rs:190-198)
+        fill_ghosts_mirror(grid, st, 0);
+        fill_ghosts_mirror(grid, st, 1);
+        parallel_blocks(nb, nthreads, [&](int64_t b) {
+            modelc_drift_block(grid, m, st.slab[b][0], st.slab[b][1], kphi[b], ku[b]);
+        });
+        if (wiener) {
+            // eval_tendency_impl: fill_zero then amp_phi = b on the interior
+            // (integrators/mod.rs:251-277, phasefield.rs:361-366)
+            parallel_blocks(nb, nthreads, [&](int64_t b) {
+                std::fill(amp[b].begin(), amp[b].end(), 0.0);
+                for_each_interior(grid, [&](const int64_t* idx) { amp[b][grid.linearize(idx, 1)] = m.noise_amplitude; });
+            });
+        }
+        // State::apply_step_with (state.rs:656-699), salt = t.to_bits()
+        uint64_t salt;
+        std::memcpy(&salt, &t, sizeof salt);
+        parallel_blocks(nb, nthreads, [&](int64_t b) {
+            // Driver::Time (driver.rs:131-138) over phi then u
+            for (int f = 0; f < 2; ++f) {
+                std::vector<double>& x = st.slab[b][f];
+                const std::vector<double>& v = f == 0 ? kphi[b] : ku[b];
+                for (int64_t i = 0; i < len; ++i) x[i] += dt * v[i];
+            }
+            if (wiener) {
+                // Driver::Wiener(0) (driver.rs:139-158)
+                double scale = std::sqrt(dt);
+                uint64_t parts[3] = {salt, (1ull << 32) | 0ull, (uint64_t)b};
+                uint64_t block_key = mix_key(seed, parts, 3);
+                std::vector<double>& x = st.slab[b][0];
+                const std::vector<double>& v = amp[b];
+                for (int64_t i = 0; i < len; ++i) {
+                    if (v[i] == 0.0) continue;
+                    uint64_t cell;
+                    if (!grid.cell_key(1, i, &cell)) continue;
+                    uint64_t key = splitmix64(block_key ^ cell);
+                    x[i] += scale * v[i] * standard_normal(key);
+                }
+            }
+        });
+        t += dt;
+    }
+    return t;
+}
+
+// phasefield.rs:227-286 (initialize_grains, orientations disabled)
+void modelc_initialize_grains(const Grid& grid, State& st, const double* grains, int64_t n, double u0) {
+    const double CUTOFF = 27.0;
+    const int64_t nx = grid.block[0], ny = grid.block[1];
+    for (int64_t b = 0; b < grid.num_blocks(); ++b) {
+        double hx = grid.spacing[0], hy = grid.spacing[1];
+        int64_t i0[3] = {0, 0, 0}, i1[3] = {nx - 1, ny - 1, 0};
+        double c0[3], c1[3];
+        grid.cell_center(b, i0, c0);
+        grid.cell_center(b, i1, c1);
+        double lo[2] = {std::fma(0.5, -hx, c0[0]), std::fma(0.5, -hy, c0[1])};
+        double hi[2] = {std::fma(0.5, hx, c1[0]), std::fma(0.5, hy, c1[1])};
+        auto dist_box = [&](double cx, double cy) {
+            double dx = std::max(std::max(lo[0] - cx, cx - hi[0]), 0.0);
+            double dy = std::max(std::max(lo[1] - cy, cy - hi[1]), 0.0);
+            return std::hypot(dx, dy);
+        };
+        std::vector<int64_t> near;
+        for (int64_t k = 0; k < n; ++k)
+            if (dist_box(grains[4 * k], grains[4 * k + 1]) <= grains[4 * k + 2] + CUTOFF) near.push_back(k);
+        std::vector<double>& phi = st.slab[b][0];
+        std::vector<double>& u = st.slab[b][1];
+        for_each_interior(grid, [&](const int64_t* idx) {
+            double v = -1.0;
+            if (!near.empty()) {
+                double xy[3];
+                grid.cell_center(b, idx, xy);
+                for (int64_t k : near) {
+                    double r = std::hypot(xy[0] - grains[4 * k], xy[1] - grains[4 * k + 1]);
+                    double pk = -std::tanh((r - grains[4 * k + 2]) / std::sqrt(2.0));
+                    v = std::fmax(v, pk);
+                }
+            }
+            phi[grid.linearize(idx, 1)] = v;
+        });
+        for_each_interior(grid, [&](const int64_t* idx) { u[grid.linearize(idx, 1)] = -u0; });
+    }
+}
+
+}  // namespace
+
+// ============================================================ C ABI =======
+extern "C" {
+
+uint64_t orc_splitmix64(uint64_t z) { return splitmix64(z); }
+uint64_t orc_mix_key(uint64_t seed, const uint64_t* parts, int64_t n) { return mix_key(seed, parts, (size_t)n); }
+double orc_unit_open(uint64_t bits) { return unit_open(bits); }
+double orc_standard_normal(uint64_t key) { return standard_normal(key); }
+void orc_standard_normal_batch(const uint64_t* keys, int64_t n, double* out) {
+    for (int64_t i = 0; i < n; ++i) out[i] = standard_normal(keys[i]);
+}
+
+void* orc_grid_create(int D, const int64_t* cells, const int64_t* block, const double* origin,
+                      const double* spacing, const int* periodic) {
+    if (D < 1 || D > 3) return nullptr;
+    Grid* g = new Grid();
+    g->D = D;
+    for (int d = 0; d < 3; ++d) {
+        bool on = d < D;
+        g->cells[d] = on ? cells[d] : 1;
+        g->block[d] = on ? block[d] : 1;
+        g->origin[d] = on ? origin[d] : 0.0;
+        g->spacing[d] = on ? spacing[d] : 1.0;
+        g->periodic[d] = on ? periodic[d] != 0 : false;
+        if (on && (g->cells[d] <= 0 || g->block[d] <= 0 || g->cells[d] % g->block[d] != 0 ||
+                   !(g->spacing[d] > 0.0) || !std::isfinite(g->spacing[d]))) {
+            delete g;
+            return nullptr;
+        }
+        g->nb[d] = g->cells[d] / g->block[d];
+    }
+    return g;
+}
+void orc_grid_destroy(void* g) { delete static_cast<Grid*>(g); }
+int64_t orc_grid_num_blocks(const void* g) { return static_cast<const Grid*>(g)->num_blocks(); }
+int64_t orc_grid_block_len(const void* g, int ghost) { return static_cast<const Grid*>(g)->block_len(ghost); }
+int64_t orc_grid_face_neighbor(const void* g, int64_t b, int dim, int dir) {
+    return static_cast<const Grid*>(g)->face_neighbor(b, dim, dir);
+}
+void orc_grid_cell_center(const void* g, int64_t b, const int64_t* idx, double* out) {
+    static_cast<const Grid*>(g)->cell_center(b, idx, out);
+}
+int orc_grid_cell_key(const void* g, int ghost, int64_t offset, uint64_t* key) {
+    return static_cast<const Grid*>(g)->cell_key(ghost, offset, key) ? 1 : 0;
+}
+
+void* orc_state_create(const void* grid, int nfields, const int* ghosts) {
+    const Grid& g = *static_cast<const Grid*>(grid);
+    std::vector<int> gh(ghosts, ghosts + nfields);
+    for (int f = 0; f < nfields; ++f)
+        for (int d = 0; d < g.D; ++d)
+            if (gh[f] < 0 || gh[f] > g.block[d]) return nullptr;  // cartesian.rs:456-462
+    std::vector<bool> keep(nfields, true);
+    return new State(make_state(g, gh, keep));
+}
+void orc_state_destroy(void* s) { delete static_cast<State*>(s); }
+
+// Copy field f of every block, block order, each slab ghost-inclusive.
+void orc_state_set_field(void* s, int f, const double* data) {
+    State& st = *static_cast<State*>(s);
+    size_t off = 0;
+    for (auto& b : st.slab) {
+        std::memcpy(b[f].data(), data + off, b[f].size() * sizeof(double));
+        off += b[f].size();
+    }
+}
+void orc_state_get_field(const void* s, int f, double* data) {
+    const State& st = *static_cast<const State*>(s);
+    size_t off = 0;
+    for (auto& b : st.slab) {
+        std::memcpy(data + off, b[f].data(), b[f].size() * sizeof(double));
+        off += b[f].size();
+    }
+}
+
+void orc_fill_ghosts_mirror(const void* grid, void* s, int f) {
+    fill_ghosts_mirror(*static_cast<const Grid*>(grid), *static_cast<State*>(s), f);
+}
+
+double orc_heat_run(const void* grid, void* s, int f, double kappa, double t0, double dt, int64_t steps,
+                    int nthreads) {
+    return heat_run(*static_cast<const Grid*>(grid), *static_cast<State*>(s), f, kappa, t0, dt, steps, nthreads);
+}
+
+double orc_modelc_run(const void* grid, void* s, const orc_modelc_params* p, double t0, double dt, uint64_t seed,
+                      int64_t steps, int wiener, int nthreads) {
+    ModelC m = make_model(p);
+    return modelc_run(*static_cast<const Grid*>(grid), *static_cast<State*>(s), m, t0, dt, seed, steps,
+                      wiener != 0, nthreads);
+}
+
+// One drift evaluation (k interior) without an update, for kernel-level tests.
+void orc_modelc_drift(const void* grid, void* s, const orc_modelc_params* p, double* kphi_out, double* ku_out) {
+    const Grid& g = *static_cast<const Grid*>(grid);
+    State& st = *static_cast<State*>(s);
+    ModelC m = make_model(p);
+    int64_t len = g.block_len(1);
+    for (int64_t b = 0; b < g.num_blocks(); ++b) {
+        std::vector<double> kp(len, 0.0), ku(len, 0.0);
+        modelc_drift_block(g, m, st.slab[b][0], st.slab[b][1], kp, ku);
+        std::memcpy(kphi_out + b * len, kp.data(), len * sizeof(double));
+        std::memcpy(ku_out + b * len, ku.data(), len * sizeof(double));
+    }
+}
+
+void orc_modelc_initialize_grains(const void* grid, void* s, const double* grains, int64_t n, double u0) {
+    modelc_initialize_grains(*static_cast<const Grid*>(grid), *static_cast<State*>(s), grains, n, u0);
+}
+
+int orc_num_threads_available(void) {
+#ifdef _OPENMP
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
+}
+
+}  // extern "C"

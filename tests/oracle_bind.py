@@ -1,0 +1,173 @@
+"""ctypes binding of the CPU oracle (oracle/liblegendre_oracle.so) for the tests.
+
+The oracle restates the reference's SerialScheduler path on the CPU; tests use
+it only as the checker of the CUDA library.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent.parent
+_PATH = ROOT / "oracle" / "liblegendre_oracle.so"
+
+
+class Params(C.Structure):
+    _fields_ = [("eps4", C.c_double), ("lambda_", C.c_double), ("d_thermal", C.c_double),
+                ("noise_amplitude", C.c_double), ("anisotropy_tol", C.c_double), ("flux_tol", C.c_double)]
+
+
+def _load():
+    if not _PATH.exists():
+        from legendre_b200 import build
+        build.build_oracle()
+    lib = C.CDLL(str(_PATH))
+    p, i64, u64, d = C.c_void_p, C.c_int64, C.c_uint64, C.c_double
+    pd, pi64 = C.POINTER(C.c_double), C.POINTER(C.c_int64)
+    sigs = {
+        "orc_splitmix64": (u64, [u64]),
+        "orc_mix_key": (u64, [u64, C.POINTER(C.c_uint64), i64]),
+        "orc_unit_open": (d, [u64]),
+        "orc_standard_normal": (d, [u64]),
+        "orc_standard_normal_batch": (None, [C.POINTER(C.c_uint64), i64, pd]),
+        "orc_grid_create": (p, [C.c_int, pi64, pi64, pd, pd, C.POINTER(C.c_int)]),
+        "orc_grid_destroy": (None, [p]),
+        "orc_grid_num_blocks": (i64, [p]),
+        "orc_grid_block_len": (i64, [p, C.c_int]),
+        "orc_grid_face_neighbor": (i64, [p, i64, C.c_int, C.c_int]),
+        "orc_grid_cell_center": (None, [p, i64, pi64, pd]),
+        "orc_grid_cell_key": (C.c_int, [p, C.c_int, i64, C.POINTER(C.c_uint64)]),
+        "orc_state_create": (p, [p, C.c_int, C.POINTER(C.c_int)]),
+        "orc_state_destroy": (None, [p]),
+        "orc_state_set_field": (None, [p, C.c_int, pd]),
+        "orc_state_get_field": (None, [p, C.c_int, pd]),
+        "orc_fill_ghosts_mirror": (None, [p, p, C.c_int]),
+        "orc_heat_run": (d, [p, p, C.c_int, d, d, d, i64, C.c_int]),
+        "orc_modelc_run": (d, [p, p, C.POINTER(Params), d, d, u64, i64, C.c_int, C.c_int]),
+        "orc_modelc_drift": (None, [p, p, C.POINTER(Params), pd, pd]),
+        "orc_modelc_initialize_grains": (None, [p, p, pd, i64, d]),
+        "orc_num_threads_available": (C.c_int, []),
+    }
+    for name, (res, args) in sigs.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    return lib
+
+
+lib = _load()
+
+
+def splitmix64(z):
+    return lib.orc_splitmix64(z)
+
+
+def mix_key(seed, parts):
+    arr = (C.c_uint64 * len(parts))(*parts)
+    return lib.orc_mix_key(seed, arr, len(parts))
+
+
+def standard_normal(keys):
+    keys = np.ascontiguousarray(keys, dtype=np.uint64)
+    out = np.empty(keys.size, dtype=np.float64)
+    lib.orc_standard_normal_batch(keys.ctypes.data_as(C.POINTER(C.c_uint64)), keys.size,
+                                  out.ctypes.data_as(C.POINTER(C.c_double)))
+    return out
+
+
+class Grid:
+    """The oracle's CartesianGrid<D>."""
+
+    def __init__(self, cells, block, origin, spacing, periodic=None):
+        D = len(cells)
+        periodic = periodic or [False] * D
+        self.D, self.cells, self.block = D, tuple(cells), tuple(block)
+        self.origin, self.spacing, self.periodic = tuple(origin), tuple(spacing), tuple(periodic)
+        self.h = lib.orc_grid_create(D, (C.c_int64 * D)(*cells), (C.c_int64 * D)(*block), (C.c_double * D)(*origin),
+                                     (C.c_double * D)(*spacing), (C.c_int * D)(*[int(x) for x in periodic]))
+        if not self.h:
+            raise ValueError("invalid grid")
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib.orc_grid_destroy(self.h)
+
+    def num_blocks(self):
+        return lib.orc_grid_num_blocks(self.h)
+
+    def block_len(self, g):
+        return lib.orc_grid_block_len(self.h, g)
+
+    def face_neighbor(self, b, dim, direction):
+        r = lib.orc_grid_face_neighbor(self.h, b, dim, direction)
+        return None if r < 0 else r
+
+    def cell_center(self, b, idx):
+        out = (C.c_double * 3)()
+        ii = (C.c_int64 * 3)(*(list(idx) + [0] * (3 - len(idx))))
+        lib.orc_grid_cell_center(self.h, b, ii, out)
+        return tuple(out[: self.D])
+
+    def slab_shape(self, g):
+        return tuple(b + 2 * g for b in reversed(self.block))
+
+
+class State:
+    """The oracle's block-major State: fields with ghost widths."""
+
+    def __init__(self, grid: Grid, ghosts):
+        self.grid = grid
+        self.ghosts = list(ghosts)
+        self.h = lib.orc_state_create(grid.h, len(ghosts), (C.c_int * len(ghosts))(*ghosts))
+        if not self.h:
+            raise ValueError("invalid state (ghost wider than a block?)")
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib.orc_state_destroy(self.h)
+
+    def get(self, f):
+        g = self.ghosts[f]
+        out = np.empty((self.grid.num_blocks(),) + self.grid.slab_shape(g), dtype=np.float64)
+        lib.orc_state_get_field(self.h, f, out.ctypes.data_as(C.POINTER(C.c_double)))
+        return out
+
+    def set(self, f, data):
+        arr = np.ascontiguousarray(data, dtype=np.float64)
+        assert arr.size == self.grid.num_blocks() * self.grid.block_len(self.ghosts[f])
+        lib.orc_state_set_field(self.h, f, arr.ctypes.data_as(C.POINTER(C.c_double)))
+
+    def interior(self, f):
+        g = self.ghosts[f]
+        a = self.get(f)
+        sl = (slice(None),) + tuple(slice(g, g + n) for n in reversed(self.grid.block))
+        return np.ascontiguousarray(a[sl])
+
+    def fill_ghosts(self, f):
+        lib.orc_fill_ghosts_mirror(self.grid.h, self.h, f)
+
+    def heat_run(self, f, kappa, t0, dt, steps, threads=1):
+        return lib.orc_heat_run(self.grid.h, self.h, f, kappa, t0, dt, steps, threads)
+
+    def modelc_run(self, params: Params, t0, dt, seed, steps, wiener, threads=1):
+        return lib.orc_modelc_run(self.grid.h, self.h, C.byref(params), t0, dt, seed, steps, int(wiener), threads)
+
+    def modelc_drift(self, params: Params):
+        n = self.grid.num_blocks() * self.grid.block_len(1)
+        kp, ku = np.zeros(n), np.zeros(n)
+        lib.orc_modelc_drift(self.grid.h, self.h, C.byref(params), kp.ctypes.data_as(C.POINTER(C.c_double)),
+                             ku.ctypes.data_as(C.POINTER(C.c_double)))
+        shape = (self.grid.num_blocks(),) + self.grid.slab_shape(1)
+        return kp.reshape(shape), ku.reshape(shape)
+
+    def initialize_grains(self, grains, u0):
+        arr = np.array([[g[0], g[1], g[2], 0.0] for g in grains], dtype=np.float64)
+        lib.orc_modelc_initialize_grains(self.grid.h, self.h, arr.ctypes.data_as(C.POINTER(C.c_double)), len(grains),
+                                         u0)
+
+
+def modelc_params(eps4=0.06, lam=3.19, d_thermal=None, noise=0.0, tol=1e-8, flux_tol=1e-8):
+    """ModelC::new (phasefield.rs:100-116): d_thermal = A2 * lambda unless given."""
+    return Params(eps4, lam, 0.6267 * lam if d_thermal is None else d_thermal, noise, tol, flux_tol)

@@ -1,0 +1,227 @@
+"""CUDA path against the oracle on the same seeded inputs (needs a GPU).
+
+FP64 results are compared bit for bit; the noisy Model C path compares the
+integer key stream exactly and the Gaussian within 1e-12 relative.
+"""
+import math
+
+import numpy as np
+import pytest
+
+import legendre_b200 as L
+from util import centers, relative_eq, with_ghosts
+
+pytestmark = pytest.mark.gpu
+
+H = 0.4
+
+
+def dev_state(sched, cells, block, ghosts, periodic=None, spacing=1.0, dtype="f64"):
+    D = len(cells)
+    grid = L.CartesianGrid(cells, block, [0.0] * D, [spacing] * D).with_periodic(periodic or [False] * D)
+    specs = [L.FieldSpec(f"f{i}", g) for i, g in enumerate(ghosts)]
+    return L.DeviceState(grid, sched, L.CudaAllocator(dtype), specs)
+
+
+HALO_CASES = [
+    ([8], [4], 1, None),
+    ([8], [4], 2, None),
+    ([8], [4], 1, [True]),
+    ([4], [4], 2, [True]),
+    ([4, 4], [4, 4], 1, [True, False]),
+    ([12, 8], [4, 4], 1, [True, False]),
+    ([8, 12], [4, 4], 2, [False, True]),
+    ([64, 64], [32, 32], 1, None),
+    ([16, 16, 16], [8, 8, 8], 1, None),
+    ([12, 12, 12], [6, 4, 3], 1, [True, False, True]),
+    ([12, 12, 12], [6, 4, 3], 3, [False, True, True]),
+    ([6, 6, 6], [6, 6, 6], 2, [True, True, True]),
+]
+
+
+@pytest.mark.parametrize("cells,block,ghost,periodic", HALO_CASES)
+@pytest.mark.parametrize("dtype", ["f64", "f32"])
+def test_halo_fill_matches_oracle(sched, orc, cells, block, ghost, periodic, dtype):
+    D = len(cells)
+    st = dev_state(sched, cells, block, [ghost], periodic, dtype=dtype)
+    og = orc.Grid(cells, block, [0.0] * D, [1.0] * D, periodic)
+    os_ = orc.State(og, [ghost])
+    rng = np.random.default_rng(sum(cells) + ghost)
+    data = rng.standard_normal((og.num_blocks(),) + og.slab_shape(ghost))
+    if dtype == "f32":
+        data = data.astype(np.float32).astype(np.float64)
+    st.upload(0, data)
+    os_.set(0, data)
+    st.fill_ghosts(0)
+    os_.fill_ghosts(0)
+    assert np.array_equal(st.download(0).astype(np.float64), os_.get(0))
+
+
+def _heat_pair(sched, orc, cells, block, periodic, h, kappa, dt, steps, graph=False, seed=3):
+    D = len(cells)
+    grid = L.CartesianGrid(cells, block, [0.0] * D, [h] * D).with_periodic(periodic or [False] * D)
+    model = L.Heat(kappa)
+    sim = L.Simulation(grid, L.FiniteDifference(), model, L.ForwardEuler(), sched, L.CudaAllocator("f64"))
+    rng = np.random.default_rng(seed)
+    u0 = with_ghosts(rng.standard_normal((grid.num_blocks(),) + tuple(reversed(block))), 1)
+    sim.state.upload("u", u0)
+    sim.run(dt, steps, graph=graph)
+    og = orc.Grid(cells, block, [0.0] * D, [h] * D, periodic)
+    os_ = orc.State(og, [1])
+    os_.set(0, u0)
+    t = os_.heat_run(0, kappa, 0.0, dt, steps)
+    return sim, os_, t
+
+
+@pytest.mark.parametrize("cells,block,periodic", [
+    ([16, 16, 16], [8, 8, 8], None),
+    ([32, 32], [16, 16], [True, True]),
+    ([32, 32], [32, 32], [True, True]),
+    ([64], [16], [True]),
+    ([24, 16, 8], [8, 8, 4], [False, True, False]),
+])
+def test_heat_bit_identical_to_oracle(sched, orc, cells, block, periodic):
+    sim, os_, t = _heat_pair(sched, orc, cells, block, periodic, 0.1, 0.7, 0.5 / 6.0 * 0.01 / 0.7, 37)
+    assert np.array_equal(sim.state.interior("u"), os_.interior(0))
+    assert sim.time() == t and sim.step_index() == 37
+
+
+def test_heat_graph_replay_identical(sched, orc):
+    sim, os_, _ = _heat_pair(sched, orc, [16, 16, 16], [8, 8, 8], None, 0.1, 0.7, 0.001, 131, graph=True)
+    assert np.array_equal(sim.state.interior("u"), os_.interior(0))
+
+
+def test_heat_benchmark_config_short(sched, orc):
+    # 96^3 periodic, 6^3 blocks of 16^3, dt = 0.15 h^2, sine + seeded noise IC
+    h = 1.0 / 96
+    grid = L.CartesianGrid([96] * 3, [16] * 3, [0.0] * 3, [h] * 3).with_periodic([True] * 3)
+    model = L.Heat(1.0)
+    sim = L.Simulation(grid, L.FiniteDifference(), model, L.ForwardEuler(), sched, L.CudaAllocator("f64"))
+    model.initialize_sine_noise(sim.state, 42, 1e-3)
+    u0 = sim.state.download("u")
+    # the initial condition against its definition
+    x, y, z = (centers([96] * 3, [16] * 3, [0.0] * 3, [h] * 3, d) for d in range(3))
+    ref = np.sin(2 * np.pi * x) * np.sin(2 * np.pi * y) * np.sin(2 * np.pi * z)
+    assert np.max(np.abs(sim.state.interior("u") - ref)) <= 1e-3 + 1e-14
+    dt = 0.15 * h * h
+    sim.run(dt, 20, graph=True)
+    og = orc.Grid([96] * 3, [16] * 3, [0.0] * 3, [h] * 3, [True] * 3)
+    os_ = orc.State(og, [1])
+    os_.set(0, u0)
+    os_.heat_run(0, 1.0, 0.0, dt, 20, 8)
+    assert np.array_equal(sim.state.interior("u"), os_.interior(0))
+
+
+def test_heat_analytic_decay_on_gpu(sched):
+    # tests/heat3d.rs:82-137 on the device
+    h, kappa, n = 0.1, 0.7, 16
+    grid = L.CartesianGrid([n] * 3, [n // 2] * 3, [0.0] * 3, [h] * 3)
+    model = L.Heat(kappa)
+    sim = L.Simulation(grid, L.FiniteDifference(), model, L.ForwardEuler(), sched, L.CudaAllocator("f64"))
+    kx = math.pi / (n * h)
+    x = centers([n] * 3, [n // 2] * 3, [0.0] * 3, [h] * 3, 0)
+    u0 = np.vectorize(math.cos)(kx * x)
+    sim.state.upload("u", with_ghosts(u0, 1))
+    dt = sim.stable_dt()
+    sim.run(dt, 200)
+    lam = (2.0 - 2.0 * math.cos(kx * h)) / (h * h)
+    assert relative_eq(sim.state.interior("u"), (1.0 - dt * kappa * lam) ** 200 * u0, 1e-10, 1e-12).all()
+
+
+# ---------------------------------------------------------------- Model C --
+def _modelc_pair(sched, orc, cells, block, grains, noise, steps, seed=7, graph=False, dtype="f64", eps4=0.06,
+                 lam=3.19, threads=4):
+    grid = L.CartesianGrid(cells, block, [0.0, 0.0], [H, H])
+    model = L.ModelC(eps4, lam, noise)
+    sim = L.Simulation(grid, L.FiniteVolume(), model, L.EulerMaruyama(seed), sched, L.CudaAllocator(dtype))
+    og = orc.Grid(cells, block, [0.0, 0.0], [H, H])
+    os_ = orc.State(og, [1, 1])
+    os_.initialize_grains([(g[0], g[1], g[2]) for g in grains], 0.7)
+    if dtype == "f64":
+        model.initialize_grains(grid, sim.state, [L.Grain((g[0], g[1]), g[2]) for g in grains], 0.7)
+        assert np.array_equal(sim.state.interior("phi"), os_.interior(0))
+        assert np.array_equal(sim.state.interior("u"), os_.interior(1))
+    else:
+        sim.state.upload("phi", os_.get(0))
+        sim.state.upload("u", os_.get(1))
+    dt = model.stable_dt(grid.spacing)
+    if steps:
+        sim.run(dt, steps, graph=graph)
+    p = orc.modelc_params(eps4=eps4, lam=lam, noise=noise)
+    t = os_.modelc_run(p, 0.0, dt, seed, steps, wiener=True, threads=threads)
+    return sim, os_, t
+
+
+@pytest.mark.parametrize("cells,block,grains", [
+    ([64, 64], [32, 32], [(H, H, 10 * H)]),
+    ([64, 64], [64, 64], [(H, H, 10 * H)]),
+    ([96, 64], [32, 32], [(10.0, 12.0, 4.0), (30.0, 14.0, 3.0)]),
+    ([48, 80], [16, 16], [(9.5, 16.0, 5.0)]),
+])
+def test_modelc_noise_free_bit_identical(sched, orc, cells, block, grains):
+    sim, os_, t = _modelc_pair(sched, orc, cells, block, grains, 0.0, 300)
+    assert np.array_equal(sim.state.interior("phi"), os_.interior(0))
+    assert np.array_equal(sim.state.interior("u"), os_.interior(1))
+    assert sim.time() == t
+
+
+def test_modelc_decomposition_independent_without_noise(sched, orc):
+    res = []
+    for block in ([64, 64], [32, 32], [16, 16]):
+        sim, _, _ = _modelc_pair(sched, orc, [64, 64], block, [(H, H, 10 * H)], 0.0, 50)
+        phi = sim.state.interior("phi")
+        nb = 64 // block[0]
+        full = phi.reshape(nb, nb, block[1], block[0]).transpose(0, 2, 1, 3).reshape(64, 64)
+        res.append(full)
+    assert np.array_equal(res[0], res[1]) and np.array_equal(res[0], res[2])
+
+
+def test_standard_normal_within_1e12(sched, orc):
+    rng = np.random.default_rng(11)
+    keys = rng.integers(0, 2**63, size=100_000, dtype=np.int64).astype(np.uint64) * np.uint64(2) + np.uint64(1)
+    keys[:4] = [0, 1, 2**64 - 1, 0xD1B54A32D192ED03]
+    import ctypes as C
+    out = np.empty(keys.size)
+    L._native.check(L._native.lib.lg_standard_normal(sched.handle, keys.ctypes.data_as(C.POINTER(C.c_uint64)),
+                                                     keys.size, out.ctypes.data_as(C.POINTER(C.c_double))),
+                    sched.handle)
+    ref = orc.standard_normal(keys)
+    assert np.all(np.abs(out - ref) <= 1e-12 * np.abs(ref))
+
+
+def test_modelc_noisy_matches_oracle(sched, orc):
+    sim, os_, t = _modelc_pair(sched, orc, [64, 64], [32, 32], [(H, H, 10 * H)], 0.05, 300)
+    phi, phi_ref = sim.state.interior("phi"), os_.interior(0)
+    assert np.allclose(phi, phi_ref, rtol=1e-12, atol=1e-12)
+    assert np.allclose(sim.state.interior("u"), os_.interior(1), rtol=1e-12, atol=1e-12)
+    # the noise must actually be there
+    quiet, _, _ = _modelc_pair(sched, orc, [64, 64], [32, 32], [(H, H, 10 * H)], 0.0, 300)
+    assert not np.allclose(phi, quiet.state.interior("phi"), atol=1e-6)
+
+
+def test_modelc_graph_replay_identical(sched, orc):
+    a, os_, _ = _modelc_pair(sched, orc, [64, 64], [32, 32], [(H, H, 10 * H)], 0.05, 150, graph=True)
+    b, _, _ = _modelc_pair(sched, orc, [64, 64], [32, 32], [(H, H, 10 * H)], 0.05, 150, graph=False)
+    assert np.array_equal(a.state.interior("phi"), b.state.interior("phi"))
+    assert np.array_equal(a.state.interior("u"), b.state.interior("u"))
+
+
+def test_modelc_fp32_error_against_fp64_oracle(sched, orc):
+    sim, os_, _ = _modelc_pair(sched, orc, [64, 64], [32, 32], [(H, H, 10 * H)], 0.0, 400, dtype="f32")
+    phi = sim.state.interior("phi").astype(np.float64)
+    ref = os_.interior(0)
+    l2 = np.sqrt(np.mean((phi - ref) ** 2))
+    assert l2 < 1e-4, l2
+    assert np.max(np.abs(phi - ref)) < 1e-3
+
+
+def test_dendrite_grows_and_stays_physical_on_gpu(sched, orc):
+    # tests/model_c.rs:70-101 on the device
+    sim, _, _ = _modelc_pair(sched, orc, [64, 64], [32, 32], [(H, H, 10 * H)], 0.0, 0)
+    phi0 = sim.state.interior("phi")
+    dt = sim.model.stable_dt(sim.grid.spacing)
+    sim.run(dt, 1200, graph=True)
+    phi, u = sim.state.interior("phi"), sim.state.interior("u")
+    assert 0.95 < phi.max() < 1.1 and -1.1 < phi.min() < -0.95
+    assert (phi > 0).mean() > 1.5 * (phi0 > 0).mean()
+    assert -0.4 < u.max() < 0.05 and u.min() >= -0.75
