@@ -224,7 +224,10 @@ def main():
     import legendre_b200 as L
 
     rank, world, local, pg = dist_setup(args.gpus)
-    stream = torch.cuda.current_stream()
+    # a dedicated stream: the library launches on it and the CUDA events
+    # below are recorded on it
+    stream = torch.cuda.Stream(device=local)
+    torch.cuda.set_stream(stream)
     sched = L.CudaScheduler(local, stream.cuda_stream)
     sim, grid, model, grains = make_sim(cfg, args.dtype, sched, seed_offset=rank)
     initialize(sim, grid, model, grains, cfg, args.dtype, sched)

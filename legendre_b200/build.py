@@ -29,6 +29,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 # which never does); units holding only freely restructured FP32 kernels may.
 SOURCES = [
     ("lg_kernels.cu", ["-fmad=false"]),
+    ("lg_modelc.cu", ["-fmad=false"]),
     ("lg_abi.cu", ["-fmad=false"]),
 ]
 

@@ -494,6 +494,7 @@ int lg_modelc_em_run(lg_state* st, const lg_modelc_params* p, double dt, uint64_
     if (st->grid->D != 2 || st->nfields < 2 || st->ghosts[0] != 1 || st->ghosts[1] != 1)
         return fail(ctx, LG_ERR_STATE, "Model C needs a 2-D state with phi and u of ghost width 1");
     if (nsteps < 0) return fail(ctx, LG_ERR_INVALID, "negative step count");
+    if (variant < 0 || variant % 1000 > 2) return fail(ctx, LG_ERR_INVALID, "unknown kernel variant");
     cudaSetDevice(ctx->device);
     if (!st->ghosts_valid) {
         int rc = fill_all_ghosts(st);
@@ -523,16 +524,25 @@ int lg_modelc_em_run(lg_state* st, const lg_modelc_params* p, double dt, uint64_
     char key[512];
     snprintf(key, sizeof key, "modelc|%a|%a|%a|%a|%a|%a|dt=%a|seed=%llu|v=%d", p->eps4, p->lambda, p->d_thermal,
              p->noise_amplitude, p->anisotropy_tol, p->flux_tol, dt, (unsigned long long)seed, variant);
+    // variant = kind + 1000 * rows: kind 0 library default, 1 one thread per
+    // cell in reference order, 2 column tile; rows fixes the tile height
+    const int kind = variant % 1000, rows = variant / 1000;
+    const bool tile = (kind == 0 || kind == 2) && lg::modelc_tile_supported(topo);
+    if (kind == 2 && !tile) return fail(ctx, LG_ERR_INVALID, "the column-tile kernel needs blocks at most 1024 wide");
     auto step = [&]() -> int {
         cudaError_t e;
+        const void* in = st->arena[st->cur];
+        void* out = st->arena[st->cur ^ 1];
         if (st->dtype == LG_F64)
-            e = lg::launch_modelc_step_f64(static_cast<const double*>(st->arena[st->cur]),
-                                           static_cast<double*>(st->arena[st->cur ^ 1]), topo, L, m, dt, nz, st->d_t,
-                                           st->tslot, variant, ctx->stream);
+            e = tile ? lg::launch_modelc_tile_f64(static_cast<const double*>(in), static_cast<double*>(out), topo, L,
+                                                  m, dt, nz, st->d_t, st->tslot, rows, ctx->stream)
+                     : lg::launch_modelc_step_f64(static_cast<const double*>(in), static_cast<double*>(out), topo, L,
+                                                  m, dt, nz, st->d_t, st->tslot, variant, ctx->stream);
         else
-            e = lg::launch_modelc_step_f32(static_cast<const float*>(st->arena[st->cur]),
-                                           static_cast<float*>(st->arena[st->cur ^ 1]), topo, L, m, dt, nz, st->d_t,
-                                           st->tslot, variant, ctx->stream);
+            e = tile ? lg::launch_modelc_tile_f32(static_cast<const float*>(in), static_cast<float*>(out), topo, L,
+                                                  m, dt, nz, st->d_t, st->tslot, rows, ctx->stream)
+                     : lg::launch_modelc_step_f32(static_cast<const float*>(in), static_cast<float*>(out), topo, L, m,
+                                                  dt, nz, st->d_t, st->tslot, variant, ctx->stream);
         ctx->launches++;
         if (e != cudaSuccess) return cuda_fail(ctx, e, "Model C step launch");
         st->cur ^= 1;

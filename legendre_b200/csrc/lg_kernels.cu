@@ -10,13 +10,10 @@
 
 #include "lg_common.cuh"
 #include "lg_kernels.h"
+#include "lg_modelc_ops.cuh"
 
 namespace lg {
 namespace {
-
-__device__ __forceinline__ int64_t slab_base(const SlabLayout& L, int b, int field) {
-    return ((int64_t)b * L.nfields + field) * L.slab_stride;
-}
 
 // Offset of interior-relative index l inside a ghost-inclusive slab
 // (cartesian.rs:189-204).
@@ -180,52 +177,6 @@ __global__ void __launch_bounds__(256) heat_step_kernel(const double* __restrict
     }
     }
 }
-
-// ----------------------------------------------------------- Model C (a) --
-template <class T>
-struct MC {
-    T lambda, d_thermal, a_bar, eps_prime, tol, f_a_bar, f_eps_prime, f_a12, f_tol, inv_h2_flux, ih0, ih1;
-};
-
-template <class T>
-MC<T> to_mc(const ModelCDev& m) {
-    MC<T> r;
-    r.lambda = (T)m.lambda;
-    r.d_thermal = (T)m.d_thermal;
-    r.a_bar = (T)m.a_bar;
-    r.eps_prime = (T)m.eps_prime;
-    r.tol = (T)m.tol;
-    r.f_a_bar = (T)m.f_a_bar;
-    r.f_eps_prime = (T)m.f_eps_prime;
-    r.f_a12 = (T)m.f_a12;
-    r.f_tol = (T)m.f_tol;
-    r.inv_h2_flux = (T)m.inv_h2_flux;
-    r.ih0 = (T)m.inv_h2[0];
-    r.ih1 = (T)m.inv_h2[1];
-    return r;
-}
-
-// KarmaRappelFlux::face (finite_volume.rs:129-142)
-template <class T>
-__device__ __forceinline__ void kr_face(const MC<T>& m, T dx, T dy, T& a, T& da) {
-    T dx2 = dx * dx;
-    T dy2 = dy * dy;
-    T sum = dx2 + dy2;
-    T mag2 = sum * sum;
-    if (mag2 <= m.f_tol) {
-        a = m.f_a_bar;
-        da = T(0);
-    } else {
-        a = m.f_a_bar * (T(1) + m.f_eps_prime * (dx2 * dx2 + dy2 * dy2) / mag2);
-        da = -(m.f_a12) * dx * dy * (dx2 - dy2) / mag2;
-    }
-}
-
-__device__ __forceinline__ double fma_t(double a, double b, double c) { return fma(a, b, c); }
-__device__ __forceinline__ float fma_t(float a, float b, float c) { return fmaf(a, b, c); }
-
-__device__ __forceinline__ double normal_t(uint64_t key, double) { return standard_normal(key); }
-__device__ __forceinline__ float normal_t(uint64_t key, float) { return standard_normal_f32(key); }
 
 // Reference-order Model C step, one thread per interior cell: the flux
 // kernel (finite_volume.rs:258-283), the local terms (phasefield.rs:395-404),

@@ -1,0 +1,126 @@
+// Model C device arithmetic shared by the step kernels, written in the
+// reference's operand order.  Include only from translation units compiled
+// with -fmad=false (see lg_kernels.cu).
+#pragma once
+
+#include "lg_common.cuh"
+#include "lg_kernels.h"
+
+namespace lg {
+
+template <class T>
+struct MC {
+    T lambda, d_thermal, a_bar, eps_prime, tol, f_a_bar, f_eps_prime, f_a12, f_tol, inv_h2_flux, ih0, ih1;
+};
+
+template <class T>
+inline MC<T> to_mc(const ModelCDev& m) {
+    MC<T> r;
+    r.lambda = (T)m.lambda;
+    r.d_thermal = (T)m.d_thermal;
+    r.a_bar = (T)m.a_bar;
+    r.eps_prime = (T)m.eps_prime;
+    r.tol = (T)m.tol;
+    r.f_a_bar = (T)m.f_a_bar;
+    r.f_eps_prime = (T)m.f_eps_prime;
+    r.f_a12 = (T)m.f_a12;
+    r.f_tol = (T)m.f_tol;
+    r.inv_h2_flux = (T)m.inv_h2_flux;
+    r.ih0 = (T)m.inv_h2[0];
+    r.ih1 = (T)m.inv_h2[1];
+    return r;
+}
+
+// KarmaRappelFlux::face (finite_volume.rs:129-142)
+template <class T>
+__device__ __forceinline__ void kr_face(const MC<T>& m, T dx, T dy, T& a, T& da) {
+    T dx2 = dx * dx;
+    T dy2 = dy * dy;
+    T sum = dx2 + dy2;
+    T mag2 = sum * sum;
+    if (mag2 <= m.f_tol) {
+        a = m.f_a_bar;
+        da = T(0);
+    } else {
+        a = m.f_a_bar * (T(1) + m.f_eps_prime * (dx2 * dx2 + dy2 * dy2) / mag2);
+        da = -(m.f_a12) * dx * dy * (dx2 - dy2) / mag2;
+    }
+}
+
+// ModelC::center_anisotropy (phasefield.rs:159-175) from the half
+// differences dx = 0.5 (p(i+1) - p(i-1)), dy likewise.
+template <class T>
+__device__ __forceinline__ T center_anisotropy(const MC<T>& m, T dx, T dy) {
+    T dx2 = dx * dx;
+    T dy2 = dy * dy;
+    T sum = dx2 + dy2;
+    T mag2 = sum * sum;
+    if (mag2 <= m.tol) return m.a_bar;
+    return m.a_bar * (T(1) + m.eps_prime * (dx2 * dx2 + dy2 * dy2) / mag2);
+}
+
+__device__ __forceinline__ double fma_t(double a, double b, double c) { return fma(a, b, c); }
+__device__ __forceinline__ float fma_t(float a, float b, float c) { return fmaf(a, b, c); }
+
+__device__ __forceinline__ double normal_t(uint64_t key, double) { return standard_normal(key); }
+__device__ __forceinline__ float normal_t(uint64_t key, float) { return standard_normal_f32(key); }
+
+__device__ __forceinline__ int64_t slab_base(const SlabLayout& L, int b, int field) {
+    return ((int64_t)b * L.nfields + field) * L.slab_stride;
+}
+
+// The eight neighbours of one block of a 2-D Cartesian grid, for ghost
+// pushes: face neighbours from the topology table, diagonals by chaining
+// (x step, then y step).  -1 where the step leaves the domain through a
+// physical boundary; such steps are never taken (mirror images stay in the
+// block itself).
+struct Nbr2 {
+    int b, l, r, d, u, dl, dr, ul, ur;
+
+    __device__ __forceinline__ void load(const CartTopo& topo, int blk) {
+        b = blk;
+        l = topo.nbr[(blk * 3 + 0) * 2 + 0];
+        r = topo.nbr[(blk * 3 + 0) * 2 + 1];
+        d = topo.nbr[(blk * 3 + 1) * 2 + 0];
+        u = topo.nbr[(blk * 3 + 1) * 2 + 1];
+        dl = l >= 0 ? topo.nbr[(l * 3 + 1) * 2 + 0] : -1;
+        ul = l >= 0 ? topo.nbr[(l * 3 + 1) * 2 + 1] : -1;
+        dr = r >= 0 ? topo.nbr[(r * 3 + 1) * 2 + 0] : -1;
+        ur = r >= 0 ? topo.nbr[(r * 3 + 1) * 2 + 1] : -1;
+    }
+    __device__ __forceinline__ int at(int sx, int sy) const {
+        if (sy == 0) return sx == 0 ? b : (sx < 0 ? l : r);
+        if (sx == 0) return sy < 0 ? d : u;
+        if (sy < 0) return sx < 0 ? dl : dr;
+        return sx < 0 ? ul : ur;
+    }
+};
+
+// Ghost push of 2-D, ghost-width-1 fields: the value of interior cell (i, j)
+// goes to every ghost entry whose source it is (the separable map of the
+// reference's dimension sweep, cartesian.rs:439-526).  Scalars only, no
+// local arrays.
+template <class T>
+__device__ __forceinline__ void push_ghosts_2d_g1(T* __restrict__ out, const SlabLayout& L, int field,
+                                                  const Nbr2& nb, int n0, int n1, int i, int j, T v) {
+    const bool lo_x = i == 0, hi_x = i == n0 - 1, lo_y = j == 0, hi_y = j == n1 - 1;
+    if (!(lo_x | hi_x | lo_y | hi_y)) return;
+    const int sy = L.gdim[0];
+    const int sA = nb.l >= 0 ? -1 : 0, iA = nb.l >= 0 ? n0 : -1;
+    const int sB = nb.r >= 0 ? 1 : 0, iB = nb.r >= 0 ? -1 : n0;
+    const int sC = nb.d >= 0 ? -1 : 0, jC = nb.d >= 0 ? n1 : -1;
+    const int sD = nb.u >= 0 ? 1 : 0, jD = nb.u >= 0 ? -1 : n1;
+    auto put = [&](int sx, int syy, int ii, int jj) {
+        out[slab_base(L, nb.at(sx, syy), field) + (ii + 1) + (int64_t)(jj + 1) * sy] = v;
+    };
+    if (lo_x) put(sA, 0, iA, j);
+    if (hi_x) put(sB, 0, iB, j);
+    if (lo_y) put(0, sC, i, jC);
+    if (hi_y) put(0, sD, i, jD);
+    if (lo_x && lo_y) put(sA, sC, iA, jC);
+    if (lo_x && hi_y) put(sA, sD, iA, jD);
+    if (hi_x && lo_y) put(sB, sC, iB, jC);
+    if (hi_x && hi_y) put(sB, sD, iB, jD);
+}
+
+}  // namespace lg

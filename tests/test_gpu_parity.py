@@ -225,3 +225,31 @@ def test_dendrite_grows_and_stays_physical_on_gpu(sched, orc):
     assert 0.95 < phi.max() < 1.1 and -1.1 < phi.min() < -0.95
     assert (phi > 0).mean() > 1.5 * (phi0 > 0).mean()
     assert -0.4 < u.max() < 0.05 and u.min() >= -0.75
+
+
+@pytest.mark.parametrize("variant", [1, 2, 2 + 1000 * 16, 2 + 1000 * 24, 2 + 1000 * 7, 2 + 1000 * 5000])
+@pytest.mark.parametrize("noise", [0.0, 0.05])
+def test_modelc_kernel_variants_bit_identical(sched, orc, variant, noise):
+    # every kernel shape (reference order, column tiles of any height) gives
+    # the same bits; without noise they equal the oracle's
+    cells, block = [96, 64], [32, 32]
+    grains = [(10.0, 12.0, 4.0), (30.0, 14.0, 3.0)]
+    grid = L.CartesianGrid(cells, block, [0.0, 0.0], [H, H])
+    model = L.ModelC(0.06, 3.19, noise)
+    sim = L.Simulation(grid, L.FiniteVolume(), model, L.EulerMaruyama(3), sched, L.CudaAllocator("f64"))
+    model.initialize_grains(grid, sim.state, [L.Grain((g[0], g[1]), g[2]) for g in grains], 0.7)
+    sim.run(model.stable_dt(grid.spacing), 40, variant=variant)
+    ref = L.Simulation(grid, L.FiniteVolume(), model, L.EulerMaruyama(3), sched, L.CudaAllocator("f64"))
+    model.initialize_grains(grid, ref.state, [L.Grain((g[0], g[1]), g[2]) for g in grains], 0.7)
+    ref.run(model.stable_dt(grid.spacing), 40, variant=1)
+    assert np.array_equal(sim.state.download("phi"), ref.state.download("phi"))
+    assert np.array_equal(sim.state.download("u"), ref.state.download("u"))
+
+
+@pytest.mark.parametrize("block", [[7, 5], [1, 3], [33, 20], [256, 8]])
+def test_modelc_tile_ragged_blocks(sched, orc, block):
+    cells = [block[0] * 3, block[1] * 2]
+    g = (cells[0] * H / 2, cells[1] * H / 2, 2.0)
+    sim, os_, _ = _modelc_pair(sched, orc, cells, block, [g], 0.0, 25)
+    assert np.array_equal(sim.state.interior("phi"), os_.interior(0))
+    assert np.array_equal(sim.state.interior("u"), os_.interior(1))
