@@ -30,6 +30,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 SOURCES = [
     ("lg_kernels.cu", ["-fmad=false"]),
     ("lg_modelc.cu", ["-fmad=false"]),
+    ("lg_modelc_f32.cu", []),
     ("lg_abi.cu", ["-fmad=false"]),
 ]
 

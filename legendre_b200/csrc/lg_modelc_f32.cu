@@ -1,0 +1,113 @@
+// Model C column-tile step in FP32 storage and arithmetic.
+//
+// Same tile schedule as the FP64 kernel, but the arithmetic is restructured
+// for single precision (this unit is compiled with contraction allowed):
+//   * one approximate reciprocal per face serves both of its ratios, using
+//     (dx^4 + dy^4)/(dx^2 + dy^2)^2 = 1 - 2 dx^2 dy^2/(dx^2 + dy^2)^2, so
+//     A = a(1 + e') - 2 a e' dx^2 dy^2 / |grad|^4;
+//   * the 1/A^2 mobility is a reciprocal times the numerator;
+//   * the Gaussian is drawn from the same counter-based key as the FP64
+//     path, with the Box-Muller transform in single precision.
+// Its error against the FP64 oracle is measured by the tests.
+#include <cmath>
+
+#include "lg_modelc_tile.cuh"
+
+namespace lg {
+namespace {
+
+struct Fast32 {
+    float lambda, d_thermal, inv_h2_flux, ih0, ih1;
+    float f_a_bar, f_a1pe, f_2ae, f_a12, f_tol;  // flux: a, a(1+e'), 2 a e', a12, tol
+    float c_a_bar, c_a1pe, c_2ae, c_tol;         // cell-centred anisotropy
+};
+
+__device__ __forceinline__ float rcp_approx(float x) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
+struct OpsFast32 {
+    using Params = Fast32;
+
+    static __device__ __forceinline__ void aniso(float dx, float dy, float a_bar, float a1pe, float two_ae,
+                                                 float tol, float& a, float& inv) {
+        const float dx2 = dx * dx, dy2 = dy * dy;
+        const float s = dx2 + dy2;
+        const float mag2 = s * s;
+        inv = rcp_approx(mag2);
+        const bool flat = mag2 <= tol;
+        a = flat ? a_bar : a1pe - two_ae * (dx2 * dy2) * inv;
+        inv = flat ? 0.0f : inv;
+    }
+    static __device__ __forceinline__ float xface(const Fast32& m, float dn, float d1, float c, float e) {
+        const float dt = 0.25f * ((d1 + c) - e);
+        float a, inv;
+        aniso(dn, dt, m.f_a_bar, m.f_a1pe, m.f_2ae, m.f_tol, a, inv);
+        const float da = -m.f_a12 * dn * dt * (dn * dn - dt * dt) * inv;
+        return a * (a * dn - da * dt);
+    }
+    static __device__ __forceinline__ float yface(const Fast32& m, float dn, float d1, float c, float e) {
+        const float dt = 0.25f * ((d1 + c) - e);
+        float a, inv;
+        aniso(dt, dn, m.f_a_bar, m.f_a1pe, m.f_2ae, m.f_tol, a, inv);
+        const float da = -m.f_a12 * dt * dn * (dt * dt - dn * dn) * inv;
+        return a * (a * dn + da * dt);
+    }
+    static __device__ __forceinline__ void cell(const Fast32& m, float jr, float jl, float jt, float jb, float p,
+                                                float cdx, float cdy, float uc, float ul, float ur, float up,
+                                                float um, float& kphi, float& ku) {
+        const float flux = ((jr - jl) + (jt - jb)) * m.inv_h2_flux;
+        const float g_prime = p * p * p - p;
+        const float one_m_p2 = 1.0f - p * p;
+        const float p_prime = one_m_p2 * one_m_p2;
+        float a, inv;
+        aniso(0.5f * cdx, 0.5f * cdy, m.c_a_bar, m.c_a1pe, m.c_2ae, m.c_tol, a, inv);
+        kphi = ((flux - g_prime) - m.lambda * uc * p_prime) * rcp_approx(a * a);
+        const float lap = ((ur + ul) - 2.0f * uc) * m.ih0 + ((up + um) - 2.0f * uc) * m.ih1;
+        ku = lap * m.d_thermal + 0.5f * kphi;
+    }
+    static __device__ __forceinline__ float axpy(float dt, float k, float x) { return x + dt * k; }
+    static __device__ __forceinline__ float add_noise(float x, float scale_amp, uint64_t key) {
+        return x + scale_amp * normal_fast32(key);
+    }
+    // Box-Muller from the reference's two uniforms (rng.rs:43-49), single
+    // precision: u keeps its full 53-bit tail (rounded to 24 bits), and
+    // cos(2 pi v) = -cos(2 pi (v - 1/2)) keeps the argument in [-pi, pi].
+    static __device__ __forceinline__ float normal_fast32(uint64_t key) {
+        const uint64_t a = splitmix64(key);
+        const uint64_t b = splitmix64(a ^ 0xD1B54A32D192ED03ull);
+        const float u = __ull2float_rn((a >> 11) + 1) * 0x1p-53f;
+        const float v = __ull2float_rn((b >> 11) + 1) * 0x1p-53f;
+        return -sqrtf(-2.0f * __logf(u)) * __cosf(6.28318530717958647692f * (v - 0.5f));
+    }
+};
+
+}  // namespace
+
+cudaError_t launch_modelc_tile_f32(const float* in, float* out, const CartTopo& topo, const SlabLayout& L,
+                                   const ModelCDev& m, double dt, const NoiseDev& nz, double* tdev, int slot,
+                                   int rows, cudaStream_t s) {
+    TileArgs g{topo, L, dt, nz.seed, tdev, slot, rows};
+    Fast32 f{};
+    f.lambda = (float)m.lambda;
+    f.d_thermal = (float)m.d_thermal;
+    f.inv_h2_flux = (float)m.inv_h2_flux;
+    f.ih0 = (float)m.inv_h2[0];
+    f.ih1 = (float)m.inv_h2[1];
+    f.f_a_bar = (float)m.f_a_bar;
+    f.f_a1pe = (float)(m.f_a_bar * (1.0 + m.f_eps_prime));
+    f.f_2ae = (float)(2.0 * m.f_a_bar * m.f_eps_prime);
+    f.f_a12 = (float)m.f_a12;
+    f.f_tol = (float)m.f_tol;
+    f.c_a_bar = (float)m.a_bar;
+    f.c_a1pe = (float)(m.a_bar * (1.0 + m.eps_prime));
+    f.c_2ae = (float)(2.0 * m.a_bar * m.eps_prime);
+    f.c_tol = (float)m.tol;
+    const float scale_amp = (float)(std::sqrt(dt) * nz.amp);
+    if (nz.on) return launch_tile_ops<float, OpsFast32, true, 3>(in, out, g, f, (float)dt, scale_amp, s);
+    return launch_tile_ops<float, OpsFast32, false, 3>(in, out, g, f, (float)dt, scale_amp, s);
+}
+
+}  // namespace lg

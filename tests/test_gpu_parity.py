@@ -253,3 +253,12 @@ def test_modelc_tile_ragged_blocks(sched, orc, block):
     sim, os_, _ = _modelc_pair(sched, orc, cells, block, [g], 0.0, 25)
     assert np.array_equal(sim.state.interior("phi"), os_.interior(0))
     assert np.array_equal(sim.state.interior("u"), os_.interior(1))
+
+
+def test_modelc_fp32_noisy_tracks_fp64_oracle(sched, orc):
+    # same counter-based noise realization in both precisions
+    sim, os_, _ = _modelc_pair(sched, orc, [64, 64], [32, 32], [(H, H, 10 * H)], 0.05, 300, dtype="f32")
+    phi = sim.state.interior("phi").astype(np.float64)
+    ref = os_.interior(0)
+    assert np.sqrt(np.mean((phi - ref) ** 2)) < 1e-4
+    assert np.max(np.abs(phi - ref)) < 2e-3
