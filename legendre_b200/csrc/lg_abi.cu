@@ -525,10 +525,10 @@ int lg_modelc_em_run(lg_state* st, const lg_modelc_params* p, double dt, uint64_
     snprintf(key, sizeof key, "modelc|%a|%a|%a|%a|%a|%a|dt=%a|seed=%llu|v=%d", p->eps4, p->lambda, p->d_thermal,
              p->noise_amplitude, p->anisotropy_tol, p->flux_tol, dt, (unsigned long long)seed, variant);
     // variant = kind + 1000 * rows: kind 0 library default, 1 one thread per
-    // cell in reference order, 2 column tile; rows fixes the tile height
+    // cell in reference order, 2 warp strips; rows fixes the strip height
     const int kind = variant % 1000, rows = variant / 1000;
     const bool tile = (kind == 0 || kind == 2) && lg::modelc_tile_supported(topo);
-    if (kind == 2 && !tile) return fail(ctx, LG_ERR_INVALID, "the column-tile kernel needs blocks at most 1024 wide");
+    if (kind == 2 && !tile) return fail(ctx, LG_ERR_INVALID, "the strip kernel needs a 2-D grid");
     auto step = [&]() -> int {
         cudaError_t e;
         const void* in = st->arena[st->cur];

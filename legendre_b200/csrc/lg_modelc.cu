@@ -43,23 +43,22 @@ struct OpsExact {
         ku = fma_t(acc, m.d_thermal, T(0.5) * kphi);
     }
     static __device__ __forceinline__ T axpy(T dt, T k, T x) { return x + dt * k; }
-    static __device__ __forceinline__ T add_noise(T x, T scale_amp, uint64_t key) {
-        return x + scale_amp * normal_t(key, T(0));
-    }
+    static __device__ __forceinline__ T noise(uint64_t key) { return normal_t(key, T(0)); }
+    static __device__ __forceinline__ T add_noise(T x, T scale_amp, T n) { return x + scale_amp * n; }
 };
 
 }  // namespace
 
-bool modelc_tile_supported(const CartTopo& topo) { return topo.D == 2 && topo.n[0] >= 1 && topo.n[0] <= 1024; }
+bool modelc_tile_supported(const CartTopo& topo) { return topo.D == 2 && topo.n[0] >= 1; }
 
 cudaError_t launch_modelc_tile_f64(const double* in, double* out, const CartTopo& topo, const SlabLayout& L,
                                    const ModelCDev& m, double dt, const NoiseDev& nz, double* tdev, int slot,
                                    int rows, cudaStream_t s) {
-    TileArgs g{topo, L, dt, nz.seed, tdev, slot, rows};
+    TileArgs g{topo, L, dt, nz.seed, tdev, slot, rows, 0, 0, 0};
     const MC<double> mc = to_mc<double>(m);
     const double scale_amp = std::sqrt(dt) * nz.amp;
-    if (nz.on) return launch_tile_ops<double, OpsExact<double>, true>(in, out, g, mc, dt, scale_amp, s);
-    return launch_tile_ops<double, OpsExact<double>, false>(in, out, g, mc, dt, scale_amp, s);
+    if (nz.on) return launch_strip_ops<double, OpsExact<double>, true>(in, out, g, mc, dt, scale_amp, s);
+    return launch_strip_ops<double, OpsExact<double>, false>(in, out, g, mc, dt, scale_amp, s);
 }
 
 }  // namespace lg

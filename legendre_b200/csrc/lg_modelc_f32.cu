@@ -69,9 +69,8 @@ struct OpsFast32 {
         ku = lap * m.d_thermal + 0.5f * kphi;
     }
     static __device__ __forceinline__ float axpy(float dt, float k, float x) { return x + dt * k; }
-    static __device__ __forceinline__ float add_noise(float x, float scale_amp, uint64_t key) {
-        return x + scale_amp * normal_fast32(key);
-    }
+    static __device__ __forceinline__ float noise(uint64_t key) { return normal_fast32(key); }
+    static __device__ __forceinline__ float add_noise(float x, float scale_amp, float n) { return x + scale_amp * n; }
     // Box-Muller from the reference's two uniforms (rng.rs:43-49), single
     // precision: u keeps its full 53-bit tail (rounded to 24 bits), and
     // cos(2 pi v) = -cos(2 pi (v - 1/2)) keeps the argument in [-pi, pi].
@@ -89,7 +88,7 @@ struct OpsFast32 {
 cudaError_t launch_modelc_tile_f32(const float* in, float* out, const CartTopo& topo, const SlabLayout& L,
                                    const ModelCDev& m, double dt, const NoiseDev& nz, double* tdev, int slot,
                                    int rows, cudaStream_t s) {
-    TileArgs g{topo, L, dt, nz.seed, tdev, slot, rows};
+    TileArgs g{topo, L, dt, nz.seed, tdev, slot, rows, 0, 0, 0};
     Fast32 f{};
     f.lambda = (float)m.lambda;
     f.d_thermal = (float)m.d_thermal;
@@ -106,8 +105,8 @@ cudaError_t launch_modelc_tile_f32(const float* in, float* out, const CartTopo& 
     f.c_2ae = (float)(2.0 * m.a_bar * m.eps_prime);
     f.c_tol = (float)m.tol;
     const float scale_amp = (float)(std::sqrt(dt) * nz.amp);
-    if (nz.on) return launch_tile_ops<float, OpsFast32, true, 3>(in, out, g, f, (float)dt, scale_amp, s);
-    return launch_tile_ops<float, OpsFast32, false, 3>(in, out, g, f, (float)dt, scale_amp, s);
+    if (nz.on) return launch_strip_ops<float, OpsFast32, true, 3>(in, out, g, f, (float)dt, scale_amp, s);
+    return launch_strip_ops<float, OpsFast32, false, 3>(in, out, g, f, (float)dt, scale_amp, s);
 }
 
 }  // namespace lg
