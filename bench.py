@@ -211,10 +211,13 @@ def main():
     ap.add_argument("--config", default="c2", choices=sorted(CONFIGS))
     ap.add_argument("--dtype", default="f64", choices=["f64", "f32"])
     ap.add_argument("--variant", type=int, default=0)
+    ap.add_argument("--noise", type=float, default=None, help="override the noise amplitude b")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
-    cfg = CONFIGS[args.config]
+    cfg = dict(CONFIGS[args.config])
+    if args.noise is not None:
+        cfg["noise"] = args.noise
     if args.impl == "reference":
         run_reference(args, cfg)
         return

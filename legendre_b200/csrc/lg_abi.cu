@@ -494,7 +494,7 @@ int lg_modelc_em_run(lg_state* st, const lg_modelc_params* p, double dt, uint64_
     if (st->grid->D != 2 || st->nfields < 2 || st->ghosts[0] != 1 || st->ghosts[1] != 1)
         return fail(ctx, LG_ERR_STATE, "Model C needs a 2-D state with phi and u of ghost width 1");
     if (nsteps < 0) return fail(ctx, LG_ERR_INVALID, "negative step count");
-    if (variant < 0 || variant % 1000 > 2) return fail(ctx, LG_ERR_INVALID, "unknown kernel variant");
+    if (variant < 0 || variant % 1000 > 4) return fail(ctx, LG_ERR_INVALID, "unknown kernel variant");
     cudaSetDevice(ctx->device);
     if (!st->ghosts_valid) {
         int rc = fill_all_ghosts(st);
@@ -525,9 +525,11 @@ int lg_modelc_em_run(lg_state* st, const lg_modelc_params* p, double dt, uint64_
     snprintf(key, sizeof key, "modelc|%a|%a|%a|%a|%a|%a|dt=%a|seed=%llu|v=%d", p->eps4, p->lambda, p->d_thermal,
              p->noise_amplitude, p->anisotropy_tol, p->flux_tol, dt, (unsigned long long)seed, variant);
     // variant = kind + 1000 * rows: kind 0 library default, 1 one thread per
-    // cell in reference order, 2 warp strips; rows fixes the strip height
+    // cell in reference order, 2/3/4 warp strips with 2/3/4 CTAs per SM;
+    // rows fixes the strip height
     const int kind = variant % 1000, rows = variant / 1000;
-    const bool tile = (kind == 0 || kind == 2) && lg::modelc_tile_supported(topo);
+    const bool tile = kind != 1 && lg::modelc_tile_supported(topo);
+    const int minb = kind >= 2 ? kind : 2;
     if (kind == 2 && !tile) return fail(ctx, LG_ERR_INVALID, "the strip kernel needs a 2-D grid");
     auto step = [&]() -> int {
         cudaError_t e;
@@ -535,12 +537,12 @@ int lg_modelc_em_run(lg_state* st, const lg_modelc_params* p, double dt, uint64_
         void* out = st->arena[st->cur ^ 1];
         if (st->dtype == LG_F64)
             e = tile ? lg::launch_modelc_tile_f64(static_cast<const double*>(in), static_cast<double*>(out), topo, L,
-                                                  m, dt, nz, st->d_t, st->tslot, rows, ctx->stream)
+                                                  m, dt, nz, st->d_t, st->tslot, rows, minb, ctx->stream)
                      : lg::launch_modelc_step_f64(static_cast<const double*>(in), static_cast<double*>(out), topo, L,
                                                   m, dt, nz, st->d_t, st->tslot, variant, ctx->stream);
         else
             e = tile ? lg::launch_modelc_tile_f32(static_cast<const float*>(in), static_cast<float*>(out), topo, L,
-                                                  m, dt, nz, st->d_t, st->tslot, rows, ctx->stream)
+                                                  m, dt, nz, st->d_t, st->tslot, rows, minb, ctx->stream)
                      : lg::launch_modelc_step_f32(static_cast<const float*>(in), static_cast<float*>(out), topo, L, m,
                                                   dt, nz, st->d_t, st->tslot, variant, ctx->stream);
         ctx->launches++;

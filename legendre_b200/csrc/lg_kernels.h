@@ -49,17 +49,18 @@ cudaError_t launch_modelc_step_f32(const float* in, float* out, const CartTopo& 
                                    const ModelCDev& m, double dt, const NoiseDev& nz, double* tdev, int slot,
                                    int variant, cudaStream_t s);
 
-// Column-tile variants of the same steps (lg_modelc.cu): each face flux is
-// evaluated once and shared by its two cells; `rows` rows of one block per
-// CTA (0 = chosen from the grid).  Results are bit-identical to the
-// reference-order kernels above.
+// Warp-strip variants of the same steps (lg_modelc.cu, lg_modelc_f32.cu):
+// each face flux is evaluated once and shared by its two cells; `rows` rows
+// of one block per warp (0 = chosen from the grid); `minb` = CTAs per SM
+// the register allocation must allow (2, 3 or 4).  The FP64 results are
+// bit-identical to the reference-order kernel above.
 bool modelc_tile_supported(const CartTopo& topo);
 cudaError_t launch_modelc_tile_f64(const double* in, double* out, const CartTopo& topo, const SlabLayout& L,
                                    const ModelCDev& m, double dt, const NoiseDev& nz, double* tdev, int slot,
-                                   int rows, cudaStream_t s);
+                                   int rows, int minb, cudaStream_t s);
 cudaError_t launch_modelc_tile_f32(const float* in, float* out, const CartTopo& topo, const SlabLayout& L,
                                    const ModelCDev& m, double dt, const NoiseDev& nz, double* tdev, int slot,
-                                   int rows, cudaStream_t s);
+                                   int rows, int minb, cudaStream_t s);
 
 // Standard normals of a key array (tests of the generator).
 cudaError_t launch_standard_normal(const uint64_t* keys, double* out, int64_t n, cudaStream_t s);

@@ -87,7 +87,7 @@ struct OpsFast32 {
 
 cudaError_t launch_modelc_tile_f32(const float* in, float* out, const CartTopo& topo, const SlabLayout& L,
                                    const ModelCDev& m, double dt, const NoiseDev& nz, double* tdev, int slot,
-                                   int rows, cudaStream_t s) {
+                                   int rows, int minb, cudaStream_t s) {
     TileArgs g{topo, L, dt, nz.seed, tdev, slot, rows, 0, 0, 0};
     Fast32 f{};
     f.lambda = (float)m.lambda;
@@ -105,8 +105,8 @@ cudaError_t launch_modelc_tile_f32(const float* in, float* out, const CartTopo& 
     f.c_2ae = (float)(2.0 * m.a_bar * m.eps_prime);
     f.c_tol = (float)m.tol;
     const float scale_amp = (float)(std::sqrt(dt) * nz.amp);
-    if (nz.on) return launch_strip_ops<float, OpsFast32, true, 3>(in, out, g, f, (float)dt, scale_amp, s);
-    return launch_strip_ops<float, OpsFast32, false, 3>(in, out, g, f, (float)dt, scale_amp, s);
+    if (nz.on) return launch_strip_ops<float, OpsFast32, true>(in, out, g, f, (float)dt, scale_amp, minb, s);
+    return launch_strip_ops<float, OpsFast32, false>(in, out, g, f, (float)dt, scale_amp, minb, s);
 }
 
 }  // namespace lg

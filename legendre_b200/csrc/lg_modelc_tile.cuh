@@ -64,32 +64,36 @@ constexpr unsigned kFull = 0xffffffffu;
 // One row: x face left of the lane's column, y face above cell (c, j), the
 // cell update, stores and ghost pushes.  A, B, C = phi rows j-1, j, j+1; D
 // receives row j+2.  uA..uD = u at the lane's column for the same rows.
-template <class T, class Ops, bool NOISE>
+// `off` is the slab offset of (col, j); ph/uu/po/uo are the warp's slab
+// bases.  NX > 0 fixes the block width (and so the row stride) at compile
+// time; FULL means every lane owns a column.
+template <class T, class Ops, bool NOISE, int NX, bool FULL>
 __device__ __forceinline__ void strip_row(const typename Ops::Params& m, const TileArgs& g, int j, int r0, int lane,
-                                          int col, bool valid, int last_lane, int n0, int n1,
-                                          const T* __restrict__ phc, const T* __restrict__ uuc, T* __restrict__ out,
-                                          T* __restrict__ phi_o, T* __restrict__ u_o, const Nbr2& nb,
+                                          int col, bool valid, int last_lane, int n0, int n1, int off,
+                                          const T* __restrict__ ph, const T* __restrict__ uu, T* __restrict__ out,
+                                          T* __restrict__ po, T* __restrict__ uo, const Nbr2& nb, bool edge_x,
                                           uint64_t block_key, T bnd, Row3<T>& A, Row3<T>& B, Row3<T>& C,
                                           Row3<T>& D, T& uA, T& uB, T& uC, T& uD, T& jin, T& jout, T dt,
                                           T scale_amp) {
-    const int sy = g.L.gdim[0];
-    const int64_t rj = (int64_t)(j - r0) * sy;  // row j relative to the lane's column pointer at row r0
+    const int sy = NX > 0 ? NX + 2 : g.L.gdim[0];
+    const bool ok = FULL || valid;
     T ul = T(0), ur = T(0);
-    if (valid) {
+    if (ok) {
+        const T* q = ph + off;
+        const T* v = uu + off;
         if (j + 2 <= n1) {
-            const T* q = phc + rj + 2 * sy;
-            D.a = __ldg(q - 1);
-            D.b = __ldg(q);
-            D.c = __ldg(q + 1);
-            uD = __ldg(uuc + rj + 2 * sy);
+            D.a = __ldg(q + 2 * sy - 1);
+            D.b = __ldg(q + 2 * sy);
+            D.c = __ldg(q + 2 * sy + 1);
+            uD = __ldg(v + 2 * sy);
         }
-        ul = __ldg(uuc + rj - 1);
-        ur = __ldg(uuc + rj + 1);
+        ul = __ldg(v - 1);
+        ur = __ldg(v + 1);
     }
     T nval = T(0);
-    if (NOISE && valid) nval = Ops::noise(splitmix64(block_key ^ (uint64_t)(col + j * n0)));
+    if (NOISE && ok) nval = Ops::noise(splitmix64(block_key ^ (uint64_t)(col + j * n0)));
     T fl = T(0), jt = T(0);
-    if (valid) {
+    if (ok) {
         fl = Ops::xface(m, B.b - B.a, C.b - A.b, C.a, A.a);
         jt = Ops::yface(m, C.b - B.b, C.c - C.a, B.c, B.a);
     }
@@ -97,27 +101,31 @@ __device__ __forceinline__ void strip_row(const typename Ops::Params& m, const T
     T fr = __shfl_down_sync(kFull, fl, 1);
     const T fb = __shfl_sync(kFull, bnd, (j - r0) & 31);
     if (lane == last_lane) fr = fb;
-    if (valid) {
+    if (ok) {
         T kphi, ku;
         Ops::cell(m, fr, fl, jt, jin, B.b, B.c - B.a, C.b - A.b, uB, ul, ur, uC, uA, kphi, ku);
         T phin = Ops::axpy(dt, kphi, B.b);
         if (NOISE) phin = Ops::add_noise(phin, scale_amp, nval);
         const T un = Ops::axpy(dt, ku, uB);
-        phi_o[rj] = phin;
-        u_o[rj] = un;
-        push_ghosts_2d_g1(out, g.L, 0, nb, n0, n1, col, j, phin);
-        push_ghosts_2d_g1(out, g.L, 1, nb, n0, n1, col, j, un);
+        po[off] = phin;
+        uo[off] = un;
+        if (edge_x || j == 0 || j == n1 - 1) {  // warp-uniform: only warps on a block edge push ghosts
+            push_ghosts_2d_g1(out, g.L, 0, nb, n0, n1, col, j, phin);
+            push_ghosts_2d_g1(out, g.L, 1, nb, n0, n1, col, j, un);
+        }
         jout = jt;
     }
 }
 
-template <class T, class Ops, bool NOISE, int MINB>
+template <class T, class Ops, bool NOISE, int MINB, int NX>
 __global__ void __launch_bounds__(256, MINB)
     modelc_strip_kernel(const T* __restrict__ in, T* __restrict__ out, TileArgs g, typename Ops::Params m, T dt,
                         T scale_amp) {
+    constexpr bool FULL = NX > 0 && NX % 32 == 0;
     const CartTopo& topo = g.topo;
-    const int n0 = topo.n[0], n1 = topo.n[1];
-    const int sy = g.L.gdim[0];
+    const int n0 = NX > 0 ? NX : topo.n[0];
+    const int n1 = topo.n[1];
+    const int sy = NX > 0 ? NX + 2 : g.L.gdim[0];
     const int lane = threadIdx.x & 31;
     const int wpc = blockDim.x >> 5;
 
@@ -137,72 +145,67 @@ __global__ void __launch_bounds__(256, MINB)
         const int r1 = min(n1, r0 + g.rows);
         const int c0 = s * 32;
         const int col = c0 + lane;
-        const bool valid = col < n0;
+        const bool valid = FULL || col < n0;
         const int last_lane = min(31, n0 - 1 - c0);
         const int cr = c0 + last_lane;  // last column of the strip; its right face is the boundary face
+        const bool edge_x = s == 0 || s == g.strips - 1;
 
         const T* ph = in + slab_base(g.L, b, 0);
         const T* uu = in + slab_base(g.L, b, 1);
+        T* po = out + slab_base(g.L, b, 0);
+        T* uo = out + slab_base(g.L, b, 1);
         Nbr2 nb;
         nb.load(topo, b);
         uint64_t block_key = 0;
         if (NOISE)
             block_key = wiener_block_key(g.seed, (uint64_t)__double_as_longlong(tnow), kWienerStream0, (uint64_t)b);
 
-        // the lane's column pointers at (col, r0)
-        const int64_t o0 = (int64_t)(col + 1) + (int64_t)(r0 + 1) * sy;
-        const T* phc = ph + o0;
-        const T* uuc = uu + o0;
-        T* phi_o = out + slab_base(g.L, b, 0) + o0;
-        T* u_o = out + slab_base(g.L, b, 1) + o0;
-
         // right-boundary face of the strip for rows rb .. rb+31 (lane = row)
         auto boundary = [&](int rb) -> T {
             const int r = rb + lane;
             if (r >= r1) return T(0);
-            const T* q = ph + (cr + 1) + (int64_t)(r + 1) * sy;  // (column cr, row r)
+            const T* q = ph + (cr + 1) + (r + 1) * sy;  // (column cr, row r)
             const T c0m = __ldg(q - sy), c1m = __ldg(q - sy + 1);
             const T c00 = __ldg(q), c10 = __ldg(q + 1);
             const T c0p = __ldg(q + sy), c1p = __ldg(q + sy + 1);
             return Ops::xface(m, c10 - c00, c1p - c1m, c0p, c0m);
         };
 
+        int off = (col + 1) + (r0 + 1) * sy;  // slab offset of (col, r0)
         Row3<T> w0{}, w1{}, w2{}, w3{};
         T u0 = T(0), u1 = T(0), u2 = T(0), u3 = T(0);
         T ja = T(0), jb = T(0);
         if (valid) {
-            w0 = {__ldg(phc - sy - 1), __ldg(phc - sy), __ldg(phc - sy + 1)};
-            w1 = {__ldg(phc - 1), __ldg(phc), __ldg(phc + 1)};
-            w2 = {__ldg(phc + sy - 1), __ldg(phc + sy), __ldg(phc + sy + 1)};
-            u0 = __ldg(uuc - sy);
-            u1 = __ldg(uuc);
-            u2 = __ldg(uuc + sy);
+            const T* q = ph + off;
+            const T* v = uu + off;
+            w0 = {__ldg(q - sy - 1), __ldg(q - sy), __ldg(q - sy + 1)};
+            w1 = {__ldg(q - 1), __ldg(q), __ldg(q + 1)};
+            w2 = {__ldg(q + sy - 1), __ldg(q + sy), __ldg(q + sy + 1)};
+            u0 = __ldg(v - sy);
+            u1 = __ldg(v);
+            u2 = __ldg(v + sy);
             // y face below the first row (between r0-1 and r0)
             ja = Ops::yface(m, w1.b - w0.b, w1.c - w1.a, w0.c, w0.a);
         }
         T bnd = boundary(r0);
+#define LG_ROW(J, A_, B_, C_, D_, UA, UB, UC, UD, JI, JO)                                                          \
+    strip_row<T, Ops, NOISE, NX, FULL>(m, g, J, r0, lane, col, valid, last_lane, n0, n1, off, ph, uu, out, po, uo, \
+                                       nb, edge_x, block_key, bnd, A_, B_, C_, D_, UA, UB, UC, UD, JI, JO, dt,      \
+                                       scale_amp);                                                                  \
+    off += sy
         int j = r0;
         for (; j + 3 < r1; j += 4) {
             if (j != r0 && ((j - r0) & 31) == 0) bnd = boundary(j);
-            strip_row<T, Ops, NOISE>(m, g, j, r0, lane, col, valid, last_lane, n0, n1, phc, uuc, out, phi_o, u_o, nb,
-                                     block_key, bnd, w0, w1, w2, w3, u0, u1, u2, u3, ja, jb, dt, scale_amp);
-            strip_row<T, Ops, NOISE>(m, g, j + 1, r0, lane, col, valid, last_lane, n0, n1, phc, uuc, out, phi_o,
-                                     u_o, nb, block_key, bnd, w1, w2, w3, w0, u1, u2, u3, u0, jb, ja, dt, scale_amp);
-            strip_row<T, Ops, NOISE>(m, g, j + 2, r0, lane, col, valid, last_lane, n0, n1, phc, uuc, out, phi_o,
-                                     u_o, nb, block_key, bnd, w2, w3, w0, w1, u2, u3, u0, u1, ja, jb, dt, scale_amp);
-            strip_row<T, Ops, NOISE>(m, g, j + 3, r0, lane, col, valid, last_lane, n0, n1, phc, uuc, out, phi_o,
-                                     u_o, nb, block_key, bnd, w3, w0, w1, w2, u3, u0, u1, u2, jb, ja, dt, scale_amp);
+            LG_ROW(j, w0, w1, w2, w3, u0, u1, u2, u3, ja, jb);
+            LG_ROW(j + 1, w1, w2, w3, w0, u1, u2, u3, u0, jb, ja);
+            LG_ROW(j + 2, w2, w3, w0, w1, u2, u3, u0, u1, ja, jb);
+            LG_ROW(j + 3, w3, w0, w1, w2, u3, u0, u1, u2, jb, ja);
         }
         if (j < r1 && j != r0 && ((j - r0) & 31) == 0) bnd = boundary(j);
-        if (j < r1)
-            strip_row<T, Ops, NOISE>(m, g, j, r0, lane, col, valid, last_lane, n0, n1, phc, uuc, out, phi_o, u_o, nb,
-                                     block_key, bnd, w0, w1, w2, w3, u0, u1, u2, u3, ja, jb, dt, scale_amp);
-        if (j + 1 < r1)
-            strip_row<T, Ops, NOISE>(m, g, j + 1, r0, lane, col, valid, last_lane, n0, n1, phc, uuc, out, phi_o,
-                                     u_o, nb, block_key, bnd, w1, w2, w3, w0, u1, u2, u3, u0, jb, ja, dt, scale_amp);
-        if (j + 2 < r1)
-            strip_row<T, Ops, NOISE>(m, g, j + 2, r0, lane, col, valid, last_lane, n0, n1, phc, uuc, out, phi_o,
-                                     u_o, nb, block_key, bnd, w2, w3, w0, w1, u2, u3, u0, u1, ja, jb, dt, scale_amp);
+        if (j < r1) { LG_ROW(j, w0, w1, w2, w3, u0, u1, u2, u3, ja, jb); }
+        if (j + 1 < r1) { LG_ROW(j + 1, w1, w2, w3, w0, u1, u2, u3, u0, jb, ja); }
+        if (j + 2 < r1) { LG_ROW(j + 2, w2, w3, w0, w1, u2, u3, u0, u1, ja, jb); }
+#undef LG_ROW
     }
 }
 
@@ -221,9 +224,9 @@ inline int strip_rows(const CartTopo& topo, int strips, int rows) {
     return std::max(1, std::min(rows, n1));
 }
 
-template <class T, class Ops, bool NOISE, int MINB = 2>
-cudaError_t launch_strip_ops(const T* in, T* out, TileArgs g, const typename Ops::Params& m, T dt, T scale_amp,
-                             cudaStream_t s) {
+template <class T, class Ops, bool NOISE, int MINB>
+cudaError_t launch_strip_minb(const T* in, T* out, TileArgs g, const typename Ops::Params& m, T dt, T scale_amp,
+                              cudaStream_t s) {
     const int n0 = g.topo.n[0], n1 = g.topo.n[1];
     g.strips = (n0 + 31) / 32;
     g.rows = strip_rows(g.topo, g.strips, g.rows);
@@ -231,8 +234,26 @@ cudaError_t launch_strip_ops(const T* in, T* out, TileArgs g, const typename Ops
     g.units = (int64_t)g.topo.nblocks * g.strips * g.chunks;
     const int wpc = 8;
     const int64_t ctas = std::min<int64_t>((g.units + wpc - 1) / wpc, (int64_t)1 << 30);
-    modelc_strip_kernel<T, Ops, NOISE, MINB><<<(unsigned)ctas, wpc * 32, 0, s>>>(in, out, g, m, dt, scale_amp);
+    const dim3 grid((unsigned)ctas), block(wpc * 32);
+    switch (n0) {  // block widths of the shipped configurations get a compile-time row stride
+        case 32: modelc_strip_kernel<T, Ops, NOISE, MINB, 32><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp); break;
+        case 64: modelc_strip_kernel<T, Ops, NOISE, MINB, 64><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp); break;
+        case 126: modelc_strip_kernel<T, Ops, NOISE, MINB, 126><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp); break;
+        case 128: modelc_strip_kernel<T, Ops, NOISE, MINB, 128><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp); break;
+        case 256: modelc_strip_kernel<T, Ops, NOISE, MINB, 256><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp); break;
+        default: modelc_strip_kernel<T, Ops, NOISE, MINB, 0><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp);
+    }
     return cudaGetLastError();
+}
+
+// occupancy: CTAs of 256 threads per SM the register allocation must allow
+// (2: up to 128 registers, 3: 80, 4: 64)
+template <class T, class Ops, bool NOISE>
+cudaError_t launch_strip_ops(const T* in, T* out, TileArgs g, const typename Ops::Params& m, T dt, T scale_amp,
+                             int minb, cudaStream_t s) {
+    if (minb == 3) return launch_strip_minb<T, Ops, NOISE, 3>(in, out, g, m, dt, scale_amp, s);
+    if (minb == 4) return launch_strip_minb<T, Ops, NOISE, 4>(in, out, g, m, dt, scale_amp, s);
+    return launch_strip_minb<T, Ops, NOISE, 2>(in, out, g, m, dt, scale_amp, s);
 }
 
 }  // namespace lg
