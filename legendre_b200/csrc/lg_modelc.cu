@@ -57,8 +57,8 @@ cudaError_t launch_modelc_tile_f64(const double* in, double* out, const CartTopo
     TileArgs g{topo, L, dt, nz.seed, tdev, slot, rows, 0, 0, 0};
     const MC<double> mc = to_mc<double>(m);
     const double scale_amp = std::sqrt(dt) * nz.amp;
-    if (nz.on) return launch_strip_ops<double, OpsExact<double>, true>(in, out, g, mc, dt, scale_amp, minb, s);
-    return launch_strip_ops<double, OpsExact<double>, false>(in, out, g, mc, dt, scale_amp, minb, s);
+    if (nz.on) return launch_strip_ops<double, OpsExact<double>, true, 1>(in, out, g, mc, dt, scale_amp, minb, s);
+    return launch_strip_ops<double, OpsExact<double>, false, 1>(in, out, g, mc, dt, scale_amp, minb, s);
 }
 
 }  // namespace lg

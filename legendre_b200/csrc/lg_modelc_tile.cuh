@@ -62,33 +62,32 @@ struct Row3 {
 constexpr unsigned kFull = 0xffffffffu;
 
 // One row: x face left of the lane's column, y face above cell (c, j), the
-// cell update, stores and ghost pushes.  A, B, C = phi rows j-1, j, j+1; D
-// receives row j+2.  uA..uD = u at the lane's column for the same rows.
-// `off` is the slab offset of (col, j); ph/uu/po/uo are the warp's slab
-// bases.  NX > 0 fixes the block width (and so the row stride) at compile
-// time; FULL means every lane owns a column.
-template <class T, class Ops, bool NOISE, int NX, bool FULL>
+// cell update, stores and ghost pushes.  A, B, C = phi rows j-1, j, j+1 at
+// columns c-1, c, c+1; UA, UB, UC = u at column c for the same rows; P / UP
+// receive the prefetch of row j+1+PF.  `off` is the slab offset of (col, j); ph/uu/po/uo
+// are the warp's slab bases.  NX > 0 fixes the block width (and the row
+// stride) at compile time; FULL means every lane owns a column.
+template <class T, class Ops, bool NOISE, int NX, bool FULL, int PF>
 __device__ __forceinline__ void strip_row(const typename Ops::Params& m, const TileArgs& g, int j, int r0, int lane,
                                           int col, bool valid, int last_lane, int n0, int n1, int off,
                                           const T* __restrict__ ph, const T* __restrict__ uu, T* __restrict__ out,
                                           T* __restrict__ po, T* __restrict__ uo, const Nbr2& nb, bool edge_x,
-                                          uint64_t block_key, T bnd, Row3<T>& A, Row3<T>& B, Row3<T>& C,
-                                          Row3<T>& D, T& uA, T& uB, T& uC, T& uD, T& jin, T& jout, T dt,
+                                          uint64_t block_key, T bnd, const Row3<T>& A, const Row3<T>& B,
+                                          const Row3<T>& C, Row3<T>& P, T UA, T UB, T UC, T& UP, T& jb, T dt,
                                           T scale_amp) {
     const int sy = NX > 0 ? NX + 2 : g.L.gdim[0];
     const bool ok = FULL || valid;
     T ul = T(0), ur = T(0);
     if (ok) {
-        const T* q = ph + off;
-        const T* v = uu + off;
-        if (j + 2 <= n1) {
-            D.a = __ldg(q + 2 * sy - 1);
-            D.b = __ldg(q + 2 * sy);
-            D.c = __ldg(q + 2 * sy + 1);
-            uD = __ldg(v + 2 * sy);
+        if (j + 1 + PF <= n1) {
+            const T* q = ph + off + (1 + PF) * sy;
+            P.a = __ldg(q - 1);
+            P.b = __ldg(q);
+            P.c = __ldg(q + 1);
+            UP = __ldg(uu + off + (1 + PF) * sy);
         }
-        ul = __ldg(v - 1);
-        ur = __ldg(v + 1);
+        ul = __ldg(uu + off - 1);
+        ur = __ldg(uu + off + 1);
     }
     T nval = T(0);
     if (NOISE && ok) nval = Ops::noise(splitmix64(block_key ^ (uint64_t)(col + j * n0)));
@@ -103,25 +102,28 @@ __device__ __forceinline__ void strip_row(const typename Ops::Params& m, const T
     if (lane == last_lane) fr = fb;
     if (ok) {
         T kphi, ku;
-        Ops::cell(m, fr, fl, jt, jin, B.b, B.c - B.a, C.b - A.b, uB, ul, ur, uC, uA, kphi, ku);
+        Ops::cell(m, fr, fl, jt, jb, B.b, B.c - B.a, C.b - A.b, UB, ul, ur, UC, UA, kphi, ku);
         T phin = Ops::axpy(dt, kphi, B.b);
         if (NOISE) phin = Ops::add_noise(phin, scale_amp, nval);
-        const T un = Ops::axpy(dt, ku, uB);
+        const T un = Ops::axpy(dt, ku, UB);
         po[off] = phin;
         uo[off] = un;
         if (edge_x || j == 0 || j == n1 - 1) {  // warp-uniform: only warps on a block edge push ghosts
             push_ghosts_2d_g1(out, g.L, 0, nb, n0, n1, col, j, phin);
             push_ghosts_2d_g1(out, g.L, 1, nb, n0, n1, col, j, un);
         }
-        jout = jt;
+        jb = jt;
     }
 }
 
-template <class T, class Ops, bool NOISE, int MINB, int NX>
+// Rows per work unit are at most 32, so one batch of boundary faces (lanes
+// across rows) serves the whole unit.
+template <class T, class Ops, bool NOISE, int MINB, int NX, int PF>
 __global__ void __launch_bounds__(256, MINB)
     modelc_strip_kernel(const T* __restrict__ in, T* __restrict__ out, TileArgs g, typename Ops::Params m, T dt,
                         T scale_amp) {
     constexpr bool FULL = NX > 0 && NX % 32 == 0;
+    constexpr int NB = PF + 3;  // window rows: j-1, j, j+1 and PF rows of prefetch
     const CartTopo& topo = g.topo;
     const int n0 = NX > 0 ? NX : topo.n[0];
     const int n1 = topo.n[1];
@@ -160,71 +162,74 @@ __global__ void __launch_bounds__(256, MINB)
         if (NOISE)
             block_key = wiener_block_key(g.seed, (uint64_t)__double_as_longlong(tnow), kWienerStream0, (uint64_t)b);
 
-        // right-boundary face of the strip for rows rb .. rb+31 (lane = row)
-        auto boundary = [&](int rb) -> T {
-            const int r = rb + lane;
-            if (r >= r1) return T(0);
-            const T* q = ph + (cr + 1) + (r + 1) * sy;  // (column cr, row r)
-            const T c0m = __ldg(q - sy), c1m = __ldg(q - sy + 1);
-            const T c00 = __ldg(q), c10 = __ldg(q + 1);
-            const T c0p = __ldg(q + sy), c1p = __ldg(q + sy + 1);
-            return Ops::xface(m, c10 - c00, c1p - c1m, c0p, c0m);
-        };
-
         int off = (col + 1) + (r0 + 1) * sy;  // slab offset of (col, r0)
-        Row3<T> w0{}, w1{}, w2{}, w3{};
-        T u0 = T(0), u1 = T(0), u2 = T(0), u3 = T(0);
-        T ja = T(0), jb = T(0);
-        if (valid) {
-            const T* q = ph + off;
-            const T* v = uu + off;
-            w0 = {__ldg(q - sy - 1), __ldg(q - sy), __ldg(q - sy + 1)};
-            w1 = {__ldg(q - 1), __ldg(q), __ldg(q + 1)};
-            w2 = {__ldg(q + sy - 1), __ldg(q + sy), __ldg(q + sy + 1)};
-            u0 = __ldg(v - sy);
-            u1 = __ldg(v);
-            u2 = __ldg(v + sy);
-            // y face below the first row (between r0-1 and r0)
-            ja = Ops::yface(m, w1.b - w0.b, w1.c - w1.a, w0.c, w0.a);
+        Row3<T> w[NB];
+        T uw[NB];
+        T jb = T(0);
+        // window: rows r0-1 .. r0+PF in w[0..NB-2]; w[NB-1] is filled by the first row
+#pragma unroll
+        for (int q = 0; q < NB - 1; ++q) {
+            w[q] = Row3<T>{};
+            uw[q] = T(0);
+            const int r = r0 - 1 + q;
+            if (valid && r <= n1) {
+                const T* p = ph + off + (q - 1) * sy;
+                w[q] = {__ldg(p - 1), __ldg(p), __ldg(p + 1)};
+                uw[q] = __ldg(uu + off + (q - 1) * sy);
+            }
         }
-        T bnd = boundary(r0);
-#define LG_ROW(J, A_, B_, C_, D_, UA, UB, UC, UD, JI, JO)                                                          \
-    strip_row<T, Ops, NOISE, NX, FULL>(m, g, J, r0, lane, col, valid, last_lane, n0, n1, off, ph, uu, out, po, uo, \
-                                       nb, edge_x, block_key, bnd, A_, B_, C_, D_, UA, UB, UC, UD, JI, JO, dt,      \
-                                       scale_amp);                                                                  \
+        w[NB - 1] = Row3<T>{};
+        uw[NB - 1] = T(0);
+        // right-boundary face of the strip for rows r0 .. r0+31 (lane = row)
+        T bnd = T(0);
+        {
+            const int r = r0 + lane;
+            if (r < r1) {
+                const T* q = ph + (cr + 1) + (r + 1) * sy;  // (column cr, row r)
+                const T c0m = __ldg(q - sy), c1m = __ldg(q - sy + 1);
+                const T c00 = __ldg(q), c10 = __ldg(q + 1);
+                const T c0p = __ldg(q + sy), c1p = __ldg(q + sy + 1);
+                bnd = Ops::xface(m, c10 - c00, c1p - c1m, c0p, c0m);
+            }
+        }
+        // y face below the first row (between r0-1 and r0)
+        if (valid) jb = Ops::yface(m, w[1].b - w[0].b, w[1].c - w[1].a, w[0].c, w[0].a);
+
+#define LG_ROW(J, Q)                                                                                            \
+    strip_row<T, Ops, NOISE, NX, FULL, PF>(m, g, J, r0, lane, col, valid, last_lane, n0, n1, off, ph, uu, out, po,  \
+                                           uo, nb, edge_x, block_key, bnd, w[(Q) % NB], w[((Q) + 1) % NB],          \
+                                           w[((Q) + 2) % NB], w[((Q) + 2 + PF) % NB], uw[(Q) % NB],                \
+                                           uw[((Q) + 1) % NB], uw[((Q) + 2) % NB], uw[((Q) + 2 + PF) % NB], jb, dt, \
+                                           scale_amp);                                                              \
     off += sy
         int j = r0;
-        for (; j + 3 < r1; j += 4) {
-            if (j != r0 && ((j - r0) & 31) == 0) bnd = boundary(j);
-            LG_ROW(j, w0, w1, w2, w3, u0, u1, u2, u3, ja, jb);
-            LG_ROW(j + 1, w1, w2, w3, w0, u1, u2, u3, u0, jb, ja);
-            LG_ROW(j + 2, w2, w3, w0, w1, u2, u3, u0, u1, ja, jb);
-            LG_ROW(j + 3, w3, w0, w1, w2, u3, u0, u1, u2, jb, ja);
+        for (; j + NB <= r1; j += NB) {
+#pragma unroll
+            for (int q = 0; q < NB; ++q) { LG_ROW(j + q, q); }
         }
-        if (j < r1 && j != r0 && ((j - r0) & 31) == 0) bnd = boundary(j);
-        if (j < r1) { LG_ROW(j, w0, w1, w2, w3, u0, u1, u2, u3, ja, jb); }
-        if (j + 1 < r1) { LG_ROW(j + 1, w1, w2, w3, w0, u1, u2, u3, u0, jb, ja); }
-        if (j + 2 < r1) { LG_ROW(j + 2, w2, w3, w0, w1, u2, u3, u0, u1, ja, jb); }
+#pragma unroll
+        for (int q = 0; q < NB - 1; ++q) {
+            if (j + q < r1) { LG_ROW(j + q, q); }
+        }
 #undef LG_ROW
     }
 }
 
-// Rows per work unit: a multiple of 32 (boundary faces come in batches of
-// 32 rows), chosen so the grid holds several waves of warps on 148 SMs.
+// Rows per work unit: at most 32 (one batch of boundary faces per unit);
+// fewer only when the grid would otherwise hold too few warps.
 inline int strip_rows(const CartTopo& topo, int strips, int rows) {
     const int n1 = topo.n[1];
     if (rows <= 0) {
-        const int64_t want_units = (int64_t)148 * 48 * 4;
+        const int64_t want_units = (int64_t)148 * 48 * 2;
         const int64_t per_chunk = (int64_t)topo.nblocks * strips;
         const int chunks =
             (int)std::max<int64_t>(1, std::min<int64_t>(n1, (want_units + per_chunk - 1) / per_chunk));
-        rows = (n1 + chunks - 1) / chunks;
-        rows = std::max(32, (rows + 31) / 32 * 32);
+        rows = std::max(8, (n1 + chunks - 1) / chunks);
     }
-    return std::max(1, std::min(rows, n1));
+    return std::max(1, std::min(std::min(rows, 32), n1));
 }
 
-template <class T, class Ops, bool NOISE, int MINB>
+template <class T, class Ops, bool NOISE, int MINB, int PF>
 cudaError_t launch_strip_minb(const T* in, T* out, TileArgs g, const typename Ops::Params& m, T dt, T scale_amp,
                               cudaStream_t s) {
     const int n0 = g.topo.n[0], n1 = g.topo.n[1];
@@ -236,24 +241,25 @@ cudaError_t launch_strip_minb(const T* in, T* out, TileArgs g, const typename Op
     const int64_t ctas = std::min<int64_t>((g.units + wpc - 1) / wpc, (int64_t)1 << 30);
     const dim3 grid((unsigned)ctas), block(wpc * 32);
     switch (n0) {  // block widths of the shipped configurations get a compile-time row stride
-        case 32: modelc_strip_kernel<T, Ops, NOISE, MINB, 32><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp); break;
-        case 64: modelc_strip_kernel<T, Ops, NOISE, MINB, 64><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp); break;
-        case 126: modelc_strip_kernel<T, Ops, NOISE, MINB, 126><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp); break;
-        case 128: modelc_strip_kernel<T, Ops, NOISE, MINB, 128><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp); break;
-        case 256: modelc_strip_kernel<T, Ops, NOISE, MINB, 256><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp); break;
-        default: modelc_strip_kernel<T, Ops, NOISE, MINB, 0><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp);
+        case 32: modelc_strip_kernel<T, Ops, NOISE, MINB, 32, PF><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp); break;
+        case 64: modelc_strip_kernel<T, Ops, NOISE, MINB, 64, PF><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp); break;
+        case 126: modelc_strip_kernel<T, Ops, NOISE, MINB, 126, PF><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp); break;
+        case 128: modelc_strip_kernel<T, Ops, NOISE, MINB, 128, PF><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp); break;
+        case 256: modelc_strip_kernel<T, Ops, NOISE, MINB, 256, PF><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp); break;
+        default: modelc_strip_kernel<T, Ops, NOISE, MINB, 0, PF><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp);
     }
     return cudaGetLastError();
 }
 
 // occupancy: CTAs of 256 threads per SM the register allocation must allow
 // (2: up to 128 registers, 3: 80, 4: 64)
-template <class T, class Ops, bool NOISE>
+// PF: rows of prefetch ahead of the row being computed
+template <class T, class Ops, bool NOISE, int PF>
 cudaError_t launch_strip_ops(const T* in, T* out, TileArgs g, const typename Ops::Params& m, T dt, T scale_amp,
                              int minb, cudaStream_t s) {
-    if (minb == 3) return launch_strip_minb<T, Ops, NOISE, 3>(in, out, g, m, dt, scale_amp, s);
-    if (minb == 4) return launch_strip_minb<T, Ops, NOISE, 4>(in, out, g, m, dt, scale_amp, s);
-    return launch_strip_minb<T, Ops, NOISE, 2>(in, out, g, m, dt, scale_amp, s);
+    if (minb == 3) return launch_strip_minb<T, Ops, NOISE, 3, PF>(in, out, g, m, dt, scale_amp, s);
+    if (minb == 4) return launch_strip_minb<T, Ops, NOISE, 4, PF>(in, out, g, m, dt, scale_amp, s);
+    return launch_strip_minb<T, Ops, NOISE, 2, PF>(in, out, g, m, dt, scale_amp, s);
 }
 
 }  // namespace lg
