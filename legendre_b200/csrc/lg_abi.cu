@@ -529,7 +529,7 @@ int lg_modelc_em_run(lg_state* st, const lg_modelc_params* p, double dt, uint64_
     // rows fixes the strip height
     const int kind = variant % 1000, rows = variant / 1000;
     const bool tile = kind != 1 && lg::modelc_tile_supported(topo);
-    const int minb = kind >= 2 ? kind : 2;
+    const int minb = kind >= 2 ? kind : (st->dtype == LG_F32 ? 3 : 2);
     if (kind == 2 && !tile) return fail(ctx, LG_ERR_INVALID, "the strip kernel needs a 2-D grid");
     auto step = [&]() -> int {
         cudaError_t e;

@@ -105,8 +105,8 @@ cudaError_t launch_modelc_tile_f32(const float* in, float* out, const CartTopo& 
     f.c_2ae = (float)(2.0 * m.a_bar * m.eps_prime);
     f.c_tol = (float)m.tol;
     const float scale_amp = (float)(std::sqrt(dt) * nz.amp);
-    if (nz.on) return launch_strip_ops<float, OpsFast32, true, 2>(in, out, g, f, (float)dt, scale_amp, minb, s);
-    return launch_strip_ops<float, OpsFast32, false, 2>(in, out, g, f, (float)dt, scale_amp, minb, s);
+    if (nz.on) return launch_strip_ops<float, OpsFast32, true, 1>(in, out, g, f, (float)dt, scale_amp, minb, s);
+    return launch_strip_ops<float, OpsFast32, false, 1>(in, out, g, f, (float)dt, scale_amp, minb, s);
 }
 
 }  // namespace lg
