@@ -71,12 +71,12 @@ def build_library(force: bool = False, verbose: bool = False) -> Path:
 
 
 def build_oracle(force: bool = False) -> Path:
-    src = ORACLE_DIR / "legendre_oracle.cpp"
-    deps = [src, ORACLE_DIR / "legendre_oracle.h"]
+    srcs = [ORACLE_DIR / "legendre_oracle.cpp", ORACLE_DIR / "legendre_oracle_amr.cpp"]
+    deps = srcs + [ORACLE_DIR / "legendre_oracle.h", ORACLE_DIR / "oracle_core.hpp"]
     if not force and not _stale(ORACLE_LIB, deps):
         return ORACLE_LIB
     cxx = shutil.which("g++") or "g++"
-    _run([cxx, "-O2", "-std=c++17", "-ffp-contract=off", "-fopenmp", "-fPIC", "-shared", str(src),
+    _run([cxx, "-O2", "-std=c++17", "-ffp-contract=off", "-fopenmp", "-fPIC", "-shared", *map(str, srcs),
           "-o", str(ORACLE_LIB)])
     return ORACLE_LIB
 

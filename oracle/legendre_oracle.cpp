@@ -17,47 +17,11 @@
 // mirroring `RayonScheduler` (src/core/scheduler.rs:65-84): blocks are
 // disjoint, so results are identical for every thread count.
 
-#include <algorithm>
-#include <cmath>
-#include <cstdint>
-#include <cstring>
-#include <vector>
-#ifdef _OPENMP
-#include <omp.h>
-#endif
-
-#include "legendre_oracle.h"
+#include "oracle_core.hpp"
 
 namespace {
 
-// ---------------------------------------------------------------- rng ------
-// src/util/rng.rs:13-18
-inline uint64_t splitmix64(uint64_t z) {
-    z += 0x9E3779B97F4A7C15ull;
-    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
-    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
-    return z ^ (z >> 31);
-}
-// src/util/rng.rs:23-29
-inline uint64_t mix_key(uint64_t seed, const uint64_t* parts, size_t n) {
-    uint64_t s = splitmix64(seed);
-    for (size_t i = 0; i < n; ++i) s = splitmix64(s ^ parts[i]);
-    return s;
-}
-// src/util/rng.rs:35-37
-inline double unit_open(uint64_t bits) {
-    return (double)((bits >> 11) + 1) * (1.0 / 9007199254740992.0);
-}
-// std::f64::consts::TAU
-constexpr double kTau = 6.283185307179586476925286766559;
-// src/util/rng.rs:43-49
-inline double standard_normal(uint64_t key) {
-    uint64_t a = splitmix64(key);
-    uint64_t b = splitmix64(a ^ 0xD1B54A32D192ED03ull);
-    double u = unit_open(a);
-    double v = unit_open(b);
-    return std::sqrt(-2.0 * std::log(u)) * std::cos(kTau * v);
-}
+using namespace orc;
 
 // --------------------------------------------------------- Cartesian ------
 // src/geometry/cartesian.rs:28-187
@@ -133,29 +97,17 @@ struct Grid {
     }
 };
 
-// Visit every index of the half-open box lo..hi, dimension 0 fastest
-// (cartesian.rs:338-358).
-template <class F>
-void for_each_box(int D, const int64_t* lo, const int64_t* hi, F f) {
-    for (int d = 0; d < D; ++d)
-        if (lo[d] >= hi[d]) return;
-    int64_t idx[3] = {lo[0], D > 1 ? lo[1] : 0, D > 2 ? lo[2] : 0};
-    for (;;) {
-        f(idx);
-        int d = 0;
-        for (;;) {
-            idx[d] += 1;
-            if (idx[d] < hi[d]) break;
-            idx[d] = lo[d];
-            if (++d == D) return;
-        }
-    }
-}
-
 template <class F>
 void for_each_interior(const Grid& g, F f) {
     int64_t lo[3] = {0, 0, 0};
     for_each_box(g.D, lo, g.block, f);
+}
+
+Ext ext_of(const Grid& g) {
+    Ext e;
+    e.D = g.D;
+    for (int d = 0; d < 3; ++d) e.n[d] = g.block[d];
+    return e;
 }
 
 // Block-major state: blocks x fields, each slab ghost-inclusive
@@ -219,36 +171,6 @@ void fill_ghosts_mirror(const Grid& grid, State& st, int f) {
     }
 }
 
-// src/discretization/finite_difference.rs:49-67 ; output interior only
-void central_laplacian(const Grid& grid, const std::vector<double>& in, std::vector<double>& out, int g) {
-    double inv_h2[3];
-    for (int d = 0; d < grid.D; ++d) inv_h2[d] = 1.0 / (grid.spacing[d] * grid.spacing[d]);
-    for_each_interior(grid, [&](const int64_t* idx) {
-        double center = in[grid.linearize(idx, g)];
-        double acc = 0.0;
-        for (int d = 0; d < grid.D; ++d) {
-            int64_t p[3] = {idx[0], idx[1], idx[2]}, m[3] = {idx[0], idx[1], idx[2]};
-            p[d] += 1;
-            m[d] -= 1;
-            acc += ((in[grid.linearize(p, g)] - (center + center)) + in[grid.linearize(m, g)]) * inv_h2[d];
-        }
-        out[grid.linearize(idx, g)] = acc;
-    });
-}
-
-template <class F>
-void parallel_blocks(int64_t nblocks, int nthreads, F f) {
-#ifdef _OPENMP
-    if (nthreads > 1) {
-#pragma omp parallel for schedule(dynamic, 1) num_threads(nthreads)
-        for (int64_t b = 0; b < nblocks; ++b) f(b);
-        return;
-    }
-#endif
-    (void)nthreads;
-    for (int64_t b = 0; b < nblocks; ++b) f(b);
-}
-
 // ------------------------------------------------------------- heat -------
 // examples/heat3d.rs:41-85 (Heat3 / tests/heat3d.rs Heat<D>): u registered
 // with ghost 1; drift = CentralLaplacian(u) then *= kappa (heat3d.rs:76-78).
@@ -258,123 +180,16 @@ double heat_run(const Grid& grid, State& st, int f, double kappa, double t, doub
                 int nthreads) {
     int g = st.ghost[f];
     std::vector<std::vector<double>> k(grid.num_blocks(), std::vector<double>(grid.block_len(g), 0.0));
+    const Ext e = ext_of(grid);
     for (int64_t s = 0; s < steps; ++s) {
         fill_ghosts_mirror(grid, st, f);
         parallel_blocks(grid.num_blocks(), nthreads, [&](int64_t b) {
-            central_laplacian(grid, st.slab[b][f], k[b], g);
-            for_each_interior(grid, [&](const int64_t* idx) {
-                int64_t o = grid.linearize(idx, g);
-                k[b][o] = k[b][o] * kappa;
-            });
+            heat_drift_block(e, grid.spacing, kappa, st.slab[b][f].data(), k[b].data());
         });
-        parallel_blocks(grid.num_blocks(), nthreads, [&](int64_t b) {
-            std::vector<double>& x = st.slab[b][f];
-            const std::vector<double>& y = k[b];
-            for (size_t i = 0; i < x.size(); ++i) x[i] += dt * y[i];
-        });
+        parallel_blocks(grid.num_blocks(), nthreads, [&](int64_t b) { apply_time(st.slab[b][f], k[b], dt); });
         t += dt;  // src/core/simulation.rs:285
     }
     return t;
-}
-
-// ---------------------------------------------------------- Model C -------
-struct ModelC {
-    double eps4, lambda, d_thermal, noise_amplitude, tol;
-    double a_bar, eps_prime;        // model (phasefield.rs:100-116)
-    double f_a_bar, f_eps_prime, f_a12, f_tol;  // flux (finite_volume.rs:113-122)
-};
-
-ModelC make_model(const orc_modelc_params* p) {
-    ModelC m;
-    m.eps4 = p->eps4;
-    m.lambda = p->lambda;
-    m.d_thermal = p->d_thermal;
-    m.noise_amplitude = p->noise_amplitude;
-    m.tol = p->anisotropy_tol;
-    m.a_bar = std::fma(3.0, -m.eps4, 1.0);
-    m.eps_prime = 3.0 * m.eps4 / m.a_bar;
-    m.f_a_bar = std::fma(3.0, -m.eps4, 1.0);
-    m.f_eps_prime = 3.0 * m.eps4 / m.f_a_bar;
-    m.f_a12 = 4.0 * m.f_a_bar * m.f_eps_prime;
-    m.f_tol = p->flux_tol;
-    return m;
-}
-
-// finite_volume.rs:129-142
-inline void kr_face(const ModelC& m, double dx, double dy, double* a, double* da) {
-    double dx2 = dx * dx;
-    double dy2 = dy * dy;
-    double sum = dx2 + dy2;
-    double mag2 = sum * sum;
-    if (mag2 <= m.f_tol) {
-        *a = m.f_a_bar;
-        *da = 0.0;
-    } else {
-        *a = m.f_a_bar * (1.0 + m.f_eps_prime * (dx2 * dx2 + dy2 * dy2) / mag2);
-        *da = -(m.f_a12) * dx * dy * (dx2 - dy2) / mag2;
-    }
-}
-
-// phasefield.rs:159-175
-inline double center_anisotropy(const ModelC& m, const double* p, int64_t sx, int64_t sy, int64_t o) {
-    double dx = 0.5 * (p[o + sx] - p[o - sx]);
-    double dy = 0.5 * (p[o + sy] - p[o - sy]);
-    double dx2 = dx * dx;
-    double dy2 = dy * dy;
-    double sum = dx2 + dy2;
-    double mag2 = sum * sum;
-    if (mag2 <= m.tol) return m.a_bar;
-    return m.a_bar * (1.0 + m.eps_prime * (dx2 * dx2 + dy2 * dy2) / mag2);
-}
-
-// ModelC::vector_field_block(Driver::Time) on CartesianGrid<2>
-// (phasefield.rs:367-421): KarmaRappelFlux::kernel (finite_volume.rs:248-285)
-// into dphi, the local-term loop (phasefield.rs:393-404), the u Laplacian and
-// the coupling (phasefield.rs:412-421).  Interior entries of kphi/ku only.
-void modelc_drift_block(const Grid& grid, const ModelC& m, const std::vector<double>& phi,
-                        const std::vector<double>& u, std::vector<double>& kphi, std::vector<double>& ku) {
-    const int g = 1;
-    const int64_t sx = 1, sy = grid.block[0] + 2 * g;
-    const double* p = phi.data();
-    double inv_h2 = 1.0 / (grid.spacing[0] * grid.spacing[1]);
-    double quarter = 0.25;
-    for_each_interior(grid, [&](const int64_t* idx) {
-        int64_t o = grid.linearize(idx, g);
-        auto P = [&](int di, int dj) { return p[o + di * sx + dj * sy]; };
-        double derx_r = P(1, 0) - P(0, 0);
-        double derx_l = P(0, 0) - P(-1, 0);
-        double derx_t = quarter * (P(1, 1) - P(-1, 1) + P(1, 0) - P(-1, 0));
-        double derx_b = quarter * (P(1, 0) - P(-1, 0) + P(1, -1) - P(-1, -1));
-        double dery_t = P(0, 1) - P(0, 0);
-        double dery_b = P(0, 0) - P(0, -1);
-        double dery_r = quarter * (P(1, 1) - P(1, -1) + P(0, 1) - P(0, -1));
-        double dery_l = quarter * (P(0, 1) - P(0, -1) + P(-1, 1) - P(-1, -1));
-        double a_r, da_r, a_l, da_l, a_t, da_t, a_b, da_b;
-        kr_face(m, derx_r, dery_r, &a_r, &da_r);
-        kr_face(m, derx_l, dery_l, &a_l, &da_l);
-        kr_face(m, derx_t, dery_t, &a_t, &da_t);
-        kr_face(m, derx_b, dery_b, &a_b, &da_b);
-        double j_r = a_r * (a_r * derx_r - da_r * dery_r);
-        double j_l = a_l * (a_l * derx_l - da_l * dery_l);
-        double j_t = a_t * (a_t * dery_t + da_t * derx_t);
-        double j_b = a_b * (a_b * dery_b + da_b * derx_b);
-        kphi[o] = (j_r - j_l + j_t - j_b) * inv_h2;
-    });
-    for_each_interior(grid, [&](const int64_t* idx) {
-        int64_t o = grid.linearize(idx, g);
-        double pv = p[o];
-        double g_prime = std::fma(pv * pv, pv, -pv);
-        double one_m_p2 = std::fma(pv, -pv, 1.0);
-        double p_prime = one_m_p2 * one_m_p2;
-        double a = center_anisotropy(m, p, sx, sy, o);
-        double val = std::fma(m.lambda * u[o], -p_prime, kphi[o] - g_prime) / (a * a);
-        kphi[o] = val;
-    });
-    central_laplacian(grid, u, ku, g);
-    for_each_interior(grid, [&](const int64_t* idx) {
-        int64_t o = grid.linearize(idx, g);
-        ku[o] = std::fma(ku[o], m.d_thermal, 0.5 * kphi[o]);
-    });
 }
 
 // EulerMaruyama::step (src/integrators/euler_maruyama.rs:34-75) with
@@ -392,8 +207,10 @@ double modelc_run(const Grid& grid, State& st, const ModelC& m, double t, double
         // StepCtx::eval_drift (integrators/mod.rs:190-198)
         fill_ghosts_mirror(grid, st, 0);
         fill_ghosts_mirror(grid, st, 1);
+        const Ext e = ext_of(grid);
         parallel_blocks(nb, nthreads, [&](int64_t b) {
-            modelc_drift_block(grid, m, st.slab[b][0], st.slab[b][1], kphi[b], ku[b]);
+            modelc_drift_block(e, grid.spacing, m, st.slab[b][0].data(), st.slab[b][1].data(), kphi[b].data(),
+                               ku[b].data());
         });
         if (wiener) {
             // eval_tendency_impl: fill_zero then amp_phi = b on the interior
@@ -404,30 +221,11 @@ double modelc_run(const Grid& grid, State& st, const ModelC& m, double t, double
             });
         }
         // State::apply_step_with (state.rs:656-699), salt = t.to_bits()
-        uint64_t salt;
-        std::memcpy(&salt, &t, sizeof salt);
+        const uint64_t salt = bits_of(t);
         parallel_blocks(nb, nthreads, [&](int64_t b) {
-            // Driver::Time (driver.rs:131-138) over phi then u
-            for (int f = 0; f < 2; ++f) {
-                std::vector<double>& x = st.slab[b][f];
-                const std::vector<double>& v = f == 0 ? kphi[b] : ku[b];
-                for (int64_t i = 0; i < len; ++i) x[i] += dt * v[i];
-            }
-            if (wiener) {
-                // Driver::Wiener(0) (driver.rs:139-158)
-                double scale = std::sqrt(dt);
-                uint64_t parts[3] = {salt, (1ull << 32) | 0ull, (uint64_t)b};
-                uint64_t block_key = mix_key(seed, parts, 3);
-                std::vector<double>& x = st.slab[b][0];
-                const std::vector<double>& v = amp[b];
-                for (int64_t i = 0; i < len; ++i) {
-                    if (v[i] == 0.0) continue;
-                    uint64_t cell;
-                    if (!grid.cell_key(1, i, &cell)) continue;
-                    uint64_t key = splitmix64(block_key ^ cell);
-                    x[i] += scale * v[i] * standard_normal(key);
-                }
-            }
+            apply_time(st.slab[b][0], kphi[b], dt);  // Driver::Time over phi then u
+            apply_time(st.slab[b][1], ku[b], dt);
+            if (wiener) apply_wiener(e, 1, st.slab[b][0], amp[b], dt, seed, salt, (uint64_t)b);
         });
         t += dt;
     }
@@ -571,9 +369,10 @@ void orc_modelc_drift(const void* grid, void* s, const orc_modelc_params* p, dou
     State& st = *static_cast<State*>(s);
     ModelC m = make_model(p);
     int64_t len = g.block_len(1);
+    const Ext e = ext_of(g);
     for (int64_t b = 0; b < g.num_blocks(); ++b) {
         std::vector<double> kp(len, 0.0), ku(len, 0.0);
-        modelc_drift_block(g, m, st.slab[b][0], st.slab[b][1], kp, ku);
+        modelc_drift_block(e, g.spacing, m, st.slab[b][0].data(), st.slab[b][1].data(), kp.data(), ku.data());
         std::memcpy(kphi_out + b * len, kp.data(), len * sizeof(double));
         std::memcpy(ku_out + b * len, ku.data(), len * sizeof(double));
     }

@@ -171,3 +171,144 @@ class State:
 def modelc_params(eps4=0.06, lam=3.19, d_thermal=None, noise=0.0, tol=1e-8, flux_tol=1e-8):
     """ModelC::new (phasefield.rs:100-116): d_thermal = A2 * lambda unless given."""
     return Params(eps4, lam, 0.6267 * lam if d_thermal is None else d_thermal, noise, tol, flux_tol)
+
+
+# ----------------------------------------------------------------- AMR ---
+def _amr_sigs():
+    p, i64, u64, d = C.c_void_p, C.c_int64, C.c_uint64, C.c_double
+    pd, pi64 = C.POINTER(C.c_double), C.POINTER(C.c_int64)
+    sigs = {
+        "orc_cluster": (i64, [C.c_int, pi64, i64, d, i64, pi64, i64]),
+        "orc_amr_sim_create": (p, [pi64, pi64, pd, pd, C.POINTER(C.c_uint32), C.c_int, pi64, i64, C.c_int,
+                                   C.POINTER(Params), d, C.c_int, u64, C.c_int, pd, C.POINTER(C.c_int)]),
+        "orc_amr_sim_destroy": (None, [p]),
+        "orc_amr_sim_set_threads": (None, [p, C.c_int]),
+        "orc_amr_sim_num_blocks": (i64, [p]),
+        "orc_amr_sim_num_levels": (C.c_int, [p]),
+        "orc_amr_sim_epoch": (i64, [p]),
+        "orc_amr_sim_patch": (None, [p, i64, pi64]),
+        "orc_amr_sim_field_len": (i64, [p]),
+        "orc_amr_sim_get_field": (None, [p, C.c_int, pd]),
+        "orc_amr_sim_set_field": (None, [p, C.c_int, pd]),
+        "orc_amr_sim_step": (d, [p, d, i64]),
+        "orc_amr_sim_suggested_dt": (d, [p]),
+        "orc_amr_sim_restrict": (None, [p, C.c_int]),
+        "orc_amr_sim_fill_ghosts": (None, [p, C.c_int]),
+        "orc_amr_sim_tag": (i64, [p, C.c_int, d, C.c_int, pi64, i64]),
+        "orc_amr_sim_cell_center": (None, [p, i64, pi64, pd]),
+    }
+    for name, (res, args) in sigs.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+
+
+_amr_sigs()
+
+
+def cluster(flags, efficiency, min_width):
+    """Berger-Rigoutsos boxes [(lo, hi)] of flagged cells (list of tuples)."""
+    D = len(flags[0]) if flags else 2
+    arr = np.ascontiguousarray(np.array(flags, dtype=np.int64).reshape(-1, D) if flags else np.zeros((0, D), np.int64))
+    cap = max(1, len(flags))
+    out = np.zeros(cap * 2 * D, dtype=np.int64)
+    n = lib.orc_cluster(D, arr.ctypes.data_as(C.POINTER(C.c_int64)), len(flags), efficiency, min_width,
+                        out.ctypes.data_as(C.POINTER(C.c_int64)), cap)
+    return [(tuple(out[i * 2 * D:i * 2 * D + D]), tuple(out[i * 2 * D + D:(i + 1) * 2 * D])) for i in range(n)]
+
+
+class AmrSim:
+    """The oracle's Simulation on an AmrGrid<2> (heat or Model C, subcycled
+    or global dt, optional Berger-Oliger policy)."""
+
+    def __init__(self, cells, block, h, ratios, patches=(), model="heat", params=None, kappa=0.7,
+                 integrator="subcycling", seed=0, wiener=False, policy=None, origin=(0.0, 0.0)):
+        pa = np.array([[lv, *lo, *hi] for lv, lo, hi in patches], dtype=np.int64).reshape(-1, 5)
+        err = C.c_int(0)
+        pol = None
+        if policy is not None:
+            pol = (C.c_double * 6)(policy["every"], policy["buffer"], policy["efficiency"], policy["min_width"],
+                                   policy["threshold"], policy.get("field", 0))
+        self.h = lib.orc_amr_sim_create(
+            (C.c_int64 * 2)(*cells), (C.c_int64 * 2)(*block), (C.c_double * 2)(*origin), (C.c_double * 2)(h, h),
+            (C.c_uint32 * len(ratios))(*ratios), len(ratios), pa.ctypes.data_as(C.POINTER(C.c_int64)), len(pa),
+            0 if model == "heat" else 1, C.byref(params) if params is not None else None, kappa,
+            0 if integrator == "subcycling" else 1, seed, int(wiener), pol, C.byref(err))
+        self.err = err.value
+        if not self.h:
+            raise ValueError(f"AmrGrid::from_patches error {err.value}")
+        self.nfields = 1 if model == "heat" else 2
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib.orc_amr_sim_destroy(self.h)
+
+    def threads(self, n):
+        lib.orc_amr_sim_set_threads(self.h, n)
+
+    @property
+    def num_blocks(self):
+        return lib.orc_amr_sim_num_blocks(self.h)
+
+    @property
+    def num_levels(self):
+        return lib.orc_amr_sim_num_levels(self.h)
+
+    @property
+    def epoch(self):
+        return lib.orc_amr_sim_epoch(self.h)
+
+    def patch(self, b):
+        out = (C.c_int64 * 5)()
+        lib.orc_amr_sim_patch(self.h, b, out)
+        return int(out[0]), (int(out[1]), int(out[2])), (int(out[3]), int(out[4]))
+
+    def patches(self):
+        return [self.patch(b) for b in range(self.num_blocks)]
+
+    def get(self, f):
+        """List of per-block slabs, each (ny+2, nx+2)."""
+        flat = np.empty(lib.orc_amr_sim_field_len(self.h))
+        lib.orc_amr_sim_get_field(self.h, f, flat.ctypes.data_as(C.POINTER(C.c_double)))
+        out, off = [], 0
+        for lv, lo, hi in self.patches():
+            nx, ny = hi[0] - lo[0], hi[1] - lo[1]
+            n = (nx + 2) * (ny + 2)
+            out.append(flat[off:off + n].reshape(ny + 2, nx + 2).copy())
+            off += n
+        return out
+
+    def set(self, f, slabs):
+        flat = np.ascontiguousarray(np.concatenate([np.asarray(s, dtype=np.float64).ravel() for s in slabs]))
+        lib.orc_amr_sim_set_field(self.h, f, flat.ctypes.data_as(C.POINTER(C.c_double)))
+
+    def step(self, dt, n=1):
+        return lib.orc_amr_sim_step(self.h, dt, n)
+
+    def suggested_dt(self):
+        return lib.orc_amr_sim_suggested_dt(self.h)
+
+    def restrict(self, f):
+        lib.orc_amr_sim_restrict(self.h, f)
+
+    def fill_ghosts(self, f):
+        lib.orc_amr_sim_fill_ghosts(self.h, f)
+
+    def tag(self, f, threshold, level):
+        cap = 1 << 20
+        out = np.zeros(2 * cap, dtype=np.int64)
+        n = lib.orc_amr_sim_tag(self.h, f, threshold, level, out.ctypes.data_as(C.POINTER(C.c_int64)), cap)
+        return [tuple(out[2 * i:2 * i + 2]) for i in range(n)]
+
+    def centers(self, b):
+        """(xc, yc) arrays of the interior cell centres of block b, shape (ny, nx)."""
+        lv, lo, hi = self.patch(b)
+        nx, ny = hi[0] - lo[0], hi[1] - lo[1]
+        xs = np.empty((ny, nx))
+        ys = np.empty((ny, nx))
+        out = (C.c_double * 2)()
+        for j in range(ny):
+            for i in range(nx):
+                lib.orc_amr_sim_cell_center(self.h, b, (C.c_int64 * 2)(i, j), out)
+                xs[j, i], ys[j, i] = out[0], out[1]
+        return xs, ys
