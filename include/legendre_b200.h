@@ -152,6 +152,67 @@ int lg_modelc_initialize_grains(lg_state* st, const double* grains, int64_t n, d
  * helper, it is a `fill_from_fn` closure (cartesian.rs:546-559). */
 int lg_heat_initialize_sine_noise(lg_state* st, int field, uint64_t seed, double amp);
 
+/* ------------------------------------------------------------------ AMR
+ * A 2-D Berger-Oliger simulation on a patch hierarchy: `AmrGrid<2>`
+ * (src/geometry/amr/grid.rs:55-279) with its state, the `Subcycling`
+ * integrator (src/integrators/subcycling.rs:48-268) or a global-dt
+ * Euler-Maruyama, and optionally the `BergerOliger` adaptivity policy
+ * (src/geometry/amr/adapt.rs:131-237), as `Simulation::adaptive` owns them
+ * (src/core/simulation.rs:137-183).  Ghost fill, restriction, tagging and
+ * the per-level steps run on the device; clustering (cluster.rs:144-290)
+ * and migration (adapt.rs:323-402) run on the host at regrid cadence.
+ * Fields have ghost width 1 (the models of the path).  FP64. */
+typedef struct lg_amr_sim lg_amr_sim;
+
+enum lg_model { LG_MODEL_HEAT = 0, LG_MODEL_C = 1 };
+enum lg_amr_integrator { LG_AMR_SUBCYCLING = 0, LG_AMR_GLOBAL_DT = 1 };
+
+/* RegridPolicy + ClusterParams + GradientTagger (adapt.rs:48-129,
+ * cluster.rs:115-135); `field` is the tagged field's index. */
+typedef struct lg_amr_policy {
+    int64_t every;
+    int64_t buffer;
+    int64_t min_width;
+    double efficiency;
+    double threshold;
+    int field;
+} lg_amr_policy;
+
+/* Base grid (cells, block, origin, spacing; 2 entries each), refinement
+ * ratios, and initial patches as npatches x (level, lo_x, lo_y, hi_x, hi_y)
+ * in their level's cell coordinates (AmrGrid::from_patches,
+ * amr/grid.rs:90-196: invalid hierarchies -> LG_ERR_INVALID).
+ * model LG_MODEL_C uses *mp; LG_MODEL_HEAT uses kappa (the heat model of
+ * tests/amr.rs:297-345).  policy NULL = the Static policy. */
+int lg_amr_sim_create(lg_ctx* ctx, const int64_t* cells, const int64_t* block, const double* origin,
+                      const double* spacing, const uint32_t* ratios, int nratios, const int64_t* patches,
+                      int64_t npatches, int model, const lg_modelc_params* mp, double kappa, int integrator,
+                      uint64_t seed, const lg_amr_policy* policy, lg_amr_sim** out);
+int lg_amr_sim_destroy(lg_amr_sim* sim);
+/* Blocks (patches), populated levels, grid epoch (simulation.rs:210-213). */
+int lg_amr_sim_info(const lg_amr_sim* sim, int64_t* num_blocks, int* num_levels, int64_t* epoch);
+/* Patch of a block: (level, lo_x, lo_y, hi_x, hi_y) (AmrGrid::patch). */
+int lg_amr_sim_patch(const lg_amr_sim* sim, int64_t block, int64_t* out5);
+/* Field data: every block's ghost-inclusive slab in BlockId order. */
+int lg_amr_sim_field_len(const lg_amr_sim* sim, int64_t* nelem);
+int lg_amr_sim_get_field(lg_amr_sim* sim, int field, double* host, int64_t nelem);
+int lg_amr_sim_set_field(lg_amr_sim* sim, int field, const double* host, int64_t nelem);
+int lg_amr_sim_time(const lg_amr_sim* sim, double* t, int64_t* step_index);
+/* Integrator::suggested_dt (integrators/mod.rs:218-223, subcycling.rs:54-61). */
+int lg_amr_sim_suggested_dt(const lg_amr_sim* sim, double* dt);
+/* `nsteps` of Simulation::step(dt) (simulation.rs:255-290): regrid at the
+ * policy's cadence, then one coarse step.  LG_RUN_GRAPH replays pairs of
+ * coarse steps between regrids from a captured CUDA graph. */
+int lg_amr_sim_step(lg_amr_sim* sim, double dt, int64_t nsteps, uint32_t flags);
+/* (c) transfers on the current state: `restrict` (intergrid.rs:97-105) of
+ * one field, finest level first; `fill_ghosts_mirror` of every level
+ * (intergrid.rs:155-168); `GradientTagger::tag_level` (adapt.rs:78-103),
+ * flagged cells sorted, *count = total (cells_out holds min(total, cap)). */
+int lg_amr_restrict(lg_amr_sim* sim, int field);
+int lg_amr_fill_ghosts(lg_amr_sim* sim);
+int lg_amr_tag_level(lg_amr_sim* sim, int field, int level, double threshold, int64_t* cells_out, int64_t cap,
+                     int64_t* count);
+
 /* Standard normals of n keys on the device (`rng::standard_normal`,
  * src/util/rng.rs:43-49); host arrays in and out. */
 int lg_standard_normal(lg_ctx* ctx, const uint64_t* keys, int64_t n, double* out);

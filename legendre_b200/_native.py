@@ -51,10 +51,27 @@ class ModelCParams(C.Structure):
     ]
 
 
+class AmrPolicy(C.Structure):
+    _fields_ = [
+        ("every", C.c_int64),
+        ("buffer", C.c_int64),
+        ("min_width", C.c_int64),
+        ("efficiency", C.c_double),
+        ("threshold", C.c_double),
+        ("field", C.c_int),
+    ]
+
+
+LG_MODEL_HEAT = 0
+LG_MODEL_C = 1
+LG_AMR_SUBCYCLING = 0
+LG_AMR_GLOBAL_DT = 1
+
+
 def _load() -> C.CDLL:
     if not _LIB_PATH.exists():
         raise ImportError(
-            f"{_LIB_PATH} is missing: build it with `python -m legendre_b200.build` "
+            f"{_LIB_PATH} is missing: build it with `python legendre_b200/build.py` "
             "(the CUDA library is required; there is no CPU fallback)")
     return C.CDLL(str(_LIB_PATH))
 
@@ -92,6 +109,20 @@ _SIGS = {
     "lg_modelc_initialize_grains": (C.c_int, [_p, _pd, _i64, _d]),
     "lg_heat_initialize_sine_noise": (C.c_int, [_p, C.c_int, _u64, _d]),
     "lg_standard_normal": (C.c_int, [_p, C.POINTER(C.c_uint64), _i64, _pd]),
+    "lg_amr_sim_create": (C.c_int, [_p, _pi64, _pi64, _pd, _pd, C.POINTER(C.c_uint32), C.c_int, _pi64, _i64, C.c_int,
+                                    C.POINTER(ModelCParams), _d, C.c_int, _u64, C.POINTER(AmrPolicy), C.POINTER(_p)]),
+    "lg_amr_sim_destroy": (C.c_int, [_p]),
+    "lg_amr_sim_info": (C.c_int, [_p, _pi64, C.POINTER(C.c_int), _pi64]),
+    "lg_amr_sim_patch": (C.c_int, [_p, _i64, _pi64]),
+    "lg_amr_sim_field_len": (C.c_int, [_p, _pi64]),
+    "lg_amr_sim_get_field": (C.c_int, [_p, C.c_int, _pd, _i64]),
+    "lg_amr_sim_set_field": (C.c_int, [_p, C.c_int, _pd, _i64]),
+    "lg_amr_sim_time": (C.c_int, [_p, _pd, _pi64]),
+    "lg_amr_sim_suggested_dt": (C.c_int, [_p, _pd]),
+    "lg_amr_sim_step": (C.c_int, [_p, _d, _i64, C.c_uint32]),
+    "lg_amr_restrict": (C.c_int, [_p, C.c_int]),
+    "lg_amr_fill_ghosts": (C.c_int, [_p]),
+    "lg_amr_tag_level": (C.c_int, [_p, C.c_int, C.c_int, _d, _pi64, _i64, _pi64]),
 }
 
 for _name, (_res, _args) in _SIGS.items():

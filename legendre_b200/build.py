@@ -5,10 +5,13 @@
 machinery, the library exports a C ABI only).  ``build_oracle()`` compiles
 the CPU restatement used by the tests into ``oracle/liblegendre_oracle.so``.
 
-Run ``python -m legendre_b200.build`` to build both.
+Run ``python legendre_b200/build.py`` to build both (by path: importing the
+package first would load a possibly stale library).
 """
 from __future__ import annotations
 
+import concurrent.futures
+import hashlib
 import os
 import shutil
 import subprocess
@@ -32,6 +35,8 @@ SOURCES = [
     ("lg_modelc.cu", ["-fmad=false"]),
     ("lg_modelc_f32.cu", []),
     ("lg_abi.cu", ["-fmad=false"]),
+    ("lg_amr_host.cu", ["-fmad=false"]),
+    ("lg_amr.cu", ["-fmad=false"]),
 ]
 
 
@@ -42,31 +47,49 @@ def _nvcc() -> str:
     raise RuntimeError("nvcc not found; the CUDA toolkit is required to build legendre_b200")
 
 
-def _stale(target: Path, deps) -> bool:
-    if not target.exists():
+def _digest(deps, extra: str) -> str:
+    h = hashlib.sha256(extra.encode())
+    for d in sorted(map(str, deps)):
+        h.update(d.encode())
+        h.update(Path(d).read_bytes())
+    return h.hexdigest()
+
+
+def _stale(target: Path, deps, extra: str = "") -> bool:
+    # content hash of the sources beside the target: robust to copies that
+    # do not preserve modification times
+    stamp = target.with_name(target.name + ".srchash")
+    if not target.exists() or not stamp.exists():
         return True
-    t = target.stat().st_mtime
-    return any(Path(d).stat().st_mtime > t for d in deps)
+    return stamp.read_text().strip() != _digest(deps, extra)
+
+
+def _stamp(target: Path, deps, extra: str = "") -> None:
+    target.with_name(target.name + ".srchash").write_text(_digest(deps, extra) + "\n")
 
 
 def build_library(force: bool = False, verbose: bool = False) -> Path:
     deps = [CSRC / s for s, _ in SOURCES] + list(CSRC.glob("*.h")) + list(CSRC.glob("*.cuh"))
     deps.append(ROOT / "include" / "legendre_b200.h")
-    if not force and not _stale(LIB, deps):
+    extra = repr(SOURCES) + repr(ARCH)
+    if not force and not _stale(LIB, deps, extra):
         return LIB
     nvcc = _nvcc()
     objdir = PKG / "_build"
     objdir.mkdir(exist_ok=True)
-    objs = []
+    cmds, objs = [], []
     for src, flags in SOURCES:
         obj = objdir / (Path(src).stem + ".o")
         cmd = [nvcc, "-O3", "-std=c++17", *ARCH, "-lineinfo", "-Xcompiler", "-fPIC", *flags,
                "-I", str(ROOT / "include"), "-c", str(CSRC / src), "-o", str(obj)]
         if verbose:
             cmd.insert(1, "-Xptxas=-v")
-        _run(cmd)
+        cmds.append(cmd)
         objs.append(str(obj))
+    with concurrent.futures.ThreadPoolExecutor(max_workers=len(cmds)) as pool:
+        list(pool.map(_run, cmds))
     _run([nvcc, "-shared", *ARCH, *objs, "-o", str(LIB)])
+    _stamp(LIB, deps, extra)
     return LIB
 
 
@@ -78,6 +101,7 @@ def build_oracle(force: bool = False) -> Path:
     cxx = shutil.which("g++") or "g++"
     _run([cxx, "-O2", "-std=c++17", "-ffp-contract=off", "-fopenmp", "-fPIC", "-shared", *map(str, srcs),
           "-o", str(ORACLE_LIB)])
+    _stamp(ORACLE_LIB, deps)
     return ORACLE_LIB
 
 

@@ -192,6 +192,14 @@ void advance_time(lg_state* st, double dt, int64_t steps) {
 
 }  // namespace
 
+namespace lg {
+// context services for the other translation units of the library
+int abi_fail(lg_ctx* ctx, int code, const std::string& msg) { return fail(ctx, code, msg); }
+cudaStream_t abi_stream(lg_ctx* ctx) { return ctx->stream; }
+int abi_device(lg_ctx* ctx) { return ctx->device; }
+void abi_count_launch(lg_ctx* ctx, int64_t n) { ctx->launches += n; }
+}  // namespace lg
+
 extern "C" {
 
 int lg_abi_version(void) { return LG_ABI_VERSION; }

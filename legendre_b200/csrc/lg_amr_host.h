@@ -1,0 +1,128 @@
+// Host side of the 2-D AMR path: the patch hierarchy, its validation,
+// Berger-Rigoutsos clustering, the Berger-Oliger flag processing and the
+// flat transfer plans uploaded to the device.  Restates the reference's
+// src/geometry/amr/{grid,cluster,adapt,intergrid}.rs; the per-step work
+// (ghost fill, restriction, tagging, stepping) runs on the device.
+#pragma once
+
+#include <array>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+namespace lg {
+namespace amr {
+
+// Half-open box of cells at one level (amr/cluster.rs:27-113), 2-D.
+struct Box {
+    int64_t lo[2] = {0, 0}, hi[2] = {0, 0};
+    int64_t extent(int d) const { return hi[d] - lo[d]; }
+    uint64_t cells() const {
+        return (extent(0) > 0 && extent(1) > 0) ? (uint64_t)extent(0) * (uint64_t)extent(1) : 0;
+    }
+    bool contains(int64_t x, int64_t y) const { return lo[0] <= x && x < hi[0] && lo[1] <= y && y < hi[1]; }
+    bool intersects(const Box& o) const {
+        return lo[0] < o.hi[0] && o.lo[0] < hi[0] && lo[1] < o.hi[1] && o.lo[1] < hi[1];
+    }
+    Box clipped(const Box& d) const;
+    bool operator==(const Box& o) const {
+        return lo[0] == o.lo[0] && lo[1] == o.lo[1] && hi[0] == o.hi[0] && hi[1] == o.hi[1];
+    }
+};
+
+struct Patch {
+    int level;
+    Box bx;
+};
+
+struct Base {
+    int64_t cells[2], block[2];
+    double origin[2], spacing[2];
+};
+
+// The hierarchy: level 0 is the base tiling, finer levels are patches in
+// their own index space; BlockId = patch index, level-major
+// (amr/grid.rs:55-70).
+struct Layout {
+    Base base{};
+    std::vector<uint32_t> ratios;
+    std::vector<Patch> patches;
+    std::vector<uint32_t> level_start;
+    std::vector<std::array<double, 2>> level_spacing;
+    std::vector<std::vector<uint32_t>> owner;  // per level, cell -> patch or UINT32_MAX
+
+    int num_levels() const { return (int)level_start.size() - 1; }
+    int max_levels() const { return (int)ratios.size() + 1; }
+    int num_blocks() const { return (int)patches.size(); }
+    Box domain(int level) const;
+    int find(int level, int64_t x, int64_t y) const;  // -1 if uncovered or outside
+};
+
+// AmrGrid::from_patches (amr/grid.rs:90-196); returns "" or the error text.
+std::string build_layout(const Base& base, const std::vector<uint32_t>& ratios,
+                         const std::vector<std::vector<Box>>& levels, Layout* out);
+
+// Berger-Rigoutsos (amr/cluster.rs:144-290); `flags` is reordered.
+std::vector<Box> cluster(std::vector<std::array<int64_t, 2>>& flags, double efficiency, int64_t min_width);
+
+struct Policy {
+    int64_t every = 4, buffer = 2, min_width = 4;
+    double efficiency = 0.8, threshold = 0.1;
+    int field = 0;
+};
+
+// BergerOliger::regrid's box construction (adapt.rs:164-226): `flags[l]`
+// are the tags of level l; returns the proposed boxes per refined level.
+std::vector<std::vector<Box>> propose(const Layout& g, std::vector<std::vector<std::array<int64_t, 2>>>& flags,
+                                      const Policy& p);
+// hierarchy_acceptable (adapt.rs:269-290)
+bool acceptable(const Layout& g, const std::vector<std::vector<Box>>& proposed);
+
+// ------------------------------------------------------------ plans ------
+// Slab placement of one block in a state arena: field f of block b starts
+// at off + f * stride; slabs are (nx+2)(ny+2), ghost 1.
+struct BlockDesc {
+    int level, nx, ny, pad;
+    int64_t off, stride;
+};
+
+// One ghost entry to fill: target (block, slab offset); copy from
+// (a, b) when b >= 0, else bilinear from corners [a, a - b).
+struct FillOp {
+    int tblock, toff, a, b;
+};
+struct Corner {
+    int block, off;
+    double w;
+};
+// One covered coarse cell: (coarse block, offset) <- mean of r x r fine
+// children starting at (fine block, offset).
+struct RestrictOp {
+    int cblock, coff, fblock, foff;
+};
+// A run of cells [start, start + count) of one block (row-major interior).
+struct Unit {
+    int block, start, count, pad;
+};
+
+struct Plans {
+    std::vector<BlockDesc> blocks;
+    int64_t arena_elems = 0;
+    std::vector<FillOp> fill;          // all levels, level-major
+    std::vector<int64_t> fill_start;   // per level, + end
+    std::vector<Corner> corners;
+    std::vector<RestrictOp> restrict_ops;  // per fine level, level-major
+    std::vector<int64_t> restrict_start;   // per fine level (index 0 unused), + end
+    std::vector<Unit> units;
+    std::vector<int64_t> unit_start;       // per level, + end
+};
+
+Plans build_plans(const Layout& g, int nfields, int unit_cells);
+
+// migrate / sample (adapt.rs:323-402) on host slabs: old[b] / out[b] are the
+// ghost-inclusive slabs of one field, block order.
+void migrate_field(const Layout& og, const std::vector<std::vector<double>>& old, const Layout& ng,
+                   std::vector<std::vector<double>>& out);
+
+}  // namespace amr
+}  // namespace lg

@@ -37,11 +37,18 @@ def pytest_collection_modifyitems(config, items):
             item.add_marker(skip)
 
 
-@pytest.fixture(scope="session", autouse=True)
-def _built():
-    from legendre_b200 import build
-    build.build_oracle()
-    yield
+def _build_module():
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("legendre_b200_build", ROOT / "legendre_b200" / "build.py")
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+# build before any test module imports the package (a stale library would
+# miss symbols); cheap when up to date
+_build_module().build_library()
+_build_module().build_oracle()
 
 
 @pytest.fixture(scope="session")

@@ -21,8 +21,11 @@ class Params(C.Structure):
 
 def _load():
     if not _PATH.exists():
-        from legendre_b200 import build
-        build.build_oracle()
+        import importlib.util
+        spec = importlib.util.spec_from_file_location("legendre_b200_build", ROOT / "legendre_b200" / "build.py")
+        mod = importlib.util.module_from_spec(spec)
+        spec.loader.exec_module(mod)
+        mod.build_oracle()
     lib = C.CDLL(str(_PATH))
     p, i64, u64, d = C.c_void_p, C.c_int64, C.c_uint64, C.c_double
     pd, pi64 = C.POINTER(C.c_double), C.POINTER(C.c_int64)
