@@ -320,6 +320,7 @@ void free_device(lg_amr_sim* s) {
 int setup_device(lg_amr_sim* s) {
     free_device(s);
     s->plans = lg::amr::build_plans(s->layout, s->nfields, 1024);
+    if (!s->plans.error.empty()) return fail(s, LG_ERR_STATE, s->plans.error);
     cudaError_t e = cudaSuccess;
     std::vector<int64_t> lo;
     for (const auto& p : s->layout.patches) {

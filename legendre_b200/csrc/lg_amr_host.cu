@@ -363,6 +363,10 @@ Plans build_plans(const Layout& g, int nfields, int unit_cells) {
                         if (weight == 0.0) continue;
                         for (int d = 0; d < 2; ++d) cc[d] = reflect(cc[d], cd.lo[d], cd.hi[d]);
                         const int q = g.find(level - 1, cc[0], cc[1]);
+                        if (q < 0) {  // the reference panics: proper nesting guarantees a donor
+                            P.error = "no coarse donor for prolongation at level " + std::to_string(level);
+                            continue;
+                        }
                         const Box& qb = g.patches[q].bx;
                         P.corners.push_back(Corner{q, slab_off(q, cc[0] - qb.lo[0], cc[1] - qb.lo[1]), weight});
                     }

@@ -106,6 +106,7 @@ struct Unit {
 };
 
 struct Plans {
+    std::string error;  // non-empty when the hierarchy is not properly nested
     std::vector<BlockDesc> blocks;
     int64_t arena_elems = 0;
     std::vector<FillOp> fill;          // all levels, level-major
