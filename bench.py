@@ -38,6 +38,18 @@ CONFIGS = {
     "c3": dict(workload="model_c_10080sq", cells=10080, block=126, h=0.4, dt=0.008, d_thermal=2.0,
                lam=2.0 / 0.6267, eps4=0.05, u0=0.5, grains=64, radius=8.0, noise=0.01, seed=42,
                full_steps=10000),
+    # 3-D heat, 96^3 periodic as 6^3 blocks of 16^3, dt = 0.15 h^2, sine + seeded noise
+    "c1": dict(kind="heat", workload="heat_96cube", cells=96, block=16, kappa=1.0, seed=42, amp=1e-3,
+               full_steps=2000, noise=0.0),
+    # the same heat model at 512^3 (32^3 blocks of 16^3): an HBM-resident variant
+    "c1big": dict(kind="heat", workload="heat_512cube", cells=512, block=16, kappa=1.0, seed=42, amp=1e-3,
+                  full_steps=2000, noise=0.0),
+    # Model C with Berger-Oliger AMR: 1024^2 base as 32^2 blocks of 32^2,
+    # ratios [2, 2, 2], tag |grad phi| > 0.05, regrid every 50 coarse steps,
+    # one central grain r = 8, u0 = -0.55, no noise, subcycled
+    "c4": dict(kind="amr", workload="model_c_amr_1024sq_3lev", cells=1024, block=32, h=0.4, d_thermal=2.0,
+               lam=2.0 / 0.6267, eps4=0.05, u0=0.55, radius=8.0, ratios=[2, 2, 2], every=50, buffer=2,
+               threshold=0.05, noise=0.0, full_steps=4000),
 }
 
 BYTES_PER_CELL = {"f64": 32, "f32": 16}  # read phi, u; write phi, u
@@ -202,6 +214,112 @@ def run_reference(args, cfg):
     print(json.dumps(line), flush=True)
 
 
+def run_other(args, cfg):
+    """The heat (c1) and AMR (c4) configurations: device-timed K steps,
+    the same JSON schema (no CPU leg, no e2e copy-in/out)."""
+    import math
+
+    import numpy as np
+    import torch
+
+    import legendre_b200 as L
+
+    rank, world, local, pg = dist_setup(args.gpus)
+    stream = torch.cuda.Stream(device=local)
+    torch.cuda.set_stream(stream)
+    sched = L.CudaScheduler(local, stream.cuda_stream)
+    if cfg["kind"] == "heat":
+        n, b = cfg["cells"], cfg["block"]
+        h = 1.0 / n
+        grid = L.CartesianGrid([n] * 3, [b] * 3, [0.0] * 3, [h] * 3).with_periodic([True] * 3)
+        model = L.Heat(cfg["kappa"])
+        sim = L.Simulation(grid, L.FiniteDifference(), model, L.ForwardEuler(), sched, L.CudaAllocator("f64"))
+        model.initialize_sine_noise(sim.state, cfg["seed"], cfg["amp"])
+        dt = 0.15 * h * h
+        run = lambda k: sim.run(dt, k, graph=True)
+        cells_per_step = lambda: float(n ** 3)
+        bytes_per_cell = 16
+        extra = {"cells": n, "block": b, "periodic": True, "dt": dt,
+                 "l2": "state fits in L2 (no flush): launch- and L2-bound" if n ** 3 * 8 * 2 < 100e6
+                 else "state larger than L2; no flush"}
+    else:
+        n, b, hh = cfg["cells"], cfg["block"], cfg["h"]
+        base = L.CartesianGrid([n, n], [b, b], [0.0, 0.0], [hh, hh])
+        grid = L.AmrGrid.from_patches(base, cfg["ratios"], [])
+        model = L.ModelC(cfg["eps4"], cfg["lam"], cfg["noise"])
+        model.d_thermal = cfg["d_thermal"]
+        adapt = L.BergerOliger(L.GradientTagger("phi", cfg["threshold"]),
+                               L.RegridPolicy(cfg["every"], cfg["buffer"], L.ClusterParams(0.8, 4)))
+        sim = L.AmrSimulation(grid, L.FiniteVolume(), model, L.Subcycling(0), sched, L.CudaAllocator("f64"), adapt)
+        c = n * hh / 2.0
+        phi, u = sim.get("phi"), sim.get("u")
+        for k in range(sim.num_blocks):
+            xs, ys = sim.centers(k)
+            r = np.hypot(xs - c, ys - c)
+            phi[k][1:-1, 1:-1] = np.maximum(-1.0, -np.tanh((r - cfg["radius"]) / math.sqrt(2.0)))
+            u[k][1:-1, 1:-1] = -cfg["u0"]
+        sim.set("phi", phi)
+        sim.set("u", u)
+        dt = sim.stable_dt()
+        run = lambda k: sim.run(dt, k, graph=True)
+
+        def cells_per_step():
+            # cell-updates of one coarse step: every level's cells times its
+            # substeps per coarse step (4 per level at ratio 2)
+            tot, mult = 0.0, 1.0
+            per_level = {}
+            for lv, lo, hi in sim.patches():
+                per_level[lv] = per_level.get(lv, 0) + (hi[0] - lo[0]) * (hi[1] - lo[1])
+            for lv in sorted(per_level):
+                tot += per_level[lv] * mult
+                mult *= 4.0
+            return tot
+        bytes_per_cell = 32
+        extra = {"cells": n, "block": b, "ratios": cfg["ratios"], "regrid_every": cfg["every"], "dt": dt,
+                 "l2": "hierarchy state below L2 size; no flush"}
+    run(args.warmup)
+    torch.cuda.synchronize()
+    c0 = cells_per_step()
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    barrier(pg)
+    torch.cuda.synchronize()
+    launches0 = sched.kernel_launches
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    run(args.steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier(pg)
+    clk = clocks.stop()
+    c1 = cells_per_step()
+    ms = max_over_ranks(pg, e0.elapsed_time(e1))
+    cells = 0.5 * (c0 + c1)
+    value = world * cells * args.steps / (ms / 1e3) / 1e9
+    if rank == 0:
+        peak, peak_kind = peaks()
+        achieved = bytes_per_cell * cells / (ms / args.steps / 1e3) / 1e9
+        line = {
+            "metric": "Gcell-updates/s", "value": value, "unit": "Gcell-updates/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": dict({"workload": cfg["workload"], "parallelism": f"replicas{world}", "graph": True}, **extra),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
+                         "algorithmic_bytes_per_cell": bytes_per_cell},
+            "cpu_baseline": None, "e2e": None,
+            "gpu_launches": sched.kernel_launches - launches0,
+            "clocks": {"sm_mhz": clk["sm_mhz"], "sm_max_mhz": clk["sm_max_mhz"], "reasons": clk["reasons"],
+                       "samples": clk["samples"]},
+        }
+        print(json.dumps(line), flush=True)
+    sched.close()
+    if pg is not None:
+        pg.destroy_process_group()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -220,6 +338,10 @@ def main():
         cfg["noise"] = args.noise
     if args.impl == "reference":
         run_reference(args, cfg)
+        return
+
+    if cfg.get("kind") in ("heat", "amr"):
+        run_other(args, cfg)
         return
 
     import torch

@@ -198,6 +198,8 @@ int abi_fail(lg_ctx* ctx, int code, const std::string& msg) { return fail(ctx, c
 cudaStream_t abi_stream(lg_ctx* ctx) { return ctx->stream; }
 int abi_device(lg_ctx* ctx) { return ctx->device; }
 void abi_count_launch(lg_ctx* ctx, int64_t n) { ctx->launches += n; }
+int64_t abi_launches(lg_ctx* ctx) { return ctx->launches; }
+void abi_set_launches(lg_ctx* ctx, int64_t n) { ctx->launches = n; }
 }  // namespace lg
 
 extern "C" {

@@ -25,6 +25,8 @@ int abi_fail(lg_ctx* ctx, int code, const std::string& msg);
 cudaStream_t abi_stream(lg_ctx* ctx);
 int abi_device(lg_ctx* ctx);
 void abi_count_launch(lg_ctx* ctx, int64_t n);
+int64_t abi_launches(lg_ctx* ctx);
+void abi_set_launches(lg_ctx* ctx, int64_t n);
 }  // namespace lg
 
 namespace {
@@ -802,11 +804,14 @@ int lg_amr_sim_step(lg_amr_sim* s, double dt, int64_t nsteps, uint32_t flags) {
             if (it == s->graphs.end()) {
                 const std::vector<int> cur0 = s->cur;
                 const int slot0 = s->tslot;
+                const int64_t before = lg::abi_launches(s->ctx);
                 cudaGraph_t graph = nullptr;
                 AMR_CUDA(s, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
                 int rc2 = one_coarse_step(s, dt);
                 if (rc2 == LG_OK) rc2 = one_coarse_step(s, dt);
                 cudaError_t ec = cudaStreamEndCapture(st, &graph);
+                const int64_t captured = lg::abi_launches(s->ctx) - before;
+                lg::abi_set_launches(s->ctx, before);
                 if (rc2 != LG_OK) {
                     if (graph) cudaGraphDestroy(graph);
                     return rc2;
@@ -820,10 +825,11 @@ int lg_amr_sim_step(lg_amr_sim* s, double dt, int64_t nsteps, uint32_t flags) {
                 cudaError_t ei = cudaGraphInstantiate(&exec, graph, 0);
                 cudaGraphDestroy(graph);
                 AMR_CUDA(s, ei);
-                it = s->graphs.emplace(gk, std::make_pair(exec, (int64_t)0)).first;
+                it = s->graphs.emplace(gk, std::make_pair(exec, captured)).first;
             }
             for (; k + 2 <= run; k += 2) {
                 AMR_CUDA(s, cudaGraphLaunch(it->second.first, st));
+                lg::abi_count_launch(s->ctx, it->second.second);
                 for (int r2 = 0; r2 < 2; ++r2) {
                     s->t += dt;
                     s->step_index += 1;
