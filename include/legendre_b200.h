@@ -46,6 +46,7 @@ enum lg_dtype { LG_F64 = 0, LG_F32 = 1 };
 
 /* Run flags. */
 #define LG_RUN_GRAPH 1u      /* capture the step sequence once in a CUDA graph and replay it */
+#define LG_RUN_PERSISTENT 2u /* AMR: every phase of a coarse step in one cooperative launch */
 
 typedef struct lg_ctx lg_ctx;
 typedef struct lg_grid lg_grid;
@@ -202,7 +203,12 @@ int lg_amr_sim_time(const lg_amr_sim* sim, double* t, int64_t* step_index);
 int lg_amr_sim_suggested_dt(const lg_amr_sim* sim, double* dt);
 /* `nsteps` of Simulation::step(dt) (simulation.rs:255-290): regrid at the
  * policy's cadence, then one coarse step.  LG_RUN_GRAPH replays pairs of
- * coarse steps between regrids from a captured CUDA graph. */
+ * coarse steps between regrids from a captured CUDA graph.
+ * LG_RUN_PERSISTENT runs every phase of a pair of coarse steps (each
+ * level's fused ghost fill + step, each restriction) in one cooperative
+ * launch whose CTAs meet at grid barriers; a barrier wait is bounded, and
+ * if one gives up the call returns LG_ERR_TIMEOUT and the state is invalid.
+ * It takes precedence over LG_RUN_GRAPH. */
 int lg_amr_sim_step(lg_amr_sim* sim, double dt, int64_t nsteps, uint32_t flags);
 /* (c) transfers on the current state: `restrict` (intergrid.rs:97-105) of
  * one field, finest level first; `fill_ghosts_mirror` of every level

@@ -21,6 +21,7 @@ LG_ERR_DEVICE = -6
 LG_F64 = 0
 LG_F32 = 1
 LG_RUN_GRAPH = 1
+LG_RUN_PERSISTENT = 2
 
 _STATUS = {
     LG_ERR_INVALID: "invalid argument",

@@ -212,9 +212,13 @@ class AmrSimulation:
     def step(self, dt: float) -> None:
         self.run(dt, 1)
 
-    def run(self, dt: float, nsteps: int, graph: bool = False) -> None:
-        N.check(N.lib.lg_amr_sim_step(self.handle, float(dt), int(nsteps), N.LG_RUN_GRAPH if graph else 0),
-                self.scheduler.handle)
+    def run(self, dt: float, nsteps: int, graph: bool = False, persistent: bool = False) -> None:
+        """`nsteps` coarse steps.  `graph` replays pairs of coarse steps from a
+        CUDA graph; `persistent` runs each pair as one cooperative launch
+        (every level's fused fill + step and every restriction, separated by
+        grid barriers) and takes precedence."""
+        flags = (N.LG_RUN_GRAPH if graph else 0) | (N.LG_RUN_PERSISTENT if persistent else 0)
+        N.check(N.lib.lg_amr_sim_step(self.handle, float(dt), int(nsteps), flags), self.scheduler.handle)
 
     # ------------------------------------------------------ transfers (c)
     def restrict(self, f) -> None:

@@ -32,8 +32,7 @@ void abi_set_launches(lg_ctx* ctx, int64_t n);
 namespace {
 
 using lg::amr::BlockDesc;
-using lg::amr::Corner;
-using lg::amr::FillOp;
+using lg::amr::GhostOp;
 using lg::amr::RestrictOp;
 using lg::amr::Unit;
 
@@ -54,57 +53,41 @@ __device__ __forceinline__ double chain_time(double t0, const TimeChain& c) {
 }
 
 // ------------------------------------------------------------ kernels ----
-// Ghost entries of one level (intergrid.rs:183-223 / 358-408): a copy of a
-// same-level interior entry, or the bilinear fold acc + v w over coarse
-// interior corners, blended in time as old (1 - alpha) + new alpha.
-// A (this level) and Ac (the coarser level) may be the same arena: the
-// kernel writes ghost entries only and reads interior entries only.
-__global__ void amr_fill_kernel(const BlockDesc* __restrict__ blocks, double* A, const double* Ac, const double* Sc,
-                                const FillOp* __restrict__ ops, int64_t nops, const Corner* __restrict__ corners,
-                                int nfields, double alpha, int interp) {
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nops; i += (int64_t)gridDim.x * blockDim.x) {
-        const FillOp op = ops[i];
-        const BlockDesc tb = blocks[op.tblock];
-        for (int f = 0; f < nfields; ++f) {
-            double v;
-            if (op.b >= 0) {
-                const BlockDesc sb = blocks[op.a];
-                v = A[sb.off + f * sb.stride + op.b];
-            } else {
-                double acc = 0.0, old = 0.0;
-                for (int k = op.a; k < op.a - op.b; ++k) {
-                    const Corner c = corners[k];
-                    const BlockDesc cb = blocks[c.block];
-                    const int64_t o = cb.off + f * cb.stride + c.off;
-                    acc = acc + Ac[o] * c.w;
-                    if (interp) old = old + Sc[o] * c.w;
-                }
-                v = interp ? old * (1.0 - alpha) + acc * alpha : acc;
-            }
-            A[tb.off + f * tb.stride + op.toff] = v;
+// The value of field f of one ghost entry (GhostOp): a copy of a same-level
+// interior entry of `in`, or the bilinear fold acc + v w over coarse
+// interior corners, blended in time as old (1 - alpha) + new alpha
+// (intergrid.rs:183-223 / 358-408).  All loads of one op are independent.
+__device__ __forceinline__ double ghost_value(const GhostOp& op, const double* in, const double* cnew,
+                                              const double* cold, int interp, double alpha, int f) {
+    if (op.n == 0) return in[op.src[0] + (int64_t)f * op.stride[0]];
+    double acc = 0.0, old = 0.0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        if (k < op.n) {
+            const int64_t o = op.src[k] + (int64_t)f * op.stride[k];
+            acc = acc + cnew[o] * op.w[k];
+            if (interp) old = old + cold[o] * op.w[k];
         }
+    }
+    return interp ? old * (1.0 - alpha) + acc * alpha : acc;
+}
+
+// Ghost entries of one level, written in place (no time blend).  A and Ac
+// (the coarser level) may be the same arena: the kernel writes ghost
+// entries only and reads interior entries only.
+__global__ void amr_fill_kernel(double* A, const double* Ac, const GhostOp* __restrict__ ops, int64_t nops,
+                                int nfields) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nops; i += (int64_t)gridDim.x * blockDim.x) {
+        const GhostOp op = ops[i];
+        for (int f = 0; f < nfields; ++f) A[op.dst + (int64_t)f * op.dst_stride] = ghost_value(op, A, Ac, Ac, 0, 0.0, f);
     }
 }
 
 // Covered coarse cells <- sum of r x r fine children (dimension 0 fastest,
 // from zero) times 1/r^2 (intergrid.rs:110-150).
 // C (coarse level) and F (fine level) may be the same arena (disjoint slabs).
-__global__ void amr_restrict_kernel(const BlockDesc* __restrict__ blocks, double* C, const double* F,
-                                    const RestrictOp* __restrict__ ops, int64_t nops,
-                                    int r, double inv, int f0, int f1) {
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nops; i += (int64_t)gridDim.x * blockDim.x) {
-        const RestrictOp op = ops[i];
-        const BlockDesc fb = blocks[op.fblock], cb = blocks[op.cblock];
-        const int sy = fb.nx + 2;
-        for (int f = f0; f < f1; ++f) {
-            const double* src = F + fb.off + f * fb.stride + op.foff;
-            double sum = 0.0;
-            for (int ky = 0; ky < r; ++ky)
-                for (int kx = 0; kx < r; ++kx) sum += src[kx + ky * sy];
-            C[cb.off + f * cb.stride + op.coff] = sum * inv;
-        }
-    }
-}
+__global__ void amr_restrict_kernel(double* C, const double* F, const RestrictOp* __restrict__ ops, int64_t nops,
+                                    int r, double inv, int f0, int f1);
 
 // GradientTagger::tag_level (adapt.rs:78-103): flag where
 // max_d |(u(+e_d) - u(-e_d)) 0.5| > threshold; cells in level coordinates.
@@ -134,104 +117,301 @@ __global__ void amr_tag_kernel(const BlockDesc* __restrict__ blocks, const int64
     }
 }
 
-struct StepArgs {
-    const BlockDesc* blocks;
-    const Unit* units;
-    int64_t nunits;
+// One fused ghost-fill + Euler-Maruyama launch over the tiles of a level.
+// `in` / `out` are the level's current and next buffers (whole arenas,
+// offsets from the block table); `cnew` / `cold` the coarse level's current
+// and pre-step buffers for the time-interpolated prolongation (the coarse
+// level's ping-pong buffer from before its step is the reference's
+// snapshot: nothing writes that level's slabs of it until its next step).
+struct TileArgs {
+    const lg::amr::Tile* tiles;
+    int64_t ntiles;
+    const GhostOp* tfill;
     const double* in;
     double* out;
+    const double* cnew;
+    const double* cold;
+    double alpha;
+    int interp;
     double dt;
     double* tdev;
     int slot;
     int write_t;   // this launch advances the level-0 time slot
     double dt0;    // level-0 step (for that advance)
     TimeChain chain;
-    int noise;
     uint64_t seed;
     double scale_amp;
 };
 
-// Model C Euler-Maruyama on the cells of one level's work list (the
-// reference-order cell update of phasefield.rs:353-422 with the Time and
-// Wiener drivers, state.rs:706-753).  Ghosts are not pushed: under AMR
-// they come from the fill plan.
-__global__ void __launch_bounds__(256) amr_modelc_kernel(StepArgs a, lg::MC<double> m) {
+constexpr int kWin = lg::amr::kTile + 2;
+
+// Stage the (w + 2) x (h + 2) window of a tile for NF fields: block interior
+// entries from `in`, block ghost entries from the tile's fill ops.
+template <int NF>
+__device__ __forceinline__ void stage_tile(const TileArgs& a, const lg::amr::Tile& T, double* s0, double* s1) {
+    const int P = T.w + 2, R = T.h + 2, sy = T.nx + 2;
+    const double* g0 = a.in + T.off;
+    for (int k = threadIdx.x; k < P * R; k += blockDim.x) {
+        const int c = k % P, r = k / P;
+        const int i = T.x0 + c - 1, j = T.y0 + r - 1;
+        if (i < 0 || i >= T.nx || j < 0 || j >= T.ny) continue;  // a ghost of the block
+        const int o = (i + 1) + (j + 1) * sy;
+        s0[k] = g0[o];
+        if (NF == 2) s1[k] = g0[T.stride + o];
+    }
+    for (int k = T.fill0 + (int)threadIdx.x; k < T.fill1; k += blockDim.x) {
+        const GhostOp op = a.tfill[k];
+        s0[op.dst] = ghost_value(op, a.in, a.cnew, a.cold, a.interp, a.alpha, 0);
+        if (NF == 2) s1[op.dst] = ghost_value(op, a.in, a.cnew, a.cold, a.interp, a.alpha, 1);
+    }
+    __syncthreads();
+}
+
+// Model C Euler-Maruyama on the tiles of one level (the reference-order cell
+// update of phasefield.rs:353-422 with the Time and Wiener drivers,
+// state.rs:706-753).  Lanes are the tile's columns, each warp a run of rows;
+// a face flux is computed once and shared by the two cells it separates
+// (right faces by shuffle, top faces down the row loop), which is bitwise
+// the reference's per-cell evaluation: the left face of cell i + 1 and the
+// right face of cell i are the same expression of the same operands.
+template <bool NOISE>
+__device__ __forceinline__ void modelc_tile(const TileArgs& a, const lg::MC<double>& m, const lg::amr::Tile& T,
+                                            double t, double* sp, double* su) {
+    using Ops = lg::OpsExact<double>;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    stage_tile<2>(a, T, sp, su);
+    const int P = T.w + 2;
+    const int rpw = (T.h + nwarps - 1) / nwarps;
+    const int r0 = warp * rpw, r1 = min(T.h, r0 + rpw);
+    if (r0 < r1) {  // warp-uniform
+        const int ci = min(lane, T.w - 1);  // idle lanes duplicate the last column
+        uint64_t block_key = 0;
+        if (NOISE)
+            block_key = lg::wiener_block_key(a.seed, (uint64_t)__double_as_longlong(t), lg::kWienerStream0,
+                                             (uint64_t)T.block);
+        // left faces of column 0, one row per lane
+        double jl0;
+        {
+            const double* q = sp + 1 + (r0 + min(lane, r1 - r0 - 1) + 1) * P;
+            jl0 = Ops::xface(m, q[0] - q[-1], q[P] - q[-P], q[P - 1], q[-P - 1]);
+        }
+        double jb;
+        {
+            const double* q = sp + (ci + 1) + (r0 + 1) * P;
+            jb = Ops::yface(m, q[0] - q[-P], q[1] - q[-1], q[1 - P], q[-1 - P]);
+        }
+        for (int cj = r0; cj < r1; ++cj) {
+            const double* q = sp + (ci + 1) + (cj + 1) * P;
+            const double* w = su + (ci + 1) + (cj + 1) * P;
+            const double jt = Ops::yface(m, q[P] - q[0], q[P + 1] - q[P - 1], q[1], q[-1]);
+            const double jr = Ops::xface(m, q[1] - q[0], q[P + 1] - q[1 - P], q[P], q[-P]);
+            double jl = __shfl_up_sync(0xffffffffu, jr, 1);
+            const double jlb = __shfl_sync(0xffffffffu, jl0, cj - r0);
+            if (lane == 0) jl = jlb;
+            double kphi, ku;
+            Ops::cell(m, jr, jl, jt, jb, q[0], q[1] - q[-1], q[P] - q[-P], w[0], w[-1], w[1], w[P], w[-P], kphi, ku);
+            jb = jt;
+            if (lane < T.w) {
+                const int i = T.x0 + ci, j = T.y0 + cj;
+                double phin = Ops::axpy(a.dt, kphi, q[0]);
+                if (NOISE)
+                    phin = Ops::add_noise(phin, a.scale_amp,
+                                          Ops::noise(lg::splitmix64(block_key ^ (uint64_t)(j * T.nx + i))));
+                const int64_t o = T.off + (i + 1) + (int64_t)(j + 1) * (T.nx + 2);
+                a.out[o] = phin;
+                a.out[o + T.stride] = Ops::axpy(a.dt, ku, w[0]);
+            }
+        }
+    }
+    __syncthreads();
+}
+
+template <bool NOISE>
+__global__ void __launch_bounds__(256) amr_modelc_tiles(TileArgs a, lg::MC<double> m) {
+    __shared__ double sp[kWin * kWin], su[kWin * kWin];
     const double t0 = a.tdev[a.slot];
     if (a.write_t && blockIdx.x == 0 && threadIdx.x == 0) a.tdev[a.slot ^ 1] = t0 + a.dt0;
-    const double t = chain_time(t0, a.chain);
-    for (int64_t u = blockIdx.x; u < a.nunits; u += gridDim.x) {
-        const Unit un = a.units[u];
-        const BlockDesc b = a.blocks[un.block];
-        const double* ph = a.in + b.off;
-        const double* uu = a.in + b.off + b.stride;
-        double* po = a.out + b.off;
-        double* uo = a.out + b.off + b.stride;
-        const int sy = b.nx + 2;
-        uint64_t block_key = 0;
-        if (a.noise)
-            block_key = lg::wiener_block_key(a.seed, (uint64_t)__double_as_longlong(t), lg::kWienerStream0,
-                                             (uint64_t)un.block);
-        for (int c = un.start + threadIdx.x; c < un.start + un.count; c += blockDim.x) {
-            const int i = c % b.nx, j = c / b.nx;
-            const int o = (i + 1) + (j + 1) * sy;
-            auto P = [&](int di, int dj) { return ph[o + di + dj * sy]; };
-            double derx_r = P(1, 0) - P(0, 0);
-            double derx_l = P(0, 0) - P(-1, 0);
-            double derx_t = 0.25 * (P(1, 1) - P(-1, 1) + P(1, 0) - P(-1, 0));
-            double derx_b = 0.25 * (P(1, 0) - P(-1, 0) + P(1, -1) - P(-1, -1));
-            double dery_t = P(0, 1) - P(0, 0);
-            double dery_b = P(0, 0) - P(0, -1);
-            double dery_r = 0.25 * (P(1, 1) - P(1, -1) + P(0, 1) - P(0, -1));
-            double dery_l = 0.25 * (P(0, 1) - P(0, -1) + P(-1, 1) - P(-1, -1));
-            double a_r, da_r, a_l, da_l, a_t, da_t, a_b, da_b;
-            lg::kr_face(m, derx_r, dery_r, a_r, da_r);
-            lg::kr_face(m, derx_l, dery_l, a_l, da_l);
-            lg::kr_face(m, derx_t, dery_t, a_t, da_t);
-            lg::kr_face(m, derx_b, dery_b, a_b, da_b);
-            double j_r = a_r * (a_r * derx_r - da_r * dery_r);
-            double j_l = a_l * (a_l * derx_l - da_l * dery_l);
-            double j_t = a_t * (a_t * dery_t + da_t * derx_t);
-            double j_b = a_b * (a_b * dery_b + da_b * derx_b);
-            double flux = (j_r - j_l + j_t - j_b) * m.inv_h2_flux;
-            double p = P(0, 0);
-            double g_prime = fma(p * p, p, -p);
-            double one_m_p2 = fma(p, -p, 1.0);
-            double p_prime = one_m_p2 * one_m_p2;
-            double ac = lg::center_anisotropy(m, 0.5 * (P(1, 0) - P(-1, 0)), 0.5 * (P(0, 1) - P(0, -1)));
-            double uc = uu[o];
-            double kphi = fma(m.lambda * uc, -p_prime, flux - g_prime) / (ac * ac);
-            double acc = 0.0;
-            acc += ((uu[o + 1] - (uc + uc)) + uu[o - 1]) * m.ih0;
-            acc += ((uu[o + sy] - (uc + uc)) + uu[o - sy]) * m.ih1;
-            double ku = fma(acc, m.d_thermal, 0.5 * kphi);
-            double phin = p + a.dt * kphi;
-            if (a.noise) phin += a.scale_amp * lg::standard_normal(lg::splitmix64(block_key ^ (uint64_t)c));
-            po[o] = phin;
-            uo[o] = uc + a.dt * ku;
+    const double t = NOISE ? chain_time(t0, a.chain) : 0.0;
+    for (int64_t ti = blockIdx.x; ti < a.ntiles; ti += gridDim.x) modelc_tile<NOISE>(a, m, a.tiles[ti], t, sp, su);
+}
+
+// Heat on the tiles of one level: k = lap(u) kappa, u + dt k
+// (tests/amr.rs:324-339, finite_difference.rs:49-67, euler.rs:51-53).
+__device__ __forceinline__ void heat_tile(const TileArgs& a, double kappa, double ih0, double ih1,
+                                          const lg::amr::Tile& T, double* sp) {
+    stage_tile<1>(a, T, sp, nullptr);
+    const int P = T.w + 2;
+    for (int k = threadIdx.x; k < T.w * T.h; k += blockDim.x) {
+        const int ci = k % T.w, cj = k / T.w;
+        const double* q = sp + (ci + 1) + (cj + 1) * P;
+        const double center = q[0];
+        double acc = 0.0;
+        acc += ((q[1] - (center + center)) + q[-1]) * ih0;
+        acc += ((q[P] - (center + center)) + q[-P]) * ih1;
+        const double kk = acc * kappa;
+        a.out[T.off + (T.x0 + ci + 1) + (int64_t)(T.y0 + cj + 1) * (T.nx + 2)] = center + a.dt * kk;
+    }
+    __syncthreads();
+}
+
+__global__ void __launch_bounds__(256) amr_heat_tiles(TileArgs a, double kappa, double ih0, double ih1) {
+    __shared__ double sp[kWin * kWin];
+    const double t0 = a.tdev[a.slot];
+    if (a.write_t && blockIdx.x == 0 && threadIdx.x == 0) a.tdev[a.slot ^ 1] = t0 + a.dt0;
+    for (int64_t ti = blockIdx.x; ti < a.ntiles; ti += gridDim.x) heat_tile(a, kappa, ih0, ih1, a.tiles[ti], sp);
+}
+
+// restriction body shared by the launch-per-phase and persistent paths
+__device__ __forceinline__ void restrict_ops(double* C, const double* F, const RestrictOp* __restrict__ ops,
+                                             int64_t nops, int r, double inv, int f0, int f1) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nops; i += (int64_t)gridDim.x * blockDim.x) {
+        const RestrictOp op = ops[i];
+        for (int f = f0; f < f1; ++f) {
+            const double* src = F + op.f + (int64_t)f * op.fstride;
+            double sum = 0.0;
+            for (int ky = 0; ky < r; ++ky)
+                for (int kx = 0; kx < r; ++kx) sum += src[kx + ky * op.fsy];
+            C[op.c + (int64_t)f * op.cstride] = sum * inv;
         }
     }
 }
 
-// Heat on the cells of one level's work list: k = lap(u) kappa, u + dt k
-// (tests/amr.rs:324-339, euler.rs:51-53).
-__global__ void __launch_bounds__(256) amr_heat_kernel(StepArgs a, double kappa, double ih0, double ih1) {
-    const double t0 = a.tdev[a.slot];
-    if (a.write_t && blockIdx.x == 0 && threadIdx.x == 0) a.tdev[a.slot ^ 1] = t0 + a.dt0;
-    for (int64_t u = blockIdx.x; u < a.nunits; u += gridDim.x) {
-        const Unit un = a.units[u];
-        const BlockDesc b = a.blocks[un.block];
-        const double* s = a.in + b.off;
-        double* o_ = a.out + b.off;
-        const int sy = b.nx + 2;
-        for (int c = un.start + threadIdx.x; c < un.start + un.count; c += blockDim.x) {
-            const int i = c % b.nx, j = c / b.nx;
-            const int o = (i + 1) + (j + 1) * sy;
-            const double center = s[o];
-            double acc = 0.0;
-            acc += ((s[o + 1] - (center + center)) + s[o - 1]) * ih0;
-            acc += ((s[o + sy] - (center + center)) + s[o - sy]) * ih1;
-            const double k = acc * kappa;
-            o_[o] = center + a.dt * k;
+__global__ void amr_restrict_kernel(double* C, const double* F, const RestrictOp* __restrict__ ops, int64_t nops,
+                                    int r, double inv, int f0, int f1) {
+    restrict_ops(C, F, ops, nops, r, inv, f0, f1);
+}
+
+// ------------------------------------------------- persistent coarse step --
+// One phase of a coarse step: a fused fill + step of one level's tiles, or
+// the restriction of one fine level, with its buffer indices resolved on the
+// host (the Berger-Oliger recursion of subcycling.rs:195-267, flattened).
+struct Phase {
+    int kind;  // 0: step, 1: restrict
+    int level;
+    int in, cnew, cold;  // step: own buffer and the coarse level's current / pre-step; restrict: fine, coarse
+    int interp, write_t, slot;
+    int r, barrier;  // restrict ratio; a grid barrier follows this phase
+    int64_t first, count;  // tiles of the level's list, or restrict ops
+    double alpha, dt, dt0, scale_amp, inv;
+    TimeChain chain;
+};
+
+struct PersistArgs {
+    const Phase* phases;
+    int nphases;
+    const lg::amr::Tile* tiles0;  // level 0's list
+    const GhostOp* tfill0;
+    const lg::amr::Tile* tiles;  // refined levels' list
+    const GhostOp* tfill;
+    const RestrictOp* rops;
+    double* arena0;
+    double* arena1;
+    double* tdev;
+    uint64_t seed;
+    int nfields;
+    double kappa;
+    lg::MC<double> mc[kMaxDepth];
+    unsigned* bar;  // [arrivals, generation]
+    int* err;       // set when a barrier wait gave up
+    long long spin_limit;
+};
+
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// Grid-wide barrier of a cooperative launch: every CTA's writes before it
+// are visible to every CTA after it.  The wait is bounded: after spin_limit
+// polls (or once another CTA has given up) the CTA records the error and
+// every thread of it returns false.
+__device__ bool grid_sync(const PersistArgs& a, unsigned& target, int* s_abort) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int abort = 0;
+        target += 1;
+        __threadfence();
+        const unsigned prev = atomicAdd(&a.bar[0], 1u);
+        if (prev == gridDim.x - 1) {
+            atomicExch(&a.bar[0], 0u);
+            __threadfence();
+            atomicExch(&a.bar[1], target);
+        } else {
+            long long it = 0;
+            while (ld_acquire_u32(&a.bar[1]) != target) {
+                if (++it > a.spin_limit || *(volatile int*)a.err) {
+                    abort = 1;
+                    atomicExch(a.err, 1);
+                    break;
+                }
+                __nanosleep(128);
+            }
+        }
+        __threadfence();
+        *s_abort = abort;
+    }
+    __syncthreads();
+    return *s_abort == 0;
+}
+
+// Every phase of one (or two) coarse steps in one cooperative launch.
+template <int MODEL, bool NOISE>
+__global__ void __launch_bounds__(256) amr_persistent(PersistArgs a) {
+    __shared__ double sp[kWin * kWin], su[kWin * kWin];
+    __shared__ int s_abort;
+    // the phase table is read-only: the next phase's descriptor is fetched
+    // into the other half of this buffer while the current phase runs
+    __shared__ Phase s_ph[2];
+    constexpr int kWords = (int)(sizeof(Phase) / sizeof(int));
+    static_assert(sizeof(Phase) % sizeof(int) == 0, "Phase is copied as words");
+    unsigned target = 0;
+    if (threadIdx.x == 0) {
+        s_abort = *(volatile int*)a.err;  // an earlier launch gave up: do nothing
+        target = ld_acquire_u32(&a.bar[1]);
+    }
+    for (int k = threadIdx.x; k < kWords; k += blockDim.x)
+        ((int*)&s_ph[0])[k] = ((const int*)&a.phases[0])[k];
+    __syncthreads();
+    if (s_abort) return;
+    for (int p = 0; p < a.nphases; ++p) {
+        const Phase& ph = s_ph[p & 1];
+        if (p + 1 < a.nphases && threadIdx.x >= blockDim.x - 32)  // last warp prefetches
+            for (int k = threadIdx.x - (blockDim.x - 32); k < kWords; k += 32)
+                ((int*)&s_ph[(p + 1) & 1])[k] = ((const int*)&a.phases[p + 1])[k];
+        if (ph.kind == 0) {
+            TileArgs t{};
+            t.tiles = (ph.level == 0 ? a.tiles0 : a.tiles) + ph.first;
+            t.ntiles = ph.count;
+            t.tfill = ph.level == 0 ? a.tfill0 : a.tfill;
+            t.in = ph.in ? a.arena1 : a.arena0;
+            t.out = ph.in ? a.arena0 : a.arena1;
+            t.cnew = ph.cnew ? a.arena1 : a.arena0;
+            t.cold = ph.cold ? a.arena1 : a.arena0;
+            t.alpha = ph.alpha;
+            t.interp = ph.interp;
+            t.dt = ph.dt;
+            t.seed = a.seed;
+            t.scale_amp = ph.scale_amp;
+            const double t0 = __ldcg(&a.tdev[ph.slot]);
+            if (ph.write_t && blockIdx.x == 0 && threadIdx.x == 0) a.tdev[ph.slot ^ 1] = t0 + ph.dt0;
+            const double tt = NOISE ? chain_time(t0, ph.chain) : 0.0;
+            for (int64_t ti = blockIdx.x; ti < t.ntiles; ti += gridDim.x) {
+                if (MODEL == LG_MODEL_C)
+                    modelc_tile<NOISE>(t, a.mc[ph.level], t.tiles[ti], tt, sp, su);
+                else
+                    heat_tile(t, a.kappa, a.mc[ph.level].ih0, a.mc[ph.level].ih1, t.tiles[ti], sp);
+            }
+        } else {
+            double* C = ph.cnew ? a.arena1 : a.arena0;
+            const double* F = ph.in ? a.arena1 : a.arena0;
+            restrict_ops(C, F, a.rops + ph.first, ph.count, ph.r, ph.inv, 0, a.nfields);
+        }
+        const bool sync = ph.barrier && p + 1 < a.nphases;
+        if (sync) {
+            if (!grid_sync(a, target, &s_abort)) return;
+        } else {
+            __syncthreads();  // the prefetched descriptor is complete before it is read
         }
     }
 }
@@ -253,6 +433,25 @@ T* dev_upload(const std::vector<T>& v, cudaError_t* err) {
 
 }  // namespace
 
+namespace {
+// the tile height of a level's plans and the rows each warp of a tile owns
+struct TileShape {
+    int rows, rows_per_warp;
+};
+// one blob on the device holding every table of a Plans
+struct Tables {
+    char* d = nullptr;
+    size_t cap = 0;
+    BlockDesc* blocks = nullptr;
+    int64_t* lo = nullptr;
+    GhostOp* fill = nullptr;
+    RestrictOp* restrict_ops = nullptr;
+    Unit* units = nullptr;
+    lg::amr::Tile* tiles = nullptr;
+    GhostOp* tfill = nullptr;
+};
+}  // namespace
+
 struct lg_amr_sim {
     lg_ctx* ctx = nullptr;
     lg::amr::Layout layout;
@@ -265,15 +464,12 @@ struct lg_amr_sim {
     bool has_policy = false;
     lg::amr::Policy policy;
     int nfields = 2;
-    // device
+    lg::amr::Plans plans0;  // level 0's ring, tiles and units: built once
+    // device: two state arenas (ping-pong per level) of arena_cap elements,
+    // and the plan tables (tab0 from plans0, uploaded once; tab from plans)
     double* arena[2] = {nullptr, nullptr};
-    double* snap = nullptr;
-    BlockDesc* d_blocks = nullptr;
-    int64_t* d_lo = nullptr;
-    FillOp* d_fill = nullptr;
-    Corner* d_corners = nullptr;
-    RestrictOp* d_restrict = nullptr;
-    Unit* d_units = nullptr;
+    int64_t arena_cap = 0;
+    Tables tab0, tab;
     int64_t* d_tags = nullptr;
     int64_t tag_cap = 0;
     unsigned long long* d_count = nullptr;
@@ -283,6 +479,14 @@ struct lg_amr_sim {
     double t = 0.0;
     int64_t step_index = 0, epoch = 0;
     std::map<std::string, std::pair<cudaGraphExec_t, int64_t>> graphs;  // exec, launches
+    // persistent path: phase tables per (epoch, dt, slot, buffers, steps),
+    // the grid barrier's state and its error flag
+    std::map<std::string, std::pair<void*, int>> phase_tabs;  // device table, phase count
+    unsigned* d_bar = nullptr;
+    int* d_err = nullptr;
+    int coop_grid[2] = {0, 0};  // per model kind (noise-free / noisy) once measured
+    std::vector<double> host_old, host_new;  // regrid staging
+    std::vector<TileShape> tile_shapes;      // per level
 };
 
 namespace {
@@ -295,56 +499,32 @@ int fail(lg_amr_sim* s, int code, const std::string& m) { return lg::abi_fail(s 
         if (e_ != cudaSuccess) return fail((s), LG_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
     } while (0)
 
+void drop_graphs(lg_amr_sim* s) {
+    for (auto& kv : s->graphs) cudaGraphExecDestroy(kv.second.first);
+    s->graphs.clear();
+    for (auto& kv : s->phase_tabs) cudaFree(kv.second.first);
+    s->phase_tabs.clear();
+}
+
 void free_device(lg_amr_sim* s) {
+    drop_graphs(s);
     for (double*& a : s->arena) {
         cudaFree(a);
         a = nullptr;
     }
-    cudaFree(s->snap);
-    cudaFree(s->d_blocks);
-    cudaFree(s->d_lo);
-    cudaFree(s->d_fill);
-    cudaFree(s->d_corners);
-    cudaFree(s->d_restrict);
-    cudaFree(s->d_units);
-    s->snap = nullptr;
-    s->d_blocks = nullptr;
-    s->d_lo = nullptr;
-    s->d_fill = nullptr;
-    s->d_corners = nullptr;
-    s->d_restrict = nullptr;
-    s->d_units = nullptr;
-    for (auto& kv : s->graphs) cudaGraphExecDestroy(kv.second.first);
-    s->graphs.clear();
+    s->arena_cap = 0;
+    for (Tables* t : {&s->tab0, &s->tab}) {
+        cudaFree(t->d);
+        *t = Tables{};
+    }
 }
 
-// (re)build plans and device tables for s->layout; fresh zeroed arenas
-int setup_device(lg_amr_sim* s) {
-    free_device(s);
-    s->plans = lg::amr::build_plans(s->layout, s->nfields, 1024);
-    if (!s->plans.error.empty()) return fail(s, LG_ERR_STATE, s->plans.error);
-    cudaError_t e = cudaSuccess;
-    std::vector<int64_t> lo;
-    for (const auto& p : s->layout.patches) {
-        lo.push_back(p.bx.lo[0]);
-        lo.push_back(p.bx.lo[1]);
-    }
-    s->d_blocks = dev_upload(s->plans.blocks, &e);
-    if (e == cudaSuccess) s->d_lo = dev_upload(lo, &e);
-    if (e == cudaSuccess) s->d_fill = dev_upload(s->plans.fill, &e);
-    if (e == cudaSuccess) s->d_corners = dev_upload(s->plans.corners, &e);
-    if (e == cudaSuccess) s->d_restrict = dev_upload(s->plans.restrict_ops, &e);
-    if (e == cudaSuccess) s->d_units = dev_upload(s->plans.units, &e);
-    const size_t bytes = (size_t)s->plans.arena_elems * sizeof(double);
-    for (int k = 0; k < 2 && e == cudaSuccess; ++k) {
-        e = cudaMalloc(&s->arena[k], bytes);
-        if (e == cudaSuccess) e = cudaMemset(s->arena[k], 0, bytes);
-    }
-    if (e == cudaSuccess) e = cudaMalloc(&s->snap, bytes);
-    if (e == cudaSuccess) e = cudaMemset(s->snap, 0, bytes);
-    if (e != cudaSuccess) return fail(s, LG_ERR_NOMEM, std::string("AMR device setup: ") + cudaGetErrorString(e));
-    s->cur.assign(s->layout.num_levels(), 0);
-    return LG_OK;
+// elements of the level-0 slabs, which lead every arena (the base tiling
+// never changes, so this prefix is the same in every layout)
+int64_t level0_elems(const lg_amr_sim* s) {
+    const uint32_t b1 = s->layout.level_start[1];
+    const BlockDesc& last = s->plans.blocks[b1 - 1];
+    return last.off + last.stride * s->nfields;
 }
 
 // level l's slabs are contiguous in the arena: [off of its first block, end of its last)
@@ -355,13 +535,183 @@ std::pair<int64_t, int64_t> level_range(const lg_amr_sim* s, int level) {
     return {s->plans.blocks[b0].off, last.off + last.stride * s->nfields};
 }
 
-int launch_fill(lg_amr_sim* s, int level, bool interp, double alpha) {
-    const int64_t a = s->plans.fill_start[level], b = s->plans.fill_start[level + 1];
+// Tile shape per level.  A level with enough cells to fill the GPU several
+// times over is throughput-bound: 32-row tiles, four rows per warp, so that
+// each face flux is shared down a warp's rows.  A sparse fine level is
+// latency-bound (its launch is one short wave): tiles of at most 8 rows with
+// one row per warp, the tallest that still gives two tiles per SM.
+constexpr int kSMs = 148;
+std::vector<TileShape> choose_tile_shapes(const lg::amr::Layout& g) {
+    std::vector<TileShape> shapes(g.max_levels(), TileShape{lg::amr::kTile, 4});
+    for (int l = 0; l < g.num_levels(); ++l) {
+        int64_t cells = 0;
+        for (uint32_t b = g.level_start[l]; b < g.level_start[l + 1]; ++b) cells += g.patches[b].bx.cells();
+        if (cells >= (int64_t)kSMs * 2048) continue;
+        for (int r : {8, 4, 2, 1}) {
+            int64_t tiles = 0;
+            for (uint32_t b = g.level_start[l]; b < g.level_start[l + 1]; ++b) {
+                const auto& bx = g.patches[b].bx;
+                tiles += ((bx.extent(0) + lg::amr::kTile - 1) / lg::amr::kTile) * ((bx.extent(1) + r - 1) / r);
+            }
+            shapes[l] = TileShape{r, 1};
+            if (tiles >= 2 * kSMs) break;
+        }
+    }
+    return shapes;
+}
+std::vector<int> rows_of(const std::vector<TileShape>& s) {
+    std::vector<int> r;
+    for (const auto& t : s) r.push_back(t.rows);
+    return r;
+}
+int tile_threads(const TileShape& t) { return 32 * std::max(1, (t.rows + t.rows_per_warp - 1) / t.rows_per_warp); }
+
+// pack every table of `P` into one blob and upload it into `T`
+// (stream-ordered; the caller has synchronised the stream, so no kernel
+// reads the old tables)
+int upload_tables(lg_amr_sim* s, const lg::amr::Plans& P, const lg::amr::Layout& g, Tables& T) {
+    std::vector<int64_t> lo;
+    for (const auto& p : g.patches) {
+        lo.push_back(p.bx.lo[0]);
+        lo.push_back(p.bx.lo[1]);
+    }
+    size_t off = 0;
+    auto reserve = [&](size_t bytes) {
+        const size_t o = off;
+        off += (bytes + 255) / 256 * 256;
+        return o;
+    };
+    const size_t o_blocks = reserve(P.blocks.size() * sizeof(BlockDesc));
+    const size_t o_lo = reserve(lo.size() * sizeof(int64_t));
+    const size_t o_fill = reserve(P.fill.size() * sizeof(GhostOp));
+    const size_t o_restrict = reserve(P.restrict_ops.size() * sizeof(RestrictOp));
+    const size_t o_units = reserve(P.units.size() * sizeof(Unit));
+    const size_t o_tiles = reserve(P.tiles.size() * sizeof(lg::amr::Tile));
+    const size_t o_tfill = reserve(P.tile_fill.size() * sizeof(GhostOp));
+    std::vector<char> blob(std::max<size_t>(off, 256), 0);
+    auto put = [&](size_t o, const void* src, size_t bytes) {
+        if (bytes) std::memcpy(blob.data() + o, src, bytes);
+    };
+    put(o_blocks, P.blocks.data(), P.blocks.size() * sizeof(BlockDesc));
+    put(o_lo, lo.data(), lo.size() * sizeof(int64_t));
+    put(o_fill, P.fill.data(), P.fill.size() * sizeof(GhostOp));
+    put(o_restrict, P.restrict_ops.data(), P.restrict_ops.size() * sizeof(RestrictOp));
+    put(o_units, P.units.data(), P.units.size() * sizeof(Unit));
+    put(o_tiles, P.tiles.data(), P.tiles.size() * sizeof(lg::amr::Tile));
+    put(o_tfill, P.tile_fill.data(), P.tile_fill.size() * sizeof(GhostOp));
+    if (blob.size() > T.cap) {
+        cudaFree(T.d);
+        T = Tables{};
+        const size_t cap = blob.size() + blob.size() / 4;
+        AMR_CUDA(s, cudaMalloc(&T.d, cap));
+        T.cap = cap;
+    }
+    cudaStream_t st = lg::abi_stream(s->ctx);
+    AMR_CUDA(s, cudaMemcpyAsync(T.d, blob.data(), blob.size(), cudaMemcpyHostToDevice, st));
+    AMR_CUDA(s, cudaStreamSynchronize(st));
+    T.blocks = (BlockDesc*)(T.d + o_blocks);
+    T.lo = (int64_t*)(T.d + o_lo);
+    T.fill = (GhostOp*)(T.d + o_fill);
+    T.restrict_ops = (RestrictOp*)(T.d + o_restrict);
+    T.units = (Unit*)(T.d + o_units);
+    T.tiles = (lg::amr::Tile*)(T.d + o_tiles);
+    T.tfill = (GhostOp*)(T.d + o_tfill);
+    return LG_OK;
+}
+
+// the ring, tile and unit lists of a level: level 0's are built once
+struct Lists {
+    const lg::amr::Plans* P;
+    const Tables* T;
+};
+Lists lists(const lg_amr_sim* s, int level) {
+    return level == 0 ? Lists{&s->plans0, &s->tab0} : Lists{&s->plans, &s->tab};
+}
+
+// arenas of at least `need` elements; when they are reallocated, the first
+// `keep` elements of the buffer `from` move to the new buffer 0 and the
+// function returns 0 in *now, else *now = from
+int ensure_arenas(lg_amr_sim* s, int64_t need, int64_t keep, int from, int* now) {
+    *now = from;
+    if (need <= s->arena_cap) return LG_OK;
+    cudaStream_t st = lg::abi_stream(s->ctx);
+    const int64_t cap = need + need / 4;
+    const size_t bytes = (size_t)cap * sizeof(double);
+    double* fresh[2] = {nullptr, nullptr};
+    cudaError_t e = cudaMalloc(&fresh[0], bytes);
+    if (e == cudaSuccess) e = cudaMalloc(&fresh[1], bytes);
+    if (e == cudaSuccess) e = cudaMemsetAsync(fresh[0], 0, bytes, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(fresh[1], 0, bytes, st);
+    if (e == cudaSuccess && keep > 0 && s->arena[from])
+        e = cudaMemcpyAsync(fresh[0], s->arena[from], (size_t)keep * sizeof(double), cudaMemcpyDeviceToDevice, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) {
+        cudaFree(fresh[0]);
+        cudaFree(fresh[1]);
+        return fail(s, LG_ERR_NOMEM, std::string("AMR arena allocation: ") + cudaGetErrorString(e));
+    }
+    drop_graphs(s);  // graphs hold the old arena pointers
+    for (int k = 0; k < 2; ++k) {
+        cudaFree(s->arena[k]);
+        s->arena[k] = fresh[k];
+    }
+    s->arena_cap = cap;
+    *now = 0;
+    return LG_OK;
+}
+
+// plans, tables and zeroed arenas for a fresh simulation
+int setup_device(lg_amr_sim* s) {
+    lg::amr::Layout base;
+    std::string err = lg::amr::build_layout(s->layout.base, s->layout.ratios, {}, &base);
+    if (!err.empty()) return fail(s, LG_ERR_STATE, err);
+    s->tile_shapes = choose_tile_shapes(s->layout);
+    s->plans0 = lg::amr::build_plans(base, s->nfields, 1024, 0, rows_of(s->tile_shapes));
+    s->plans = lg::amr::build_plans(s->layout, s->nfields, 1024, 1, rows_of(s->tile_shapes));
+    if (!s->plans.error.empty()) return fail(s, LG_ERR_STATE, s->plans.error);
+    int rc = upload_tables(s, s->plans0, base, s->tab0);
+    if (rc == LG_OK) rc = upload_tables(s, s->plans, s->layout, s->tab);
+    if (rc != LG_OK) return rc;
+    int now = 0;
+    rc = ensure_arenas(s, s->plans.arena_elems, 0, 0, &now);
+    if (rc != LG_OK) return rc;
+    s->cur.assign(s->layout.num_levels(), 0);
+    return LG_OK;
+}
+
+// the whole state (each level's current buffer) into `host`, arena layout
+int download_state(lg_amr_sim* s, std::vector<double>& host) {
+    cudaStream_t st = lg::abi_stream(s->ctx);
+    host.resize((size_t)s->plans.arena_elems);
+    for (int l = 0; l < s->layout.num_levels(); ++l) {
+        const auto r = level_range(s, l);
+        if (r.second > r.first)
+            AMR_CUDA(s, cudaMemcpyAsync(host.data() + r.first, s->arena[s->cur[l]] + r.first,
+                                        (size_t)(r.second - r.first) * sizeof(double), cudaMemcpyDeviceToHost, st));
+    }
+    AMR_CUDA(s, cudaStreamSynchronize(st));
+    return LG_OK;
+}
+
+int upload_state(lg_amr_sim* s, const std::vector<double>& host) {
+    cudaStream_t st = lg::abi_stream(s->ctx);
+    for (int l = 0; l < s->layout.num_levels(); ++l) {
+        const auto r = level_range(s, l);
+        if (r.second > r.first)
+            AMR_CUDA(s, cudaMemcpyAsync(s->arena[s->cur[l]] + r.first, host.data() + r.first,
+                                        (size_t)(r.second - r.first) * sizeof(double), cudaMemcpyHostToDevice, st));
+    }
+    AMR_CUDA(s, cudaStreamSynchronize(st));
+    return LG_OK;
+}
+
+int launch_fill(lg_amr_sim* s, int level) {
+    const Lists L = lists(s, level);
+    const int64_t a = L.P->fill_start[level], b = L.P->fill_start[level + 1];
     if (b == a) return LG_OK;
     const double* coarse = level > 0 ? s->arena[s->cur[level - 1]] : nullptr;
-    amr_fill_kernel<<<grid_for(b - a, 256), 256, 0, lg::abi_stream(s->ctx)>>>(
-        s->d_blocks, s->arena[s->cur[level]], coarse, s->snap, s->d_fill + a, b - a, s->d_corners, s->nfields, alpha,
-        interp ? 1 : 0);
+    amr_fill_kernel<<<grid_for(b - a, 256), 256, 0, lg::abi_stream(s->ctx)>>>(s->arena[s->cur[level]], coarse,
+                                                                                L.T->fill + a, b - a, s->nfields);
     lg::abi_count_launch(s->ctx, 1);
     AMR_CUDA(s, cudaGetLastError());
     return LG_OK;
@@ -373,7 +723,7 @@ int launch_restrict(lg_amr_sim* s, int fine, int f0, int f1) {
     const int r = (int)s->layout.ratios[fine - 1];
     const double inv = 1.0 / ((double)r * (double)r);
     amr_restrict_kernel<<<grid_for(b - a, 256), 256, 0, lg::abi_stream(s->ctx)>>>(
-        s->d_blocks, s->arena[s->cur[fine - 1]], s->arena[s->cur[fine]], s->d_restrict + a, b - a, r, inv, f0, f1);
+        s->arena[s->cur[fine - 1]], s->arena[s->cur[fine]], s->tab.restrict_ops + a, b - a, r, inv, f0, f1);
     lg::abi_count_launch(s->ctx, 1);
     AMR_CUDA(s, cudaGetLastError());
     return LG_OK;
@@ -398,32 +748,45 @@ lg::MC<double> level_mc(const lg_amr_sim* s, int level) {
     return lg::to_mc<double>(m);
 }
 
-// one Euler-Maruyama update of the units [u0, u1) (level l, or every level
-// for the global-dt path), reading buffer `in_buf` and writing the other
-int launch_step(lg_amr_sim* s, int level_for_consts, int64_t u0, int64_t u1, int in_buf, double dt,
-                const TimeChain& chain, bool write_t, double dt0) {
-    if (u1 == u0) return LG_OK;
-    StepArgs a{};
-    a.blocks = s->d_blocks;
-    a.units = s->d_units + u0;
-    a.nunits = u1 - u0;
-    a.in = s->arena[in_buf];
-    a.out = s->arena[in_buf ^ 1];
+// one fused ghost fill + Euler-Maruyama update of level `level`, reading
+// its current buffer and writing the other; the coarse source is the
+// coarse level's current buffer, blended with its pre-step buffer when
+// `interp`
+int launch_level(lg_amr_sim* s, int level, bool interp, double alpha, double dt, const TimeChain& chain,
+                 bool write_t, double dt0) {
+    const Lists L = lists(s, level);
+    const int64_t t0 = L.P->tile_start[level], t1 = L.P->tile_start[level + 1];
+    if (t1 == t0) return LG_OK;
+    TileArgs a{};
+    a.tiles = L.T->tiles + t0;
+    a.ntiles = t1 - t0;
+    a.tfill = L.T->tfill;
+    const int in = s->cur[level];
+    a.in = s->arena[in];
+    a.out = s->arena[in ^ 1];
+    a.cnew = level > 0 ? s->arena[s->cur[level - 1]] : nullptr;
+    a.cold = level > 0 ? s->arena[s->cur[level - 1] ^ 1] : nullptr;
+    a.alpha = alpha;
+    a.interp = interp ? 1 : 0;
     a.dt = dt;
     a.tdev = s->d_t;
     a.slot = s->tslot;
     a.write_t = write_t ? 1 : 0;
     a.dt0 = dt0;
     a.chain = chain;
-    a.noise = (s->model == LG_MODEL_C && s->mp.noise_amplitude != 0.0) ? 1 : 0;
     a.seed = s->seed;
     a.scale_amp = std::sqrt(dt) * s->mp.noise_amplitude;
-    const unsigned g = (unsigned)std::min<int64_t>(u1 - u0, 65535);
+    const unsigned g = (unsigned)std::min<int64_t>(t1 - t0, kSMs * 16);
+    const int threads = tile_threads(s->tile_shapes[level]);
+    cudaStream_t st = lg::abi_stream(s->ctx);
     if (s->model == LG_MODEL_C) {
-        amr_modelc_kernel<<<g, 256, 0, lg::abi_stream(s->ctx)>>>(a, level_mc(s, level_for_consts));
+        if (s->mp.noise_amplitude != 0.0)
+            amr_modelc_tiles<true><<<g, threads, 0, st>>>(a, level_mc(s, level));
+        else
+            amr_modelc_tiles<false><<<g, threads, 0, st>>>(a, level_mc(s, level));
     } else {
-        const auto& h = s->layout.level_spacing[level_for_consts];
-        amr_heat_kernel<<<g, 256, 0, lg::abi_stream(s->ctx)>>>(a, s->kappa, 1.0 / (h[0] * h[0]), 1.0 / (h[1] * h[1]));
+        const auto& h = s->layout.level_spacing[level];
+        amr_heat_tiles<<<g, threads, 0, st>>>(a, s->kappa, 1.0 / (h[0] * h[0]), 1.0 / (h[1] * h[1]));
     }
     lg::abi_count_launch(s->ctx, 1);
     AMR_CUDA(s, cudaGetLastError());
@@ -437,23 +800,13 @@ double stable_dt_at(const lg_amr_sim* s, int level) {
     return 0.25 * (hm * hm) / s->kappa;                                     // tests/amr.rs:341-343
 }
 
-// Subcycle::advance (subcycling.rs:195-267)
+// Subcycle::advance (subcycling.rs:195-267): ghosts (coarse source
+// interpolated in time) and the step of this level in one launch, then the
+// next level subcycled and restricted
 int advance(lg_amr_sim* s, int level, TimeChain chain, double dt, double alpha, bool first) {
-    cudaStream_t st = lg::abi_stream(s->ctx);
-    // 1. snapshot this level (only level-l slabs are ever read from it)
-    auto rng = level_range(s, level);
-    if (rng.second > rng.first)
-        AMR_CUDA(s, cudaMemcpyAsync(s->snap + rng.first, s->arena[s->cur[level]] + rng.first,
-                                    (rng.second - rng.first) * sizeof(double), cudaMemcpyDeviceToDevice, st));
-    // 2. ghosts of this level, coarse source interpolated in time
-    int rc = launch_fill(s, level, level > 0, alpha);
-    if (rc != LG_OK) return rc;
-    // 3. Euler-Maruyama on this level's blocks
-    rc = launch_step(s, level, s->plans.unit_start[level], s->plans.unit_start[level + 1], s->cur[level], dt, chain,
-                     first, dt);
+    int rc = launch_level(s, level, level > 0, alpha, dt, chain, first, dt);
     if (rc != LG_OK) return rc;
     s->cur[level] ^= 1;
-    // 4. subcycle the next level, then restrict it
     const int child = level + 1;
     if (child < s->layout.num_levels()) {
         const double n_f = std::round(stable_dt_at(s, level) / stable_dt_at(s, child));
@@ -474,21 +827,186 @@ int advance(lg_amr_sim* s, int level, TimeChain chain, double dt, double alpha, 
     return LG_OK;
 }
 
-// the model's AMR fill_ghosts (phasefield.rs:454-467): restrict then fill,
-// for fields [f0, f1)
-int sync_fields(lg_amr_sim* s, int f0, int f1) {
+// The phases of Subcycle::advance from `level` down, recorded instead of
+// launched: the same buffer bookkeeping as advance(), on copies.
+void record_advance(const lg_amr_sim* s, int level, TimeChain chain, double dt, double alpha, bool first,
+                    std::vector<int>& cur, int slot, std::vector<Phase>& out) {
+    const Lists L = lists(s, level);
+    Phase ph{};
+    ph.kind = 0;
+    ph.level = level;
+    ph.in = cur[level];
+    ph.cnew = level > 0 ? cur[level - 1] : 0;
+    ph.cold = level > 0 ? cur[level - 1] ^ 1 : 0;
+    ph.interp = level > 0 ? 1 : 0;
+    ph.write_t = first ? 1 : 0;
+    ph.slot = slot;
+    ph.barrier = 1;
+    ph.first = L.P->tile_start[level];
+    ph.count = L.P->tile_start[level + 1] - ph.first;
+    ph.alpha = alpha;
+    ph.dt = dt;
+    ph.dt0 = dt;
+    ph.scale_amp = std::sqrt(dt) * s->mp.noise_amplitude;
+    ph.chain = chain;
+    out.push_back(ph);
+    cur[level] ^= 1;
+    const int child = level + 1;
+    if (child < s->layout.num_levels()) {
+        const double n_f = std::round(stable_dt_at(s, level) / stable_dt_at(s, child));
+        const uint64_t n = (uint64_t)std::max(n_f, 1.0);
+        const double dt_child = dt / (double)n;
+        for (uint64_t k = 0; k < n; ++k) {
+            TimeChain c = chain;
+            c.s[c.depth] = (int)k;
+            c.dt[c.depth] = dt_child;
+            c.depth += 1;
+            record_advance(s, child, c, dt_child, (double)k / (double)n, false, cur, slot, out);
+        }
+        Phase rp{};
+        rp.kind = 1;
+        rp.level = child;
+        rp.in = cur[child];
+        rp.cnew = cur[child - 1];
+        rp.barrier = 1;
+        rp.first = s->plans.restrict_start[child];
+        rp.count = s->plans.restrict_start[child + 1] - rp.first;
+        rp.r = (int)s->layout.ratios[child - 1];
+        rp.inv = 1.0 / ((double)rp.r * (double)rp.r);
+        if (rp.count > 0) out.push_back(rp);
+    }
+}
+
+// one coarse step of either integrator, recorded
+void record_coarse_step(const lg_amr_sim* s, double dt, std::vector<int>& cur, int slot, std::vector<Phase>& out) {
+    TimeChain c{};
+    if (s->integrator == LG_AMR_SUBCYCLING) {
+        record_advance(s, 0, c, dt, 0.0, true, cur, slot, out);
+        return;
+    }
     for (int fine = s->layout.num_levels() - 1; fine >= 1; --fine) {
-        int rc = launch_restrict(s, fine, f0, f1);
-        if (rc != LG_OK) return rc;
+        Phase rp{};
+        rp.kind = 1;
+        rp.level = fine;
+        rp.in = cur[fine];
+        rp.cnew = cur[fine - 1];
+        rp.barrier = 1;
+        rp.first = s->plans.restrict_start[fine];
+        rp.count = s->plans.restrict_start[fine + 1] - rp.first;
+        rp.r = (int)s->layout.ratios[fine - 1];
+        rp.inv = 1.0 / ((double)rp.r * (double)rp.r);
+        if (rp.count > 0) out.push_back(rp);
     }
-    // per-field fill: the plan fills all fields; fill only [f0, f1) by
-    // temporarily narrowing nfields is not possible, so fill all fields --
-    // their values are consistent with the reference only when every field
-    // is being synchronised, which is the case for the model's fill.
-    for (int level = 0; level < s->layout.num_levels(); ++level) {
-        int rc = launch_fill(s, level, false, 0.0);
-        if (rc != LG_OK) return rc;
+    // every level steps from the pre-step buffers: one phase, no barriers
+    // between the levels' tile lists
+    const int L = s->layout.num_levels();
+    for (int l = 0; l < L; ++l) {
+        const Lists lst = lists(s, l);
+        Phase ph{};
+        ph.kind = 0;
+        ph.level = l;
+        ph.in = cur[l];
+        ph.cnew = l > 0 ? cur[l - 1] : 0;
+        ph.cold = ph.cnew;
+        ph.write_t = l == 0 ? 1 : 0;
+        ph.slot = slot;
+        ph.barrier = l == L - 1 ? 1 : 0;
+        ph.first = lst.P->tile_start[l];
+        ph.count = lst.P->tile_start[l + 1] - ph.first;
+        ph.dt = dt;
+        ph.dt0 = dt;
+        ph.scale_amp = std::sqrt(dt) * s->mp.noise_amplitude;
+        ph.chain = c;
+        out.push_back(ph);
     }
+    for (int l = 0; l < L; ++l) cur[l] ^= 1;
+}
+
+template <int MODEL, bool NOISE>
+int launch_persistent_kernel(lg_amr_sim* s, const PersistArgs& a) {
+    const int kind = NOISE ? 1 : 0;
+    auto kernel = amr_persistent<MODEL, NOISE>;
+    if (s->coop_grid[kind] == 0) {
+        int per_sm = 0, sms = 0;
+        AMR_CUDA(s, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 256, 0));
+        AMR_CUDA(s, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, lg::abi_device(s->ctx)));
+        if (per_sm < 1) return fail(s, LG_ERR_DEVICE, "persistent AMR kernel cannot be resident");
+        s->coop_grid[kind] = per_sm * sms;
+    }
+    PersistArgs args = a;
+    void* params[] = {&args};
+    AMR_CUDA(s, cudaLaunchCooperativeKernel((const void*)kernel, dim3((unsigned)s->coop_grid[kind]), dim3(256), params,
+                                            0, lg::abi_stream(s->ctx)));
+    lg::abi_count_launch(s->ctx, 1);
+    return LG_OK;
+}
+
+// `nsteps` (1 or 2) coarse steps in one cooperative launch
+int run_persistent(lg_amr_sim* s, double dt, int nsteps) {
+    char key[160];
+    snprintf(key, sizeof key, "%lld|%a|%d|%d|", (long long)s->epoch, dt, s->tslot, nsteps);
+    std::string k = key;
+    for (int c : s->cur) k += c ? '1' : '0';
+    std::vector<int> cur = s->cur;
+    int slot = s->tslot;
+    auto it = s->phase_tabs.find(k);
+    if (it == s->phase_tabs.end()) {
+        std::vector<Phase> ph;
+        for (int n = 0; n < nsteps; ++n) {
+            record_coarse_step(s, dt, cur, slot, ph);
+            slot ^= 1;
+        }
+        void* d = nullptr;
+        AMR_CUDA(s, cudaMalloc(&d, ph.size() * sizeof(Phase)));
+        cudaStream_t st = lg::abi_stream(s->ctx);
+        cudaError_t e = cudaMemcpyAsync(d, ph.data(), ph.size() * sizeof(Phase), cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) {
+            cudaFree(d);
+            return fail(s, LG_ERR_CUDA, std::string("phase table upload: ") + cudaGetErrorString(e));
+        }
+        it = s->phase_tabs.emplace(k, std::make_pair(d, (int)ph.size())).first;
+    } else {
+        std::vector<Phase> ph;
+        for (int n = 0; n < nsteps; ++n) {  // the buffer bookkeeping only
+            record_coarse_step(s, dt, cur, slot, ph);
+            slot ^= 1;
+        }
+    }
+    PersistArgs a{};
+    a.phases = (const Phase*)it->second.first;
+    a.nphases = it->second.second;
+    a.tiles0 = s->tab0.tiles;
+    a.tfill0 = s->tab0.tfill;
+    a.tiles = s->tab.tiles;
+    a.tfill = s->tab.tfill;
+    a.rops = s->tab.restrict_ops;
+    a.arena0 = s->arena[0];
+    a.arena1 = s->arena[1];
+    a.tdev = s->d_t;
+    a.seed = s->seed;
+    a.nfields = s->nfields;
+    a.kappa = s->kappa;
+    for (int l = 0; l < s->layout.num_levels() && l < kMaxDepth; ++l) {
+        a.mc[l] = level_mc(s, l);
+        if (s->model != LG_MODEL_C) {
+            const auto& h = s->layout.level_spacing[l];
+            a.mc[l].ih0 = 1.0 / (h[0] * h[0]);
+            a.mc[l].ih1 = 1.0 / (h[1] * h[1]);
+        }
+    }
+    a.bar = s->d_bar;
+    a.err = s->d_err;
+    a.spin_limit = 4000000;  // polls of >= 128 ns: well over a second
+    int rc;
+    if (s->model == LG_MODEL_C)
+        rc = s->mp.noise_amplitude != 0.0 ? launch_persistent_kernel<LG_MODEL_C, true>(s, a)
+                                          : launch_persistent_kernel<LG_MODEL_C, false>(s, a);
+    else
+        rc = launch_persistent_kernel<LG_MODEL_HEAT, false>(s, a);
+    if (rc != LG_OK) return rc;
+    s->cur = cur;
+    s->tslot = slot;
     return LG_OK;
 }
 
@@ -498,43 +1016,21 @@ int one_coarse_step(lg_amr_sim* s, double dt) {
         int rc = advance(s, 0, c, dt, 0.0, true);
         if (rc != LG_OK) return rc;
     } else {
-        int rc = sync_fields(s, 0, s->nfields);
-        if (rc != LG_OK) return rc;
-        // every level steps together; buffers of all levels agree here
+        // the model's AMR fill_ghosts (phasefield.rs:454-467): restrict, then
+        // every level filled and stepped together from the pre-step buffers
+        for (int fine = s->layout.num_levels() - 1; fine >= 1; --fine) {
+            int rc = launch_restrict(s, fine, 0, s->nfields);
+            if (rc != LG_OK) return rc;
+        }
         for (int l = 1; l < s->layout.num_levels(); ++l)
             if (s->cur[l] != s->cur[0]) return fail(s, LG_ERR_STATE, "level buffers out of step");
         for (int l = 0; l < s->layout.num_levels(); ++l) {
-            rc = launch_step(s, l, s->plans.unit_start[l], s->plans.unit_start[l + 1], s->cur[l], dt, c, l == 0, dt);
+            int rc = launch_level(s, l, false, 0.0, dt, c, l == 0, dt);
             if (rc != LG_OK) return rc;
         }
         for (int l = 0; l < s->layout.num_levels(); ++l) s->cur[l] ^= 1;
     }
     s->tslot ^= 1;
-    return LG_OK;
-}
-
-// host copies of field f of every block (current buffer of its level)
-int download_blocks(lg_amr_sim* s, int f, std::vector<std::vector<double>>& out) {
-    cudaStream_t st = lg::abi_stream(s->ctx);
-    out.assign(s->layout.num_blocks(), {});
-    for (int b = 0; b < s->layout.num_blocks(); ++b) {
-        const BlockDesc& d = s->plans.blocks[b];
-        out[b].resize((size_t)(d.nx + 2) * (d.ny + 2));
-        AMR_CUDA(s, cudaMemcpyAsync(out[b].data(), s->arena[s->cur[d.level]] + d.off + f * d.stride,
-                                    out[b].size() * sizeof(double), cudaMemcpyDeviceToHost, st));
-    }
-    AMR_CUDA(s, cudaStreamSynchronize(st));
-    return LG_OK;
-}
-
-int upload_blocks(lg_amr_sim* s, int f, const std::vector<std::vector<double>>& in) {
-    cudaStream_t st = lg::abi_stream(s->ctx);
-    for (int b = 0; b < s->layout.num_blocks(); ++b) {
-        const BlockDesc& d = s->plans.blocks[b];
-        AMR_CUDA(s, cudaMemcpyAsync(s->arena[s->cur[d.level]] + d.off + f * d.stride, in[b].data(),
-                                    in[b].size() * sizeof(double), cudaMemcpyHostToDevice, st));
-    }
-    AMR_CUDA(s, cudaStreamSynchronize(st));
     return LG_OK;
 }
 
@@ -551,10 +1047,11 @@ int tag_level(lg_amr_sim* s, int field, int level, double threshold, std::vector
     }
     if (!s->d_count) AMR_CUDA(s, cudaMalloc(&s->d_count, sizeof(unsigned long long)));
     AMR_CUDA(s, cudaMemsetAsync(s->d_count, 0, sizeof(unsigned long long), st));
-    const int64_t u0 = s->plans.unit_start[level], u1 = s->plans.unit_start[level + 1];
+    const Lists L = lists(s, level);
+    const int64_t u0 = L.P->unit_start[level], u1 = L.P->unit_start[level + 1];
     if (u1 > u0) {
         amr_tag_kernel<<<(unsigned)std::min<int64_t>(u1 - u0, 65535), 256, 0, st>>>(
-            s->d_blocks, s->d_lo, s->d_units + u0, u1 - u0, s->arena[s->cur[level]], field, threshold, s->d_tags,
+            s->tab.blocks, s->tab.lo, L.T->units + u0, u1 - u0, s->arena[s->cur[level]], field, threshold, s->d_tags,
             s->tag_cap, s->d_count);
         lg::abi_count_launch(s->ctx, 1);
         AMR_CUDA(s, cudaGetLastError());
@@ -563,15 +1060,29 @@ int tag_level(lg_amr_sim* s, int field, int level, double threshold, std::vector
     AMR_CUDA(s, cudaMemcpyAsync(&n, s->d_count, sizeof n, cudaMemcpyDeviceToHost, st));
     AMR_CUDA(s, cudaStreamSynchronize(st));
     std::vector<int64_t> host(2 * n);
-    if (n) AMR_CUDA(s, cudaMemcpy(host.data(), s->d_tags, 2 * n * sizeof(int64_t), cudaMemcpyDeviceToHost));
+    if (n)
+        AMR_CUDA(s, cudaMemcpyAsync(host.data(), s->d_tags, 2 * n * sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+    AMR_CUDA(s, cudaStreamSynchronize(st));
     cells.resize(n);
     for (unsigned long long k = 0; k < n; ++k) cells[k] = {host[2 * k], host[2 * k + 1]};
     return LG_OK;
 }
 
+// slab pointers of field f of every block of `g`, whose arena layout is
+// `P`, inside the host arena image `base` (which starts at element `first`)
+template <class Ptr, class Vec>
+std::vector<Ptr> slab_ptrs(const lg::amr::Plans& P, Vec& base, int64_t first, int f) {
+    std::vector<Ptr> out(P.blocks.size(), nullptr);
+    for (size_t b = 0; b < P.blocks.size(); ++b)
+        if (P.blocks[b].off >= first) out[b] = base.data() + (P.blocks[b].off - first) + f * P.blocks[b].stride;
+    return out;
+}
+
 // BergerOliger::regrid (adapt.rs:152-237): prepare (restrict + fill of the
 // tagged field), tag every level on the device, build boxes on the host,
-// keep the hierarchy if acceptable, else rebuild and migrate.
+// keep the hierarchy if acceptable, else rebuild and migrate.  The level-0
+// slabs stay on the device (the base tiling never changes); refined levels
+// are sampled on the host from one download of the state.
 int maybe_regrid(lg_amr_sim* s) {
     if (!s->has_policy || s->step_index % s->policy.every != 0) return LG_OK;
     const int f = s->policy.field;
@@ -579,11 +1090,10 @@ int maybe_regrid(lg_amr_sim* s) {
         int rc = launch_restrict(s, fine, f, f + 1);
         if (rc != LG_OK) return rc;
     }
-    // the global fill of the tagged field only: fill writes every field's
-    // ghosts, and ghosts are rewritten before any other read, so the extra
-    // fields' ghost values are unobservable
+    // the global fill writes every field's ghosts; ghosts are rewritten
+    // before any other read, so the extra fields' ghost values are unobservable
     for (int level = 0; level < s->layout.num_levels(); ++level) {
-        int rc = launch_fill(s, level, false, 0.0);
+        int rc = launch_fill(s, level);
         if (rc != LG_OK) return rc;
     }
     std::vector<std::vector<std::array<int64_t, 2>>> flags(s->layout.num_levels());
@@ -596,20 +1106,82 @@ int maybe_regrid(lg_amr_sim* s) {
     lg::amr::Layout ng;
     std::string err = lg::amr::build_layout(s->layout.base, s->layout.ratios, proposed, &ng);
     if (!err.empty()) return fail(s, LG_ERR_STATE, "regrid produced an invalid hierarchy: " + err);
-    std::vector<std::vector<std::vector<double>>> migrated(s->nfields);
-    for (int k = 0; k < s->nfields; ++k) {
-        std::vector<std::vector<double>> old;
-        int rc = download_blocks(s, k, old);
-        if (rc != LG_OK) return rc;
-        lg::amr::migrate_field(s->layout, old, ng, migrated[k]);
+    std::vector<TileShape> shapes = choose_tile_shapes(ng);
+    shapes[0] = s->tile_shapes[0];  // level 0's plans are kept
+    lg::amr::Plans np = lg::amr::build_plans(ng, s->nfields, 1024, 1, rows_of(shapes));
+    if (!np.error.empty()) return fail(s, LG_ERR_STATE, np.error);
+    // download the slabs the sampling can reach: every refined slab, and the
+    // level-0 blocks within two coarse cells of a new level-1 patch (all of
+    // them, should the sampling still miss one)
+    std::vector<char> want(s->layout.num_blocks(), 0);
+    for (uint32_t b = s->layout.level_start[1]; b < (uint32_t)s->layout.num_blocks(); ++b) want[b] = 1;
+    {
+        const auto& base = s->layout.base;
+        const int64_t nbx = base.cells[0] / base.block[0], nby = base.cells[1] / base.block[1];
+        const int64_t r = ng.num_levels() > 1 ? ng.ratios[0] : 1;
+        for (uint32_t b = ng.num_levels() > 1 ? ng.level_start[1] : 0; ng.num_levels() > 1 && b < ng.level_start[2];
+             ++b) {
+            const auto& bx = ng.patches[b].bx;
+            int64_t lo[2], hi[2];
+            for (int d = 0; d < 2; ++d) {
+                lo[d] = std::max<int64_t>(0, bx.lo[d] / r - 2) / base.block[d];
+                hi[d] = std::min<int64_t>(base.cells[d] - 1, (bx.hi[d] + r - 1) / r + 1) / base.block[d];
+            }
+            for (int64_t by = lo[1]; by <= hi[1] && by < nby; ++by)
+                for (int64_t bx2 = lo[0]; bx2 <= hi[0] && bx2 < nbx; ++bx2) want[(size_t)(bx2 + by * nbx)] = 1;
+        }
+    }
+    s->host_old.resize((size_t)s->plans.arena_elems);
+    int rc = LG_OK;
+    for (int attempt = 0; attempt < 2; ++attempt) {
+        cudaStream_t st = lg::abi_stream(s->ctx);
+        const int nb = s->layout.num_blocks();
+        for (int b = 0; b < nb;) {  // runs of wanted blocks of one level are contiguous in the arena
+            if (!want[b]) {
+                ++b;
+                continue;
+            }
+            int e = b;
+            while (e + 1 < nb && want[e + 1] && s->plans.blocks[e + 1].level == s->plans.blocks[b].level) ++e;
+            const auto& first = s->plans.blocks[b];
+            const auto& last = s->plans.blocks[e];
+            const int64_t a0 = first.off, a1 = last.off + last.stride * s->nfields;
+            AMR_CUDA(s, cudaMemcpyAsync(s->host_old.data() + a0, s->arena[s->cur[first.level]] + a0,
+                                        (size_t)(a1 - a0) * sizeof(double), cudaMemcpyDeviceToHost, st));
+            b = e + 1;
+        }
+        AMR_CUDA(s, cudaStreamSynchronize(st));
+        const int64_t l0 = level0_elems(s);
+        s->host_new.assign((size_t)(np.arena_elems - l0), 0.0);
+        bool complete = true;
+        for (int k = 0; k < s->nfields; ++k) {
+            auto old = slab_ptrs<const double*>(s->plans, s->host_old, 0, k);
+            for (int b = 0; b < nb; ++b)
+                if (!want[b]) old[b] = nullptr;
+            const auto out = slab_ptrs<double*>(np, s->host_new, l0, k);
+            complete = complete && lg::amr::migrate_field(s->layout, old, ng, out, false);
+        }
+        if (complete) break;
+        if (attempt == 1) return fail(s, LG_ERR_STATE, "migration needs a slab that was not downloaded");
+        std::fill(want.begin(), want.end(), 1);
+    }
+    const int64_t l0 = level0_elems(s);
+    int keep = 0;
+    rc = ensure_arenas(s, np.arena_elems, l0, s->cur[0], &keep);
+    if (rc != LG_OK) return rc;
+    if (!s->host_new.empty()) {
+        cudaStream_t st = lg::abi_stream(s->ctx);
+        AMR_CUDA(s, cudaMemcpyAsync(s->arena[keep] + l0, s->host_new.data(), s->host_new.size() * sizeof(double),
+                                    cudaMemcpyHostToDevice, st));
+        AMR_CUDA(s, cudaStreamSynchronize(st));
     }
     s->layout = std::move(ng);
-    int rc = setup_device(s);
+    s->plans = std::move(np);
+    s->tile_shapes = shapes;
+    drop_graphs(s);
+    rc = upload_tables(s, s->plans, s->layout, s->tab);
     if (rc != LG_OK) return rc;
-    for (int k = 0; k < s->nfields; ++k) {
-        rc = upload_blocks(s, k, migrated[k]);
-        if (rc != LG_OK) return rc;
-    }
+    s->cur.assign(s->layout.num_levels(), keep);
     s->epoch += 1;
     return LG_OK;
 }
@@ -683,11 +1255,18 @@ int lg_amr_sim_create(lg_ctx* ctx, const int64_t* cells, const int64_t* block, c
     int rc = setup_device(s);
     if (rc == LG_OK && cudaMalloc(&s->d_t, 2 * sizeof(double)) != cudaSuccess) rc = LG_ERR_NOMEM;
     if (rc == LG_OK && cudaMemset(s->d_t, 0, 2 * sizeof(double)) != cudaSuccess) rc = LG_ERR_CUDA;
+    if (rc == LG_OK && cudaMalloc(&s->d_bar, 2 * sizeof(unsigned)) != cudaSuccess) rc = LG_ERR_NOMEM;
+    if (rc == LG_OK && cudaMemset(s->d_bar, 0, 2 * sizeof(unsigned)) != cudaSuccess) rc = LG_ERR_CUDA;
+    if (rc == LG_OK && cudaMalloc(&s->d_err, sizeof(int)) != cudaSuccess) rc = LG_ERR_NOMEM;
+    if (rc == LG_OK && cudaMemset(s->d_err, 0, sizeof(int)) != cudaSuccess) rc = LG_ERR_CUDA;
     if (rc != LG_OK) {
+        const std::string why = lg_last_error(ctx);
         free_device(s);
         cudaFree(s->d_t);
+        cudaFree(s->d_bar);
+        cudaFree(s->d_err);
         delete s;
-        return lg::abi_fail(ctx, rc, "AMR state allocation failed");
+        return lg::abi_fail(ctx, rc, "AMR state set-up failed: " + why);
     }
     *out = s;
     return LG_OK;
@@ -699,6 +1278,8 @@ int lg_amr_sim_destroy(lg_amr_sim* s) {
     cudaStreamSynchronize(lg::abi_stream(s->ctx));
     free_device(s);
     cudaFree(s->d_t);
+    cudaFree(s->d_bar);
+    cudaFree(s->d_err);
     cudaFree(s->d_tags);
     cudaFree(s->d_count);
     delete s;
@@ -738,12 +1319,12 @@ int lg_amr_sim_get_field(lg_amr_sim* s, int field, double* host, int64_t nelem) 
     lg_amr_sim_field_len(s, &n);
     if (nelem != n) return fail(s, LG_ERR_INVALID, "element count must equal lg_amr_sim_field_len");
     cudaSetDevice(lg::abi_device(s->ctx));
-    std::vector<std::vector<double>> blocks;
-    int rc = download_blocks(s, field, blocks);
+    int rc = download_state(s, s->host_old);
     if (rc != LG_OK) return rc;
-    for (const auto& b : blocks) {
-        std::memcpy(host, b.data(), b.size() * sizeof(double));
-        host += b.size();
+    for (const auto& b : s->plans.blocks) {
+        const size_t len = (size_t)(b.nx + 2) * (b.ny + 2);
+        std::memcpy(host, s->host_old.data() + b.off + field * b.stride, len * sizeof(double));
+        host += len;
     }
     return LG_OK;
 }
@@ -754,13 +1335,14 @@ int lg_amr_sim_set_field(lg_amr_sim* s, int field, const double* host, int64_t n
     lg_amr_sim_field_len(s, &n);
     if (nelem != n) return fail(s, LG_ERR_INVALID, "element count must equal lg_amr_sim_field_len");
     cudaSetDevice(lg::abi_device(s->ctx));
-    std::vector<std::vector<double>> blocks(s->layout.num_blocks());
-    for (int b = 0; b < s->layout.num_blocks(); ++b) {
-        const auto& d = s->plans.blocks[b];
-        blocks[b].assign(host, host + (size_t)(d.nx + 2) * (d.ny + 2));
-        host += blocks[b].size();
+    int rc = download_state(s, s->host_old);  // the other fields and the padding stay as they are
+    if (rc != LG_OK) return rc;
+    for (const auto& b : s->plans.blocks) {
+        const size_t len = (size_t)(b.nx + 2) * (b.ny + 2);
+        std::memcpy(s->host_old.data() + b.off + field * b.stride, host, len * sizeof(double));
+        host += len;
     }
-    return upload_blocks(s, field, blocks);
+    return upload_state(s, s->host_old);
 }
 
 int lg_amr_sim_time(const lg_amr_sim* s, double* t, int64_t* step_index) {
@@ -784,6 +1366,7 @@ int lg_amr_sim_step(lg_amr_sim* s, double dt, int64_t nsteps, uint32_t flags) {
     cudaSetDevice(lg::abi_device(s->ctx));
     cudaStream_t st = lg::abi_stream(s->ctx);
     AMR_CUDA(s, cudaMemcpyAsync(s->d_t + s->tslot, &s->t, sizeof(double), cudaMemcpyHostToDevice, st));
+    AMR_CUDA(s, cudaStreamSynchronize(st));  // the source is a host scalar that changes below
     int64_t done = 0;
     while (done < nsteps) {
         int rc = maybe_regrid(s);
@@ -795,7 +1378,19 @@ int lg_amr_sim_step(lg_amr_sim* s, double dt, int64_t nsteps, uint32_t flags) {
             run = std::min(run, next - s->step_index);
         }
         int64_t k = 0;
-        if ((flags & LG_RUN_GRAPH) && run >= 2) {
+        if (flags & LG_RUN_PERSISTENT) {
+            for (; k < run; k += 2) {
+                const int n = run - k >= 2 ? 2 : 1;
+                int rc2 = run_persistent(s, dt, n);
+                if (rc2 != LG_OK) return rc2;
+                for (int r2 = 0; r2 < n; ++r2) {
+                    s->t += dt;
+                    s->step_index += 1;
+                }
+            }
+            k = run;
+        }
+        if ((flags & LG_RUN_GRAPH) && run - k >= 2) {
             char key[160];
             snprintf(key, sizeof key, "%lld|%a|%d", (long long)s->epoch, dt, s->tslot);
             std::string gk = key;
@@ -844,6 +1439,17 @@ int lg_amr_sim_step(lg_amr_sim* s, double dt, int64_t nsteps, uint32_t flags) {
         }
         done += run;
     }
+    if (flags & LG_RUN_PERSISTENT) {  // did a grid barrier give up?
+        int err = 0;
+        AMR_CUDA(s, cudaMemcpyAsync(&err, s->d_err, sizeof err, cudaMemcpyDeviceToHost, st));
+        AMR_CUDA(s, cudaStreamSynchronize(st));
+        if (err) {
+            AMR_CUDA(s, cudaMemsetAsync(s->d_bar, 0, 2 * sizeof(unsigned), st));
+            AMR_CUDA(s, cudaMemsetAsync(s->d_err, 0, sizeof(int), st));
+            AMR_CUDA(s, cudaStreamSynchronize(st));
+            return fail(s, LG_ERR_TIMEOUT, "a grid barrier of the persistent AMR kernel timed out; the state is invalid");
+        }
+    }
     return LG_OK;
 }
 
@@ -861,7 +1467,7 @@ int lg_amr_fill_ghosts(lg_amr_sim* s) {
     if (!s) return LG_ERR_INVALID;
     cudaSetDevice(lg::abi_device(s->ctx));
     for (int level = 0; level < s->layout.num_levels(); ++level) {
-        int rc = launch_fill(s, level, false, 0.0);
+        int rc = launch_fill(s, level);
         if (rc != LG_OK) return rc;
     }
     return LG_OK;

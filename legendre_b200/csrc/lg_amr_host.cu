@@ -2,6 +2,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdlib>
+#include <unordered_map>
 
 #include "lg_amr_host.h"
 
@@ -31,23 +32,34 @@ int64_t reflect(int64_t c, int64_t lo, int64_t hi) {
     return c;
 }
 
-// every cell of `need` lies in some box of `cover` (amr/grid.rs:293-322)
-bool covered(const Box& need, const std::vector<Box>& cover) {
-    if (need.cells() == 0) return true;
-    for (int64_t y = need.lo[1]; y < need.hi[1]; ++y) {
-        int64_t x = need.lo[0];
-        while (x < need.hi[0]) {
-            const Box* hit = nullptr;
-            for (const Box& b : cover)
-                if (b.contains(x, y)) {
-                    hit = &b;
-                    break;
+// bucket index of the patches [p0, p1) of one level (see Layout::Index)
+Layout::Index build_index(const std::vector<Patch>& patches, uint32_t p0, uint32_t p1, const Box& dom) {
+    Layout::Index ix;
+    ix.side = 32;
+    while ((dom.hi[0] / ix.side + 1) * (dom.hi[1] / ix.side + 1) > (int64_t(1) << 22)) ix.side *= 2;
+    ix.nbx = (dom.hi[0] + ix.side - 1) / ix.side;
+    ix.nby = (dom.hi[1] + ix.side - 1) / ix.side;
+    ix.start.assign((size_t)(ix.nbx * ix.nby + 1), 0);
+    for (int pass = 0; pass < 2; ++pass) {
+        std::vector<uint32_t> fillpos;
+        if (pass == 1) {
+            for (size_t k = 1; k < ix.start.size(); ++k) ix.start[k] += ix.start[k - 1];
+            ix.items.assign(ix.start.back(), 0);
+            fillpos.assign(ix.start.begin(), ix.start.end() - 1);
+        }
+        for (uint32_t p = p0; p < p1; ++p) {
+            const Box& b = patches[p].bx;
+            for (int64_t by = b.lo[1] / ix.side; by <= (b.hi[1] - 1) / ix.side; ++by)
+                for (int64_t bx = b.lo[0] / ix.side; bx <= (b.hi[0] - 1) / ix.side; ++bx) {
+                    const size_t k = (size_t)(bx + by * ix.nbx);
+                    if (pass == 0)
+                        ix.start[k + 1] += 1;
+                    else
+                        ix.items[fillpos[k]++] = p;
                 }
-            if (!hit) return false;
-            x = hit->hi[0];
         }
     }
-    return true;
+    return ix;
 }
 
 }  // namespace
@@ -62,11 +74,27 @@ Box Layout::domain(int level) const {
 }
 
 int Layout::find(int level, int64_t x, int64_t y) const {
-    if (level < 0 || level >= (int)owner.size()) return -1;
+    if (level < 0 || level >= (int)index.size()) return -1;
     const Box d = domain(level);
     if (!d.contains(x, y)) return -1;
-    const uint32_t p = owner[level][(size_t)x + (size_t)y * (size_t)d.hi[0]];
-    return p == UINT32_MAX ? -1 : (int)p;
+    const Index& ix = index[level];
+    const size_t k = (size_t)(x / ix.side + (y / ix.side) * ix.nbx);
+    for (uint32_t q = ix.start[k]; q < ix.start[k + 1]; ++q)
+        if (patches[ix.items[q]].bx.contains(x, y)) return (int)ix.items[q];
+    return -1;
+}
+
+bool Layout::covers(int level, const Box& need) const {
+    if (need.cells() == 0) return true;
+    for (int64_t y = need.lo[1]; y < need.hi[1]; ++y) {
+        int64_t x = need.lo[0];
+        while (x < need.hi[0]) {
+            const int p = find(level, x, y);
+            if (p < 0) return false;
+            x = patches[p].bx.hi[0];
+        }
+    }
+    return true;
 }
 
 std::string build_layout(const Base& base, const std::vector<uint32_t>& ratios,
@@ -91,8 +119,7 @@ std::string build_layout(const Base& base, const std::vector<uint32_t>& ratios,
         g.patches.push_back(p);
     }
     g.level_start = {0, (uint32_t)g.patches.size()};
-    std::vector<Box> coarser;
-    for (const Patch& p : g.patches) coarser.push_back(p.bx);
+    g.index.push_back(build_index(g.patches, 0, g.level_start[1], g.domain(0)));
     for (size_t l = 0; l < levels.size(); ++l) {
         const int level = (int)l + 1;
         const int64_t r = ratios[l];
@@ -113,27 +140,17 @@ std::string build_layout(const Base& base, const std::vector<uint32_t>& ratios,
                 need.hi[d] = floor_div(b.hi[d] + r - 1, r) + 1;
             }
             need = need.clipped(g.domain(level - 1));
-            if (!covered(need, coarser)) return "patch not properly nested at level " + std::to_string(level);
+            if (!g.covers(level - 1, need)) return "patch not properly nested at level " + std::to_string(level);
         }
+        const uint32_t p0 = (uint32_t)g.patches.size();
         for (const Box& b : boxes) g.patches.push_back(Patch{level, b});
         g.level_start.push_back((uint32_t)g.patches.size());
-        coarser = boxes;
+        g.index.push_back(build_index(g.patches, p0, g.level_start.back(), dom));
     }
     g.level_spacing.push_back({base.spacing[0], base.spacing[1]});
     for (uint32_t r : g.ratios) {
         const auto prev = g.level_spacing.back();
         g.level_spacing.push_back({prev[0] / (double)r, prev[1] / (double)r});
-    }
-    for (int level = 0; level < g.num_levels(); ++level) {
-        const Box d = g.domain(level);
-        std::vector<uint32_t> map((size_t)d.hi[0] * (size_t)d.hi[1], UINT32_MAX);
-        for (uint32_t p = g.level_start[level]; p < g.level_start[level + 1]; ++p) {
-            const Box& b = g.patches[p].bx;
-            for (int64_t y = b.lo[1]; y < b.hi[1]; ++y)
-                std::fill(map.begin() + (size_t)(b.lo[0] + y * d.hi[0]), map.begin() + (size_t)(b.hi[0] + y * d.hi[0]),
-                          p);
-        }
-        g.owner.push_back(std::move(map));
     }
     *out = std::move(g);
     return "";
@@ -243,36 +260,85 @@ std::vector<Box> cluster(std::vector<std::array<int64_t, 2>>& flags, double effi
     return out;
 }
 
+// The cells of the union of `boxes` inside `dom`, sorted (x, then y) and
+// without duplicates (adapt.rs:208-210): a bitmap over the boxes' bounding
+// box, scanned x-major, or packed 64-bit keys sorted when that box is huge.
+static std::vector<std::array<int64_t, 2>> union_cells(const std::vector<Box>& boxes, const Box& dom) {
+    std::vector<std::array<int64_t, 2>> out;
+    Box bb;
+    bool any = false;
+    for (const Box& b0 : boxes) {
+        const Box b = b0.clipped(dom);
+        if (b.cells() == 0) continue;
+        if (!any) {
+            bb = b;
+            any = true;
+            continue;
+        }
+        for (int d = 0; d < 2; ++d) {
+            bb.lo[d] = std::min(bb.lo[d], b.lo[d]);
+            bb.hi[d] = std::max(bb.hi[d], b.hi[d]);
+        }
+    }
+    if (!any) return out;
+    const int64_t w = bb.extent(0), h = bb.extent(1);
+    if ((uint64_t)w * (uint64_t)h <= (uint64_t(1) << 27)) {
+        std::vector<uint8_t> bits((size_t)(w * h), 0);  // x-major
+        for (const Box& b0 : boxes) {
+            const Box b = b0.clipped(dom);
+            if (b.cells() == 0) continue;
+            for (int64_t x = b.lo[0]; x < b.hi[0]; ++x)
+                std::fill_n(bits.begin() + (size_t)((x - bb.lo[0]) * h + (b.lo[1] - bb.lo[1])), (size_t)b.extent(1),
+                            uint8_t(1));
+        }
+        for (int64_t x = 0; x < w; ++x)
+            for (int64_t y = 0; y < h; ++y)
+                if (bits[(size_t)(x * h + y)]) out.push_back({bb.lo[0] + x, bb.lo[1] + y});
+        return out;
+    }
+    std::vector<uint64_t> keys;  // cells of a level domain: non-negative, below 2^31
+    for (const Box& b0 : boxes) {
+        const Box b = b0.clipped(dom);
+        for (int64_t x = b.lo[0]; x < b.hi[0]; ++x)
+            for (int64_t y = b.lo[1]; y < b.hi[1]; ++y) keys.push_back(((uint64_t)x << 32) | (uint64_t)y);
+    }
+    std::sort(keys.begin(), keys.end());
+    keys.erase(std::unique(keys.begin(), keys.end()), keys.end());
+    out.resize(keys.size());
+    for (size_t k = 0; k < keys.size(); ++k) out[k] = {(int64_t)(keys[k] >> 32), (int64_t)(keys[k] & 0xffffffffu)};
+    return out;
+}
+
 std::vector<std::vector<Box>> propose(const Layout& g, std::vector<std::vector<std::array<int64_t, 2>>>& flags,
                                       const Policy& p) {
     const int capacity = g.max_levels() - 1;
     std::vector<std::vector<Box>> nl(capacity);
     for (int target = capacity; target >= 1; --target) {
         const int src = target - 1;
-        std::vector<Cell> f;
+        std::vector<Box> parts;  // dilated tags and nesting boxes
         if (src < (int)flags.size()) {
-            if (p.buffer > 0) {
-                for (const Cell& c : flags[src])
-                    for (int64_t y = c[1] - p.buffer; y <= c[1] + p.buffer; ++y)
-                        for (int64_t x = c[0] - p.buffer; x <= c[0] + p.buffer; ++x) f.push_back({x, y});
-            } else {
-                f = flags[src];
+            const int64_t bf = std::max<int64_t>(p.buffer, 0);
+            for (const Cell& c : flags[src]) {
+                Box b;
+                b.lo[0] = c[0] - bf;
+                b.lo[1] = c[1] - bf;
+                b.hi[0] = c[0] + bf + 1;
+                b.hi[1] = c[1] + bf + 1;
+                parts.push_back(b);
             }
         }
         if (target < capacity && !nl[target].empty()) {  // nesting flags (adapt.rs:188-205)
             const int64_t rf = g.ratios[target], rs = g.ratios[target - 1];
             for (const Box& b : nl[target]) {
-                const int64_t lo0 = floor_div(b.lo[0] / rf - 1, rs), lo1 = floor_div(b.lo[1] / rf - 1, rs);
-                const int64_t hi0 = floor_div(b.hi[0] / rf + 1 + rs - 1, rs), hi1 = floor_div(b.hi[1] / rf + 1 + rs - 1, rs);
-                for (int64_t y = lo1; y < hi1; ++y)
-                    for (int64_t x = lo0; x < hi0; ++x) f.push_back({x, y});
+                Box n;
+                n.lo[0] = floor_div(b.lo[0] / rf - 1, rs);
+                n.lo[1] = floor_div(b.lo[1] / rf - 1, rs);
+                n.hi[0] = floor_div(b.hi[0] / rf + 1 + rs - 1, rs);
+                n.hi[1] = floor_div(b.hi[1] / rf + 1 + rs - 1, rs);
+                parts.push_back(n);
             }
         }
-        const Box dom = g.domain(src);
-        f.erase(std::remove_if(f.begin(), f.end(), [&](const Cell& c) { return !dom.contains(c[0], c[1]); }),
-                f.end());
-        std::sort(f.begin(), f.end());
-        f.erase(std::unique(f.begin(), f.end()), f.end());
+        std::vector<Cell> f = union_cells(parts, g.domain(src));
         if (f.empty()) continue;
         const int64_t r = g.ratios[target - 1];
         for (Box b : cluster(f, p.efficiency, p.min_width)) {
@@ -290,20 +356,18 @@ std::vector<std::vector<Box>> propose(const Layout& g, std::vector<std::vector<s
 bool acceptable(const Layout& g, const std::vector<std::vector<Box>>& proposed) {
     if ((int)proposed.size() != g.num_levels() - 1) return false;
     for (size_t l = 0; l < proposed.size(); ++l) {
-        std::vector<Box> cur;
-        for (uint32_t b = g.level_start[l + 1]; b < g.level_start[l + 2]; ++b) cur.push_back(g.patches[b].bx);
         uint64_t pc = 0, cc = 0;
         for (const Box& b : proposed[l]) pc += b.cells();
-        for (const Box& b : cur) cc += b.cells();
+        for (uint32_t b = g.level_start[l + 1]; b < g.level_start[l + 2]; ++b) cc += g.patches[b].bx.cells();
         if (cc > pc + pc / 2) return false;
         for (const Box& b : proposed[l])
-            if (!covered(b, cur)) return false;
+            if (!g.covers((int)l + 1, b)) return false;
     }
     return true;
 }
 
 // ------------------------------------------------------------- plans -----
-Plans build_plans(const Layout& g, int nfields, int unit_cells) {
+Plans build_plans(const Layout& g, int nfields, int unit_cells, int first_level, const std::vector<int>& tile_rows) {
     Plans P;
     int64_t off = 0;
     for (const Patch& p : g.patches) {
@@ -320,22 +384,27 @@ Plans build_plans(const Layout& g, int nfields, int unit_cells) {
     P.arena_elems = off;
     auto slab_off = [&](int b, int64_t i, int64_t j) { return (int)((i + 1) + (j + 1) * (P.blocks[b].nx + 2)); };
 
-    // ghost fill (intergrid.rs:267-351, ghost width 1)
+    // ghost fill (intergrid.rs:267-351, ghost width 1), and the tiles of
+    // every block with the ring entries their windows need
     for (int level = 0; level < g.num_levels(); ++level) {
         P.fill_start.push_back((int64_t)P.fill.size());
+        P.tile_start.push_back((int64_t)P.tiles.size());
+        if (level < first_level) continue;
         const Box dom = g.domain(level);
         for (uint32_t pb = g.level_start[level]; pb < g.level_start[level + 1]; ++pb) {
             const Box& bx = g.patches[pb].bx;
+            const size_t ring0 = P.fill.size();
             auto visit = [&](int64_t x, int64_t y) {
-                FillOp op{};
-                op.tblock = (int)pb;
-                op.toff = slab_off((int)pb, x - bx.lo[0], y - bx.lo[1]);
+                GhostOp op{};
+                op.dst = P.blocks[pb].off + slab_off((int)pb, x - bx.lo[0], y - bx.lo[1]);
+                op.dst_stride = (int32_t)P.blocks[pb].stride;
                 const int64_t tx = reflect(x, dom.lo[0], dom.hi[0]), ty = reflect(y, dom.lo[1], dom.hi[1]);
                 const int src = g.find(level, tx, ty);
                 if (src >= 0) {
                     const Box& sb = g.patches[src].bx;
-                    op.a = src;
-                    op.b = slab_off(src, tx - sb.lo[0], ty - sb.lo[1]);
+                    op.n = 0;
+                    op.src[0] = P.blocks[src].off + slab_off(src, tx - sb.lo[0], ty - sb.lo[1]);
+                    op.stride[0] = (int32_t)P.blocks[src].stride;
                 } else {
                     const double r = (double)g.ratios[level - 1];
                     const Box cd = g.domain(level - 1);
@@ -348,7 +417,7 @@ Plans build_plans(const Layout& g, int nfields, int unit_cells) {
                         c0[d] = (int64_t)fl;
                         w[d] = pc - fl;
                     }
-                    const int start = (int)P.corners.size();
+                    op.n = 0;
                     for (unsigned corner = 0; corner < 4; ++corner) {
                         int64_t cc[2] = {c0[0], c0[1]};
                         double weight = 1.0;
@@ -368,10 +437,11 @@ Plans build_plans(const Layout& g, int nfields, int unit_cells) {
                             continue;
                         }
                         const Box& qb = g.patches[q].bx;
-                        P.corners.push_back(Corner{q, slab_off(q, cc[0] - qb.lo[0], cc[1] - qb.lo[1]), weight});
+                        op.src[op.n] = P.blocks[q].off + slab_off(q, cc[0] - qb.lo[0], cc[1] - qb.lo[1]);
+                        op.stride[op.n] = (int32_t)P.blocks[q].stride;
+                        op.w[op.n] = weight;
+                        op.n += 1;
                     }
-                    op.a = start;
-                    op.b = -((int)P.corners.size() - start);
                 }
                 P.fill.push_back(op);
             };
@@ -380,9 +450,37 @@ Plans build_plans(const Layout& g, int nfields, int unit_cells) {
             for (int64_t y = bx.lo[1]; y < bx.hi[1]; ++y) visit(bx.hi[0], y);
             for (int64_t x = bx.lo[0] - 1; x < bx.hi[0] + 1; ++x) visit(x, bx.lo[1] - 1);
             for (int64_t x = bx.lo[0] - 1; x < bx.hi[0] + 1; ++x) visit(x, bx.hi[1]);
+            const int nx = (int)bx.extent(0), ny = (int)bx.extent(1);
+            const int th = level < (int)tile_rows.size() ? std::max(1, std::min(kTile, tile_rows[level])) : kTile;
+            for (int y0 = 0; y0 < ny; y0 += th)
+                for (int x0 = 0; x0 < nx; x0 += kTile) {
+                    Tile t{};
+                    t.block = (int)pb;
+                    t.off = P.blocks[pb].off;
+                    t.stride = (int32_t)P.blocks[pb].stride;
+                    t.nx = nx;
+                    t.ny = ny;
+                    t.x0 = x0;
+                    t.y0 = y0;
+                    t.w = std::min(kTile, nx - x0);
+                    t.h = std::min(th, ny - y0);
+                    t.fill0 = (int)P.tile_fill.size();
+                    for (size_t k = ring0; k < P.fill.size(); ++k) {
+                        const int toff = (int)(P.fill[k].dst - P.blocks[pb].off);
+                        const int i = toff % (nx + 2) - 1, j = toff / (nx + 2) - 1;
+                        const int c = i - (x0 - 1), r = j - (y0 - 1);
+                        if (c < 0 || c > t.w + 1 || r < 0 || r > t.h + 1) continue;
+                        GhostOp op = P.fill[k];
+                        op.dst = c + r * (t.w + 2);
+                        P.tile_fill.push_back(op);
+                    }
+                    t.fill1 = (int)P.tile_fill.size();
+                    P.tiles.push_back(t);
+                }
         }
     }
     P.fill_start.push_back((int64_t)P.fill.size());
+    P.tile_start.push_back((int64_t)P.tiles.size());
 
     // restriction (intergrid.rs:110-150)
     P.restrict_start.push_back(0);
@@ -402,9 +500,11 @@ Plans build_plans(const Layout& g, int nfields, int unit_cells) {
                 if (ov.cells() == 0) continue;
                 for (int64_t y = ov.lo[1]; y < ov.hi[1]; ++y)
                     for (int64_t x = ov.lo[0]; x < ov.hi[0]; ++x)
-                        P.restrict_ops.push_back(RestrictOp{(int)cb, slab_off((int)cb, x - cp.lo[0], y - cp.lo[1]),
-                                                            (int)fb,
-                                                            slab_off((int)fb, x * r - fp.lo[0], y * r - fp.lo[1])});
+                        P.restrict_ops.push_back(
+                            RestrictOp{P.blocks[cb].off + slab_off((int)cb, x - cp.lo[0], y - cp.lo[1]),
+                                       P.blocks[fb].off + slab_off((int)fb, x * r - fp.lo[0], y * r - fp.lo[1]),
+                                       (int32_t)P.blocks[cb].stride, (int32_t)P.blocks[fb].stride,
+                                       P.blocks[fb].nx + 2, 0});
             }
         }
     }
@@ -413,6 +513,7 @@ Plans build_plans(const Layout& g, int nfields, int unit_cells) {
     // step work units
     for (int level = 0; level < g.num_levels(); ++level) {
         P.unit_start.push_back((int64_t)P.units.size());
+        if (level < first_level) continue;
         for (uint32_t b = g.level_start[level]; b < g.level_start[level + 1]; ++b) {
             const int cells = P.blocks[b].nx * P.blocks[b].ny;
             for (int s = 0; s < cells; s += unit_cells) P.units.push_back(Unit{(int)b, s, std::min(unit_cells, cells - s), 0});
@@ -425,62 +526,92 @@ Plans build_plans(const Layout& g, int nfields, int unit_cells) {
 // ----------------------------------------------------------- migrate -----
 namespace {
 
-double sample(const Layout& g, const std::vector<std::vector<double>>& s, int level, int64_t x, int64_t y) {
-    if (level < g.num_levels()) {
-        const int b = g.find(level, x, y);
-        if (b >= 0) {
-            const Box& bx = g.patches[b].bx;
-            return s[b][(size_t)((x - bx.lo[0] + 1) + (y - bx.lo[1] + 1) * (bx.extent(0) + 2))];
-        }
-    }
-    const double r = (double)g.ratios[level - 1];
-    const Box cd = g.domain(level - 1);
-    const int64_t cell[2] = {x, y};
-    int64_t c0[2];
-    double w[2];
-    for (int d = 0; d < 2; ++d) {
-        const double pc = ((double)cell[d] + 0.5) / r - 0.5;
-        const double fl = std::floor(pc);
-        c0[d] = (int64_t)fl;
-        w[d] = pc - fl;
-    }
-    double acc = 0.0;
-    for (unsigned corner = 0; corner < 4; ++corner) {
-        int64_t cc[2] = {c0[0], c0[1]};
-        double weight = 1.0;
-        for (int d = 0; d < 2; ++d) {
-            if ((corner >> d) & 1) {
-                cc[d] += 1;
-                weight *= w[d];
-            } else {
-                weight *= 1.0 - w[d];
+// sample (adapt.rs:323-402) with the bilinear values of the coarser cells it
+// recurses into memoised: sample is a pure function of (level, cell), and
+// neighbouring fine cells share coarse corners.
+struct Sampler {
+    const Layout& g;
+    const std::vector<const double*>& s;
+    std::vector<std::unordered_map<uint64_t, double>> memo;
+    std::vector<int> last;  // per level, the patch of the previous hit (patches of a level are disjoint)
+    bool missing = false;
+
+    Sampler(const Layout& g_, const std::vector<const double*>& s_)
+        : g(g_), s(s_), memo(g_.max_levels()), last(g_.max_levels(), -1) {}
+
+    double at(int level, int64_t x, int64_t y, bool keep) {
+        if (level < g.num_levels()) {
+            int b = last[level];
+            if (b < 0 || !g.patches[b].bx.contains(x, y)) {
+                b = g.find(level, x, y);
+                if (b >= 0) last[level] = b;
+            }
+            if (b >= 0) {
+                if (!s[b]) {
+                    missing = true;
+                    return 0.0;
+                }
+                const Box& bx = g.patches[b].bx;
+                return s[b][(size_t)((x - bx.lo[0] + 1) + (y - bx.lo[1] + 1) * (bx.extent(0) + 2))];
             }
         }
-        if (weight == 0.0) continue;
-        for (int d = 0; d < 2; ++d) cc[d] = reflect(cc[d], cd.lo[d], cd.hi[d]);
-        acc += sample(g, s, level - 1, cc[0], cc[1]) * weight;
+        const uint64_t key = ((uint64_t)x << 32) | (uint64_t)y;  // cells of a level domain: below 2^31
+        if (keep) {
+            auto it = memo[level].find(key);
+            if (it != memo[level].end()) return it->second;
+        }
+        const double r = (double)g.ratios[level - 1];
+        const Box cd = g.domain(level - 1);
+        const int64_t cell[2] = {x, y};
+        int64_t c0[2];
+        double w[2];
+        for (int d = 0; d < 2; ++d) {
+            const double pc = ((double)cell[d] + 0.5) / r - 0.5;
+            const double fl = std::floor(pc);
+            c0[d] = (int64_t)fl;
+            w[d] = pc - fl;
+        }
+        double acc = 0.0;
+        for (unsigned corner = 0; corner < 4; ++corner) {
+            int64_t cc[2] = {c0[0], c0[1]};
+            double weight = 1.0;
+            for (int d = 0; d < 2; ++d) {
+                if ((corner >> d) & 1) {
+                    cc[d] += 1;
+                    weight *= w[d];
+                } else {
+                    weight *= 1.0 - w[d];
+                }
+            }
+            if (weight == 0.0) continue;
+            for (int d = 0; d < 2; ++d) cc[d] = reflect(cc[d], cd.lo[d], cd.hi[d]);
+            acc += at(level - 1, cc[0], cc[1], true) * weight;
+        }
+        if (keep) memo[level].emplace(key, acc);
+        return acc;
     }
-    return acc;
-}
+};
 
 }  // namespace
 
-void migrate_field(const Layout& og, const std::vector<std::vector<double>>& old, const Layout& ng,
-                   std::vector<std::vector<double>>& out) {
-    out.assign(ng.num_blocks(), {});
-    for (int b = 0; b < ng.num_blocks(); ++b) {
-        const Box& bx = ng.patches[b].bx;
-        out[b].assign((size_t)(bx.extent(0) + 2) * (size_t)(bx.extent(1) + 2), 0.0);
-    }
-    for (uint32_t b = ng.level_start[0]; b < ng.level_start[1]; ++b) out[b] = old[b];  // the base tiling never changes
+bool migrate_field(const Layout& og, const std::vector<const double*>& old, const Layout& ng,
+                   const std::vector<double*>& out, bool copy_level0) {
+    if (copy_level0)  // the base tiling never changes
+        for (uint32_t b = ng.level_start[0]; b < ng.level_start[1]; ++b) {
+            const Box& bx = ng.patches[b].bx;
+            if (!old[b]) return false;
+            std::copy(old[b], old[b] + (size_t)(bx.extent(0) + 2) * (size_t)(bx.extent(1) + 2), out[b]);
+        }
+    Sampler smp(og, old);
     for (int level = 1; level < ng.num_levels(); ++level)
         for (uint32_t b = ng.level_start[level]; b < ng.level_start[level + 1]; ++b) {
             const Box& bx = ng.patches[b].bx;
             for (int64_t j = 0; j < bx.extent(1); ++j)
                 for (int64_t i = 0; i < bx.extent(0); ++i)
                     out[b][(size_t)((i + 1) + (j + 1) * (bx.extent(0) + 2))] =
-                        sample(og, old, level, bx.lo[0] + i, bx.lo[1] + j);
+                        smp.at(level, bx.lo[0] + i, bx.lo[1] + j, false);
         }
+    return !smp.missing;
 }
 
 }  // namespace amr

@@ -49,13 +49,23 @@ struct Layout {
     std::vector<Patch> patches;
     std::vector<uint32_t> level_start;
     std::vector<std::array<double, 2>> level_spacing;
-    std::vector<std::vector<uint32_t>> owner;  // per level, cell -> patch or UINT32_MAX
+    // Per level, a bucket grid over the level's domain: bucket (bx, by) of
+    // side `side` lists the patches of the level that intersect it (CSR).
+    // Memory is proportional to the domain / side^2 plus the patch count,
+    // not to the number of cells of a fine level's domain.
+    struct Index {
+        int64_t side = 32, nbx = 0, nby = 0;
+        std::vector<uint32_t> start, items;
+    };
+    std::vector<Index> index;
 
     int num_levels() const { return (int)level_start.size() - 1; }
     int max_levels() const { return (int)ratios.size() + 1; }
     int num_blocks() const { return (int)patches.size(); }
     Box domain(int level) const;
     int find(int level, int64_t x, int64_t y) const;  // -1 if uncovered or outside
+    // every cell of `need` lies in a patch of `level` (amr/grid.rs:293-322)
+    bool covers(int level, const Box& need) const;
 };
 
 // AmrGrid::from_patches (amr/grid.rs:90-196); returns "" or the error text.
@@ -86,44 +96,73 @@ struct BlockDesc {
     int64_t off, stride;
 };
 
-// One ghost entry to fill: target (block, slab offset); copy from
-// (a, b) when b >= 0, else bilinear from corners [a, a - b).
-struct FillOp {
-    int tblock, toff, a, b;
+// One ghost entry to fill, every address resolved to an arena offset:
+// field f of the target is dst + f * dst_stride; with n == 0 the value is a
+// copy of src[0] + f * stride[0], else the bilinear fold acc + v w over the
+// n <= 4 coarse corners src[k] + f * stride[k] with weights w[k], in corner
+// order (intergrid.rs:183-223).  For the ops of a tile, dst is the window
+// index instead.
+struct GhostOp {
+    int64_t dst;
+    int32_t dst_stride, n;
+    int64_t src[4];
+    int32_t stride[4];
+    double w[4];
 };
-struct Corner {
-    int block, off;
-    double w;
-};
-// One covered coarse cell: (coarse block, offset) <- mean of r x r fine
-// children starting at (fine block, offset).
+// One covered coarse cell, arena offsets of field 0: coarse c <- mean of the
+// r x r fine children starting at f (row pitch fsy).
 struct RestrictOp {
-    int cblock, coff, fblock, foff;
+    int64_t c, f;
+    int32_t cstride, fstride, fsy, pad;
 };
 // A run of cells [start, start + count) of one block (row-major interior).
 struct Unit {
     int block, start, count, pad;
+};
+// A rectangle of at most kTile x rows interior cells of one block (rows <=
+// kTile, chosen per level), the work item of the fused fill + step
+// kernels: [x0, x0 + w) x [y0, y0 + h) in block-interior coordinates of the
+// block whose slab of field f starts at off + f * stride.  Its
+// (w + 2) x (h + 2) window is staged in shared memory; the window entries
+// that are ghosts of the block come from tile_fill[fill0, fill1), whose dst
+// is the window index c + r (w + 2).
+constexpr int kTile = 32;
+struct Tile {
+    int64_t off;
+    int32_t stride, nx, ny, x0, y0, w, h, fill0, fill1, block;
 };
 
 struct Plans {
     std::string error;  // non-empty when the hierarchy is not properly nested
     std::vector<BlockDesc> blocks;
     int64_t arena_elems = 0;
-    std::vector<FillOp> fill;          // all levels, level-major
+    std::vector<GhostOp> fill;         // all levels, level-major
     std::vector<int64_t> fill_start;   // per level, + end
-    std::vector<Corner> corners;
     std::vector<RestrictOp> restrict_ops;  // per fine level, level-major
     std::vector<int64_t> restrict_start;   // per fine level (index 0 unused), + end
     std::vector<Unit> units;
     std::vector<int64_t> unit_start;       // per level, + end
+    std::vector<Tile> tiles;               // level-major
+    std::vector<int64_t> tile_start;       // per level, + end
+    std::vector<GhostOp> tile_fill;
 };
 
-Plans build_plans(const Layout& g, int nfields, int unit_cells);
+// Ring, tile and unit lists are built for the levels >= first_level only
+// (the others' ranges are empty).  Level-0 ghosts come from level 0 alone,
+// so a caller may build level 0's lists once (first_level 0 on the base
+// layout) and only the refined levels' at each regrid (first_level 1).
+// `tile_rows[l]` (default kTile) is the tile height of level l.
+Plans build_plans(const Layout& g, int nfields, int unit_cells, int first_level = 0,
+                  const std::vector<int>& tile_rows = {});
 
-// migrate / sample (adapt.rs:323-402) on host slabs: old[b] / out[b] are the
-// ghost-inclusive slabs of one field, block order.
-void migrate_field(const Layout& og, const std::vector<std::vector<double>>& old, const Layout& ng,
-                   std::vector<std::vector<double>>& out);
+// migrate / sample (adapt.rs:323-402) on host slabs: old[b] / out[b] point
+// at the ghost-inclusive slabs of one field, block order.  Refined blocks'
+// interiors are sampled; level-0 slabs are copied verbatim when
+// `copy_level0` (the base tiling never changes, so a caller may move them
+// itself).  A null old[b] marks a slab the caller did not provide; the
+// function returns false if the sampling needed one.
+bool migrate_field(const Layout& og, const std::vector<const double*>& old, const Layout& ng,
+                   const std::vector<double*>& out, bool copy_level0);
 
 }  // namespace amr
 }  // namespace lg

@@ -65,6 +65,47 @@ __device__ __forceinline__ float fma_t(float a, float b, float c) { return fmaf(
 __device__ __forceinline__ double normal_t(uint64_t key, double) { return standard_normal(key); }
 __device__ __forceinline__ float normal_t(uint64_t key, float) { return standard_normal_f32(key); }
 
+// The exact FP64 arithmetic policy of the step kernels: face fluxes from
+// the normal difference dn and the transverse quarter sum 0.25 ((d1 + c) - e)
+// (finite_volume.rs:258-283), the cell update (phasefield.rs:395-421) and
+// the Euler-Maruyama axpy (driver.rs:210-236), in the reference's operand
+// order.
+template <class T>
+struct OpsExact {
+    using Params = MC<T>;
+
+    // x face: KarmaRappelFlux::face(derx, dery) and j = a (a derx - da dery)
+    static __device__ __forceinline__ T xface(const MC<T>& m, T dn, T d1, T c, T e) {
+        const T dt = T(0.25) * (d1 + c - e);
+        T a, da;
+        kr_face(m, dn, dt, a, da);
+        return a * (a * dn - da * dt);
+    }
+    // y face: face(derx, dery) with derx transverse, j = a (a dery + da derx)
+    static __device__ __forceinline__ T yface(const MC<T>& m, T dn, T d1, T c, T e) {
+        const T dt = T(0.25) * (d1 + c - e);
+        T a, da;
+        kr_face(m, dt, dn, a, da);
+        return a * (a * dn + da * dt);
+    }
+    static __device__ __forceinline__ void cell(const MC<T>& m, T jr, T jl, T jt, T jb, T p, T cdx, T cdy, T uc,
+                                                T ul, T ur, T up, T um, T& kphi, T& ku) {
+        const T flux = (jr - jl + jt - jb) * m.inv_h2_flux;
+        const T g_prime = fma_t(p * p, p, -p);
+        const T one_m_p2 = fma_t(p, -p, T(1));
+        const T p_prime = one_m_p2 * one_m_p2;
+        const T a = center_anisotropy(m, T(0.5) * cdx, T(0.5) * cdy);
+        kphi = fma_t(m.lambda * uc, -p_prime, flux - g_prime) / (a * a);
+        T acc = T(0);
+        acc += ((ur - (uc + uc)) + ul) * m.ih0;
+        acc += ((up - (uc + uc)) + um) * m.ih1;
+        ku = fma_t(acc, m.d_thermal, T(0.5) * kphi);
+    }
+    static __device__ __forceinline__ T axpy(T dt, T k, T x) { return x + dt * k; }
+    static __device__ __forceinline__ T noise(uint64_t key) { return normal_t(key, T(0)); }
+    static __device__ __forceinline__ T add_noise(T x, T scale_amp, T n) { return x + scale_amp * n; }
+};
+
 __device__ __forceinline__ int64_t slab_base(const SlabLayout& L, int b, int field) {
     return ((int64_t)b * L.nfields + field) * L.slab_stride;
 }

@@ -86,14 +86,18 @@ TILED = [(1, (0, 0), (8, 16)), (1, (8, 0), (16, 16))]
 INIT = staticmethod(lambda x, y: np.vectorize(math.cos)(0.6 * x) + np.vectorize(math.sin)(1.1 * y))
 
 
+MODES = {"launches": {}, "graph": {"graph": True}, "persistent": {"persistent": True}}
+
+
+@pytest.mark.parametrize("mode", sorted(MODES))
 @pytest.mark.parametrize("integrator", ["subcycling", "global"])
-def test_tiled_heat_bit_identical(sched, orc, integrator):
+def test_tiled_heat_bit_identical(sched, orc, integrator, mode):
     # tests/amr.rs:346-448 and 1016-1113 on the device
     dev, ref = make_pair(sched, orc, [8, 8], [8, 8], 0.5, [2], TILED, integrator=integrator)
     set_both(dev, ref, 0, lambda x, y: np.vectorize(math.cos)(0.6 * x) + np.vectorize(math.sin)(1.1 * y))
     dt = ref.suggested_dt()
     assert dev.stable_dt() == dt
-    dev.run(dt, 25)
+    dev.run(dt, 25, **MODES[mode])
     ref.step(dt, 25)
     same_state(dev, ref, 1)
     assert dev.time() == ref.step(dt, 0)
@@ -102,13 +106,13 @@ def test_tiled_heat_bit_identical(sched, orc, integrator):
 HEAT_POLICY = dict(every=2, buffer=2, efficiency=0.7, min_width=4, threshold=0.03)
 
 
-@pytest.mark.parametrize("graph", [False, True])
-def test_adaptive_subcycled_heat_bit_identical(sched, orc, graph):
+@pytest.mark.parametrize("mode", sorted(MODES))
+def test_adaptive_subcycled_heat_bit_identical(sched, orc, mode):
     # tests/amr.rs:1115-1180 setup: regrids every 2 steps
     dev, ref = make_pair(sched, orc, [32, 32], [16, 16], 0.5, [2], [], policy=HEAT_POLICY)
     set_both(dev, ref, 0, lambda x, y: np.exp(-((x - 8.0) * (x - 8.0) + (y - 8.0) * (y - 8.0)) / 3.0))
     dt = ref.suggested_dt()
-    dev.run(dt, 30, graph=graph)
+    dev.run(dt, 30, **MODES[mode])
     ref.step(dt, 30)
     assert dev.num_levels == 2 and dev.epoch == ref.epoch
     same_state(dev, ref, 1)
@@ -122,28 +126,30 @@ def _seed(x, y):
     return np.maximum(-1.0, -np.vectorize(math.tanh)((r - 4.0) / math.sqrt(2.0)))
 
 
-@pytest.mark.parametrize("integrator,steps", [("subcycling", 40), ("global", 60)])
-def test_adaptive_model_c_bit_identical(sched, orc, integrator, steps):
+@pytest.mark.parametrize("mode", ["graph", "persistent"])
+@pytest.mark.parametrize("integrator,steps", [("subcycling", 40), ("global", 60), ("subcycling", 41)])
+def test_adaptive_model_c_bit_identical(sched, orc, integrator, steps, mode):
     # tests/amr.rs:918-989 and 1182-1228 setups
     dev, ref = make_pair(sched, orc, [48, 48], [24, 24], 0.4, [2], [], model="modelc", integrator=integrator,
                          seed=7, policy=MC_POLICY)
     set_both(dev, ref, 0, _seed)
     set_both(dev, ref, 1, lambda x, y: np.full_like(x, -0.7))
     dt = ref.suggested_dt()
-    dev.run(dt, steps, graph=True)
+    dev.run(dt, steps, **MODES[mode])
     ref.step(dt, steps)
     assert dev.num_levels == 2
     same_state(dev, ref, 2)
 
 
-def test_adaptive_model_c_three_levels_with_noise(sched, orc):
+@pytest.mark.parametrize("mode", ["graph", "persistent"])
+def test_adaptive_model_c_three_levels_with_noise(sched, orc, mode):
     dev, ref = make_pair(sched, orc, [64, 64], [32, 32], 0.4, [2, 2], [], model="modelc", seed=3, noise=0.02,
                          policy=dict(every=5, buffer=2, efficiency=0.8, min_width=4, threshold=0.1))
     set_both(dev, ref, 0, lambda x, y: np.maximum(-1.0, -np.vectorize(math.tanh)(
         (np.vectorize(math.hypot)(x - 12.8, y - 12.8) - 5.0) / math.sqrt(2.0))))
     set_both(dev, ref, 1, lambda x, y: np.full_like(x, -0.6))
     dt = ref.suggested_dt()
-    dev.run(dt, 12, graph=True)
+    dev.run(dt, 12, **MODES[mode])
     ref.step(dt, 12)
     assert dev.num_levels == ref.num_levels == 3
     same_state(dev, ref, 2, exact=False)
