@@ -218,6 +218,17 @@ int lg_amr_restrict(lg_amr_sim* sim, int field);
 int lg_amr_fill_ghosts(lg_amr_sim* sim);
 int lg_amr_tag_level(lg_amr_sim* sim, int field, int level, double threshold, int64_t* cells_out, int64_t cap,
                      int64_t* count);
+/* lg_amr_tag_level without any allocation.  No counterpart in the reference:
+ * it serves callers that cannot allocate device memory (a step loop whose
+ * memory a caching allocator holds, or a latency-bound loop that a
+ * synchronising cudaMalloc/cudaFree would stall).  The flags are compacted in
+ * a static device scratch of 2^18 cells (4 MiB) and sorted in place in
+ * cells_out.  Fails with LG_ERR_INVALID when the level has more than 2^18
+ * cells, or when cap < *count (nothing copied, *count set).  Calls that
+ * overlap on the GPU race on the scratch; the first call on a device
+ * resolves the scratch's address and must come before any stream capture. */
+int lg_amr_tag_level_static(lg_amr_sim* sim, int field, int level, double threshold, int64_t* cells_out,
+                            int64_t cap, int64_t* count);
 
 /* Standard normals of n keys on the device (`rng::standard_normal`,
  * src/util/rng.rs:43-49); host arrays in and out. */

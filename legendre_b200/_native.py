@@ -124,6 +124,7 @@ _SIGS = {
     "lg_amr_restrict": (C.c_int, [_p, C.c_int]),
     "lg_amr_fill_ghosts": (C.c_int, [_p]),
     "lg_amr_tag_level": (C.c_int, [_p, C.c_int, C.c_int, _d, _pi64, _i64, _pi64]),
+    "lg_amr_tag_level_static": (C.c_int, [_p, C.c_int, C.c_int, _d, _pi64, _i64, _pi64]),
 }
 
 for _name, (_res, _args) in _SIGS.items():

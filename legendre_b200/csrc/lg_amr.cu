@@ -11,6 +11,7 @@
 #include <cmath>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -123,6 +124,43 @@ __global__ void amr_tag_kernel(const BlockDesc* __restrict__ blocks, const int64
 // and pre-step buffers for the time-interpolated prolongation (the coarse
 // level's ping-pong buffer from before its step is the reference's
 // snapshot: nothing writes that level's slabs of it until its next step).
+// ------------------------------------------- tagging without allocation --
+// Static scratch of lg_amr_tag_level_static: word 0 is the flag counter,
+// then one (x, y) pair per flagged cell.  It holds kStaticTagCells cells
+// (4 MiB), and a level with more cells is rejected before any launch, so the
+// compaction cannot overflow.  The array is file-scope and shared by every
+// call in the process on a device: calls that overlap on the GPU race.
+constexpr int64_t kStaticTagCells = int64_t(1) << 18;
+__device__ __align__(256) int64_t g_tag_scratch[2 + 2 * kStaticTagCells];
+
+// amr_tag_kernel with its output in the static scratch (count at word 0)
+__global__ void amr_tag_static_kernel(const BlockDesc* __restrict__ blocks, const int64_t* __restrict__ lo,
+                                      const Unit* __restrict__ units, int64_t nunits, const double* __restrict__ A,
+                                      int field, double threshold, int64_t* __restrict__ scratch) {
+    unsigned long long* count = (unsigned long long*)scratch;
+    int64_t* out = scratch + 2;
+    for (int64_t u = blockIdx.x; u < nunits; u += gridDim.x) {
+        const Unit un = units[u];
+        const BlockDesc b = blocks[un.block];
+        const double* v = A + b.off + field * b.stride;
+        const int sy = b.nx + 2;
+        for (int c = un.start + threadIdx.x; c < un.start + un.count; c += blockDim.x) {
+            const int i = c % b.nx, j = c / b.nx;
+            const int o = (i + 1) + (j + 1) * sy;
+            double gmax = 0.0;
+            gmax = fmax(gmax, fabs((v[o + 1] - v[o - 1]) * 0.5));
+            gmax = fmax(gmax, fabs((v[o + sy] - v[o - sy]) * 0.5));
+            if (gmax > threshold) {
+                const unsigned long long k = atomicAdd(count, 1ull);
+                if ((int64_t)k < kStaticTagCells) {
+                    out[2 * k] = lo[2 * un.block] + i;
+                    out[2 * k + 1] = lo[2 * un.block + 1] + j;
+                }
+            }
+        }
+    }
+}
+
 struct TileArgs {
     const lg::amr::Tile* tiles;
     int64_t ntiles;
@@ -1486,6 +1524,84 @@ int lg_amr_tag_level(lg_amr_sim* s, int field, int level, double threshold, int6
     for (int64_t k = 0; k < (int64_t)cells.size() && k < cap; ++k) {
         cells_out[2 * k] = cells[k][0];
         cells_out[2 * k + 1] = cells[k][1];
+    }
+    return LG_OK;
+}
+
+// A tagging entry point that allocates nothing (no cudaMalloc, cudaFree or
+// allocating library call on the device, no host heap): the flags are
+// compacted into the file-scope static scratch above, whose address is
+// resolved once per device, and sorted in place in the caller's buffer.  It
+// serves callers that cannot allocate: a step loop whose device memory is
+// all held by a caching allocator (a cudaMalloc there fails or forces the
+// cache to be released), and latency-bound loops in which cudaMalloc /
+// cudaFree, which synchronise the device, would stall the stream.
+// Limits: the level has at most 2^18 cells; cells_out needs room for every
+// flagged cell (cap >= *count), else nothing is copied and the call fails
+// with *count set.  Calls that overlap on the GPU race on the scratch; the
+// first call on a device (which resolves the scratch address) must come
+// before any stream capture.
+namespace {
+std::mutex g_scratch_mutex;
+int64_t* g_scratch_ptr[64] = {};
+}  // namespace
+
+int lg_amr_tag_level_static(lg_amr_sim* s, int field, int level, double threshold, int64_t* cells_out, int64_t cap,
+                            int64_t* count) {
+    if (!s || !count || (cap > 0 && !cells_out) || cap < 0 || field < 0 || field >= s->nfields || level < 0 ||
+        level >= s->layout.num_levels())
+        return fail(s, LG_ERR_INVALID, "bad tag arguments");
+    const int dev = lg::abi_device(s->ctx);
+    if (dev < 0 || dev >= 64) return fail(s, LG_ERR_INVALID, "device ordinal out of range for the static scratch");
+    int64_t cells = 0;
+    for (uint32_t b = s->layout.level_start[level]; b < s->layout.level_start[level + 1]; ++b)
+        cells += (int64_t)s->plans.blocks[b].nx * s->plans.blocks[b].ny;
+    if (cells > kStaticTagCells)
+        return fail(s, LG_ERR_INVALID, "level " + std::to_string(level) + " has " + std::to_string(cells) +
+                                           " cells; the static tag scratch holds at most " +
+                                           std::to_string(kStaticTagCells));
+    AMR_CUDA(s, cudaSetDevice(dev));
+    int64_t* scratch = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(g_scratch_mutex);
+        if (!g_scratch_ptr[dev]) {
+            void* p = nullptr;
+            const cudaError_t e = cudaGetSymbolAddress(&p, g_tag_scratch);
+            if (e != cudaSuccess)
+                return fail(s, LG_ERR_CUDA, std::string("cudaGetSymbolAddress(static tag scratch): ") +
+                                                cudaGetErrorString(e));
+            g_scratch_ptr[dev] = (int64_t*)p;
+        }
+        scratch = g_scratch_ptr[dev];
+    }
+    cudaStream_t st = lg::abi_stream(s->ctx);
+    AMR_CUDA(s, cudaMemsetAsync(scratch, 0, sizeof(int64_t), st));  // the counter starts at zero
+    const Lists L = lists(s, level);
+    const int64_t u0 = L.P->unit_start[level], u1 = L.P->unit_start[level + 1];
+    if (u1 > u0) {
+        amr_tag_static_kernel<<<(unsigned)std::min<int64_t>(u1 - u0, 65535), 256, 0, st>>>(
+            s->tab.blocks, s->tab.lo, L.T->units + u0, u1 - u0, s->arena[s->cur[level]], field, threshold, scratch);
+        lg::abi_count_launch(s->ctx, 1);
+        AMR_CUDA(s, cudaGetLastError());
+    }
+    int64_t n = 0;
+    AMR_CUDA(s, cudaMemcpyAsync(&n, scratch, sizeof n, cudaMemcpyDeviceToHost, st));
+    AMR_CUDA(s, cudaStreamSynchronize(st));
+    *count = n;
+    if (n > cap)
+        return fail(s, LG_ERR_INVALID, "cells_out holds " + std::to_string(cap) + " cells; " + std::to_string(n) +
+                                           " were flagged");
+    if (n > 0) {
+        AMR_CUDA(s, cudaMemcpyAsync(cells_out, scratch + 2, (size_t)n * 2 * sizeof(int64_t), cudaMemcpyDeviceToHost,
+                                    st));
+        AMR_CUDA(s, cudaStreamSynchronize(st));
+        struct Cell2 {
+            int64_t x, y;
+            bool operator<(const Cell2& o) const { return x < o.x || (x == o.x && y < o.y); }
+        };
+        static_assert(sizeof(Cell2) == 2 * sizeof(int64_t), "cells are packed pairs");
+        Cell2* c = reinterpret_cast<Cell2*>(cells_out);
+        std::sort(c, c + n);  // in place
     }
     return LG_OK;
 }
