@@ -230,6 +230,39 @@ int lg_amr_tag_level(lg_amr_sim* sim, int field, int level, double threshold, in
 int lg_amr_tag_level_static(lg_amr_sim* sim, int field, int level, double threshold, int64_t* cells_out,
                             int64_t cap, int64_t* count);
 
+/* ----------------------------------------------------------- ensembles --
+ * Batched Model C: `ninst` independent instances of one 2-D grid geometry
+ * (cells[2] in blocks of block[2], spacing[2], zero-flux boundaries), each
+ * with its own eps4 and Wiener seed, sharing lambda, D, the noise amplitude
+ * and the tolerances of `p`.  No counterpart in the reference, which runs
+ * one Simulation per realisation; each instance's trajectory is the one its
+ * own Simulation (lg_modelc_em_run on the same grid) produces -- bit for bit
+ * in FP64.  Host arrays are instance-major, then row-major (x fastest):
+ * n = ninst * cells[0] * cells[1]. */
+typedef struct lg_ensemble lg_ensemble;
+int lg_ensemble_create(lg_ctx* ctx, const int64_t* cells, const int64_t* block, const double* spacing, int64_t ninst,
+                       const lg_modelc_params* p, const double* eps4, const uint64_t* seeds, int dtype,
+                       lg_ensemble** out);
+int lg_ensemble_destroy(lg_ensemble* e);
+int lg_ensemble_upload(lg_ensemble* e, int field, const double* host, int64_t n);
+int lg_ensemble_download(lg_ensemble* e, int field, double* host, int64_t n);
+int lg_ensemble_set_time(lg_ensemble* e, double t, int64_t step_index);
+int lg_ensemble_get_time(const lg_ensemble* e, double* t, int64_t* step_index);
+/* `nsteps` Euler-Maruyama steps of every instance (LG_RUN_GRAPH: pairs of
+ * steps replayed from a CUDA graph). */
+int lg_ensemble_run(lg_ensemble* e, double dt, int64_t nsteps, uint32_t flags);
+/* Differentiation.  From the current state x_0, runs `nsteps` steps storing
+ * the state every `ckpt_every` steps, evaluates
+ * L_i = sum over the cells of (phi_T - target)^2 per instance, and runs the
+ * hand-written adjoint of the fused step back to x_0, recomputing each
+ * segment from its checkpoint (the noise replays from its keys).  Returns
+ * loss[i], grad_params[4 i + k] = dL_i/d(lambda, D, eps4, Delta) -- Delta
+ * taken as the undercooling of an initial u = -Delta on every cell -- and,
+ * when non-null, dL_i/dphi_0 and dL_i/du_0 per cell.  The state is left at
+ * x_T.  Parameter gradients accumulate in FP64 (FP32 ensembles included). */
+int lg_ensemble_value_and_grad(lg_ensemble* e, double dt, int64_t nsteps, int64_t ckpt_every, const double* target,
+                               double* loss, double* grad_params, double* grad_phi0, double* grad_u0);
+
 /* Standard normals of n keys on the device (`rng::standard_normal`,
  * src/util/rng.rs:43-49); host arrays in and out. */
 int lg_standard_normal(lg_ctx* ctx, const uint64_t* keys, int64_t n, double* out);

@@ -8,13 +8,15 @@ from .core import CudaAllocator, CudaScheduler, DeviceState, FieldSpec, Simulati
 from .geometry import CartesianGrid, GridError
 from .integrators import EulerMaruyama, FiniteDifference, FiniteVolume, ForwardEuler
 from .physics import A1, A2, Grain, Heat, ModelC, seed_positions
+from .ensemble import Ensemble
 from .amr import (AmrGrid, AmrSimulation, BergerOliger, CellBox, ClusterParams, GradientTagger, RegridPolicy,
                   Subcycling)
 
 __all__ = [
     "AmrGrid", "AmrSimulation", "BergerOliger", "CellBox", "ClusterParams", "GradientTagger", "RegridPolicy",
     "Subcycling",
-    "A1", "A2", "CartesianGrid", "CudaAllocator", "CudaScheduler", "DeviceState", "EulerMaruyama", "FieldSpec",
+    "A1", "A2", "CartesianGrid", "CudaAllocator", "CudaScheduler", "DeviceState", "Ensemble", "EulerMaruyama",
+    "FieldSpec",
     "FiniteDifference", "FiniteVolume", "ForwardEuler", "Grain", "GridError", "Heat", "LegendreError", "ModelC",
     "Simulation", "StateBuilder", "TIME", "seed_positions", "wiener",
 ]

@@ -124,6 +124,15 @@ _SIGS = {
     "lg_amr_restrict": (C.c_int, [_p, C.c_int]),
     "lg_amr_fill_ghosts": (C.c_int, [_p]),
     "lg_amr_tag_level": (C.c_int, [_p, C.c_int, C.c_int, _d, _pi64, _i64, _pi64]),
+    "lg_ensemble_create": (C.c_int, [_p, _pi64, _pi64, _pd, _i64, C.POINTER(ModelCParams), _pd, C.POINTER(C.c_uint64),
+                                     C.c_int, C.POINTER(_p)]),
+    "lg_ensemble_destroy": (C.c_int, [_p]),
+    "lg_ensemble_upload": (C.c_int, [_p, C.c_int, _pd, _i64]),
+    "lg_ensemble_download": (C.c_int, [_p, C.c_int, _pd, _i64]),
+    "lg_ensemble_set_time": (C.c_int, [_p, _d, _i64]),
+    "lg_ensemble_get_time": (C.c_int, [_p, _pd, _pi64]),
+    "lg_ensemble_run": (C.c_int, [_p, _d, _i64, C.c_uint32]),
+    "lg_ensemble_value_and_grad": (C.c_int, [_p, _d, _i64, _i64, _pd, _pd, _pd, _pd, _pd]),
     "lg_amr_tag_level_static": (C.c_int, [_p, C.c_int, C.c_int, _d, _pi64, _i64, _pi64]),
 }
 

@@ -37,6 +37,8 @@ SOURCES = [
     ("lg_abi.cu", ["-fmad=false"]),
     ("lg_amr_host.cu", ["-fmad=false"]),
     ("lg_amr.cu", ["-fmad=false"]),
+    ("lg_adjoint.cu", []),      # not bit-matched to anything: contraction allowed
+    ("lg_ensemble.cu", ["-fmad=false"]),
 ]
 
 

@@ -62,6 +62,21 @@ cudaError_t launch_modelc_tile_f32(const float* in, float* out, const CartTopo& 
                                    const ModelCDev& m, double dt, const NoiseDev& nz, double* tdev, int slot,
                                    int rows, int minb, cudaStream_t s);
 
+// Batched instances (an ensemble of independent grids of one geometry):
+// block b of the topology belongs to instance b / bpi, with the parameter
+// record params[instance] (built by modelc_record_*) and Wiener seed
+// seeds[instance]; noise keys use the instance-local block index.
+size_t modelc_record_size_f64();
+void modelc_record_f64(const ModelCDev& m, void* out);
+size_t modelc_record_size_f32();
+void modelc_record_f32(const ModelCDev& m, void* out);
+cudaError_t launch_modelc_batch_f64(const double* in, double* out, const CartTopo& topo, const SlabLayout& L,
+                                    const void* params, const uint64_t* seeds, int bpi, double dt, double amp,
+                                    double* tdev, int slot, int rows, cudaStream_t s);
+cudaError_t launch_modelc_batch_f32(const float* in, float* out, const CartTopo& topo, const SlabLayout& L,
+                                    const void* params, const uint64_t* seeds, int bpi, double dt, double amp,
+                                    double* tdev, int slot, int rows, cudaStream_t s);
+
 // Standard normals of a key array (tests of the generator).
 cudaError_t launch_standard_normal(const uint64_t* keys, double* out, int64_t n, cudaStream_t s);
 

@@ -22,4 +22,19 @@ cudaError_t launch_modelc_tile_f64(const double* in, double* out, const CartTopo
     return launch_strip_ops<double, OpsExact<double>, false, 1>(in, out, g, mc, dt, scale_amp, minb, s);
 }
 
+size_t modelc_record_size_f64() { return sizeof(MC<double>); }
+void modelc_record_f64(const ModelCDev& m, void* out) { *static_cast<MC<double>*>(out) = to_mc<double>(m); }
+
+cudaError_t launch_modelc_batch_f64(const double* in, double* out, const CartTopo& topo, const SlabLayout& L,
+                                    const void* params, const uint64_t* seeds, int bpi, double dt, double amp,
+                                    double* tdev, int slot, int rows, cudaStream_t s) {
+    TileArgs g{topo, L, dt, 0, tdev, slot, rows, 0, 0, 0};
+    g.params = params;
+    g.seeds = seeds;
+    g.bpi = bpi;
+    const double scale_amp = std::sqrt(dt) * amp;
+    if (amp != 0.0) return launch_strip_batch<double, OpsExact<double>, true, 2>(in, out, g, dt, scale_amp, s);
+    return launch_strip_batch<double, OpsExact<double>, false, 2>(in, out, g, dt, scale_amp, s);
+}
+
 }  // namespace lg

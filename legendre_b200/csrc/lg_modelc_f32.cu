@@ -85,10 +85,8 @@ struct OpsFast32 {
 
 }  // namespace
 
-cudaError_t launch_modelc_tile_f32(const float* in, float* out, const CartTopo& topo, const SlabLayout& L,
-                                   const ModelCDev& m, double dt, const NoiseDev& nz, double* tdev, int slot,
-                                   int rows, int minb, cudaStream_t s) {
-    TileArgs g{topo, L, dt, nz.seed, tdev, slot, rows, 0, 0, 0};
+namespace {
+Fast32 fast32_of(const ModelCDev& m) {
     Fast32 f{};
     f.lambda = (float)m.lambda;
     f.d_thermal = (float)m.d_thermal;
@@ -104,9 +102,33 @@ cudaError_t launch_modelc_tile_f32(const float* in, float* out, const CartTopo& 
     f.c_a1pe = (float)(m.a_bar * (1.0 + m.eps_prime));
     f.c_2ae = (float)(2.0 * m.a_bar * m.eps_prime);
     f.c_tol = (float)m.tol;
+    return f;
+}
+}  // namespace
+
+cudaError_t launch_modelc_tile_f32(const float* in, float* out, const CartTopo& topo, const SlabLayout& L,
+                                   const ModelCDev& m, double dt, const NoiseDev& nz, double* tdev, int slot,
+                                   int rows, int minb, cudaStream_t s) {
+    TileArgs g{topo, L, dt, nz.seed, tdev, slot, rows, 0, 0, 0};
+    const Fast32 f = fast32_of(m);
     const float scale_amp = (float)(std::sqrt(dt) * nz.amp);
     if (nz.on) return launch_strip_ops<float, OpsFast32, true, 1>(in, out, g, f, (float)dt, scale_amp, minb, s);
     return launch_strip_ops<float, OpsFast32, false, 1>(in, out, g, f, (float)dt, scale_amp, minb, s);
+}
+
+size_t modelc_record_size_f32() { return sizeof(Fast32); }
+void modelc_record_f32(const ModelCDev& m, void* out) { *static_cast<Fast32*>(out) = fast32_of(m); }
+
+cudaError_t launch_modelc_batch_f32(const float* in, float* out, const CartTopo& topo, const SlabLayout& L,
+                                    const void* params, const uint64_t* seeds, int bpi, double dt, double amp,
+                                    double* tdev, int slot, int rows, cudaStream_t s) {
+    TileArgs g{topo, L, dt, 0, tdev, slot, rows, 0, 0, 0};
+    g.params = params;
+    g.seeds = seeds;
+    g.bpi = bpi;
+    const float scale_amp = (float)(std::sqrt(dt) * amp);
+    if (amp != 0.0) return launch_strip_batch<float, OpsFast32, true, 3>(in, out, g, (float)dt, scale_amp, s);
+    return launch_strip_batch<float, OpsFast32, false, 3>(in, out, g, (float)dt, scale_amp, s);
 }
 
 }  // namespace lg

@@ -52,6 +52,13 @@ struct TileArgs {
     int strips;   // 32-column strips per block
     int chunks;   // row chunks per block
     int64_t units;
+    // batched instances (BATCH kernels): block b belongs to instance
+    // b / bpi, whose parameters are params[instance] (an Ops::Params array
+    // on the device) and whose Wiener seed is seeds[instance]; its noise
+    // keys use the instance-local block index b % bpi
+    const void* params = nullptr;
+    const uint64_t* seeds = nullptr;
+    int bpi = 0;
 };
 
 template <class T>
@@ -118,9 +125,9 @@ __device__ __forceinline__ void strip_row(const typename Ops::Params& m, const T
 
 // Rows per work unit are at most 32, so one batch of boundary faces (lanes
 // across rows) serves the whole unit.
-template <class T, class Ops, bool NOISE, int MINB, int NX, int PF>
+template <class T, class Ops, bool NOISE, int MINB, int NX, int PF, bool BATCH = false>
 __global__ void __launch_bounds__(256, MINB)
-    modelc_strip_kernel(const T* __restrict__ in, T* __restrict__ out, TileArgs g, typename Ops::Params m, T dt,
+    modelc_strip_kernel(const T* __restrict__ in, T* __restrict__ out, TileArgs g, typename Ops::Params m0, T dt,
                         T scale_amp) {
     constexpr bool FULL = NX > 0 && NX % 32 == 0;
     constexpr int NB = PF + 3;  // window rows: j-1, j, j+1 and PF rows of prefetch
@@ -158,9 +165,19 @@ __global__ void __launch_bounds__(256, MINB)
         T* uo = out + slab_base(g.L, b, 1);
         Nbr2 nb;
         nb.load(topo, b);
+        typename Ops::Params m = m0;
+        uint64_t seed = g.seed;
+        int key_block = b;
+        if (BATCH) {
+            const int inst = b / g.bpi;
+            m = static_cast<const typename Ops::Params*>(g.params)[inst];
+            seed = g.seeds[inst];
+            key_block = b - inst * g.bpi;
+        }
         uint64_t block_key = 0;
         if (NOISE)
-            block_key = wiener_block_key(g.seed, (uint64_t)__double_as_longlong(tnow), kWienerStream0, (uint64_t)b);
+            block_key = wiener_block_key(seed, (uint64_t)__double_as_longlong(tnow), kWienerStream0,
+                                         (uint64_t)key_block);
 
         int off = (col + 1) + (r0 + 1) * sy;  // slab offset of (col, r0)
         Row3<T> w[NB];
@@ -227,6 +244,32 @@ inline int strip_rows(const CartTopo& topo, int strips, int rows) {
         rows = std::max(8, (n1 + chunks - 1) / chunks);
     }
     return std::max(1, std::min(std::min(rows, 32), n1));
+}
+
+// work decomposition of a launch: units of (block, strip, row chunk)
+inline dim3 strip_grid(TileArgs& g) {
+    const int n0 = g.topo.n[0], n1 = g.topo.n[1];
+    g.strips = (n0 + 31) / 32;
+    g.rows = strip_rows(g.topo, g.strips, g.rows);
+    g.chunks = (n1 + g.rows - 1) / g.rows;
+    g.units = (int64_t)g.topo.nblocks * g.strips * g.chunks;
+    const int wpc = 8;
+    const int64_t ctas = std::min<int64_t>((g.units + wpc - 1) / wpc, (int64_t)1 << 30);
+    return dim3((unsigned)ctas);
+}
+
+// batched instances: block widths 64 (the ensemble configuration) and 32
+// get a compile-time row stride
+template <class T, class Ops, bool NOISE, int MINB>
+cudaError_t launch_strip_batch(const T* in, T* out, TileArgs g, T dt, T scale_amp, cudaStream_t s) {
+    const dim3 grid = strip_grid(g), block(256);
+    const typename Ops::Params m{};
+    switch (g.topo.n[0]) {
+        case 32: modelc_strip_kernel<T, Ops, NOISE, MINB, 32, 1, true><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp); break;
+        case 64: modelc_strip_kernel<T, Ops, NOISE, MINB, 64, 1, true><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp); break;
+        default: modelc_strip_kernel<T, Ops, NOISE, MINB, 0, 1, true><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp);
+    }
+    return cudaGetLastError();
 }
 
 template <class T, class Ops, bool NOISE, int MINB, int PF>
