@@ -50,6 +50,13 @@ CONFIGS = {
     "c4": dict(kind="amr", workload="model_c_amr_1024sq_3lev", cells=1024, block=32, h=0.4, d_thermal=2.0,
                lam=2.0 / 0.6267, eps4=0.05, u0=0.55, radius=8.0, ratios=[2, 2, 2], every=50, buffer=2,
                threshold=0.05, noise=0.0, full_steps=4000),
+    # batched ensemble + adjoint: 256 instances of 256^2 as 4x4 blocks of 64^2,
+    # per-instance eps4 ~ U[0.02, 0.07], Delta ~ U[0.45, 0.65] and seed drawn
+    # by unit_open(mix_key(master, [i, k])); one central grain r = 8; noise
+    # b = 0.005; FP32 forward, FP64 gradient accumulation; 2000 steps with a
+    # checkpoint every 100; loss against phi_T at perturbed eps4 and Delta
+    "c5": dict(kind="ensemble", workload="model_c_ensemble_256x256sq", instances=256, cells=256, block=64, h=0.4,
+               d_thermal=2.0, lam=2.0 / 0.6267, radius=8.0, noise=0.005, seed=42, ckpt=100, full_steps=2000),
 }
 
 BYTES_PER_CELL = {"f64": 32, "f32": 16}  # read phi, u; write phi, u
@@ -320,6 +327,163 @@ def run_other(args, cfg):
         pg.destroy_process_group()
 
 
+def ensemble_setup(cfg, ninst):
+    """Per-instance eps4, Delta, seed and the initial fields of the ensemble
+    workload (instances, ny, nx)."""
+    import math
+
+    import numpy as np
+
+    from legendre_b200.rng import mix_key, unit_open
+
+    m = cfg["seed"]
+    eps4 = [0.02 + 0.05 * unit_open(mix_key(m, [i, 0])) for i in range(ninst)]
+    delta = [0.45 + 0.2 * unit_open(mix_key(m, [i, 1])) for i in range(ninst)]
+    seeds = [mix_key(m, [i, 2]) for i in range(ninst)]
+    n, h = cfg["cells"], cfg["h"]
+    x = (np.arange(n) + 0.5) * h
+    r = np.hypot(x[None, :] - n * h / 2, x[:, None] - n * h / 2)
+    phi = np.maximum(-1.0, -np.tanh((r - cfg["radius"]) / math.sqrt(2.0)))
+    phi0 = np.broadcast_to(phi, (ninst, n, n))
+    u0 = -np.asarray(delta)[:, None, None] * np.ones((1, n, n))
+    return eps4, delta, seeds, phi0, u0
+
+
+def run_ensemble(args, cfg):
+    """The batched ensemble (c5): forward throughput of all instances, and
+    the cost of the value-and-gradient pass against the forward pass alone."""
+    import numpy as np
+    import torch
+
+    import legendre_b200 as L
+
+    rank, world, local, pg = dist_setup(args.gpus)
+    stream = torch.cuda.Stream(device=local)
+    torch.cuda.set_stream(stream)
+    sched = L.CudaScheduler(local, stream.cuda_stream)
+    dtype = args.dtype if args.dtype_given else "f32"
+    ninst, n, b, h = cfg["instances"], cfg["cells"], cfg["block"], cfg["h"]
+    grid = L.CartesianGrid([n, n], [b, b], [0.0, 0.0], [h, h])
+    model = L.ModelC(0.05, cfg["lam"], cfg["noise"])
+    model.d_thermal = cfg["d_thermal"]
+    eps4, delta, seeds, phi0, u0 = ensemble_setup(cfg, ninst)
+    seeds = [(s + rank) % (1 << 64) for s in seeds]
+    dt = 0.2 * h * h / cfg["d_thermal"]
+    cells = ninst * n * n
+
+    def fresh(e4, dl):
+        ens = L.Ensemble(grid, model, e4, seeds, sched, dtype=dtype)
+        ens.set("phi", phi0)
+        ens.set("u", -np.asarray(dl)[:, None, None] * np.ones((1, n, n)))
+        return ens
+
+    # forward throughput
+    ens = fresh(eps4, delta)
+    ens.run(dt, args.warmup, graph=True)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    barrier(pg)
+    torch.cuda.synchronize()
+    launches0 = sched.kernel_launches
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    ens.run(dt, args.steps, graph=True)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier(pg)
+    clk = clocks.stop()
+    launches = sched.kernel_launches - launches0
+    ms = max_over_ranks(pg, e0.elapsed_time(e1))
+    value = world * cells * args.steps / (ms / 1e3) / 1e9
+
+    # end to end through the public API: host fields in, K steps, phi out
+    barrier(pg)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e2.record(stream)
+    ens.set("phi", phi0)
+    ens.set("u", u0)
+    ens.run(dt, args.steps, graph=True)
+    phi_out = ens.get("phi")
+    e3.record(stream)
+    torch.cuda.synchronize()
+    ms_e2e = max_over_ranks(pg, 1e3 * (time.perf_counter() - t0))
+    ens._destroy()
+
+    # value and gradient over the configuration's horizon against a target at
+    # perturbed eps4 and Delta, and the forward pass of the same horizon
+    T = min(args.steps, cfg["full_steps"])
+    tgt = fresh([e + 0.005 for e in eps4], [d + 0.01 for d in delta])
+    tgt.run(dt, T, graph=True)
+    target = tgt.get("phi")
+    tgt._destroy()
+    ens = fresh(eps4, delta)
+    torch.cuda.synchronize()
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    ens.run(dt, T, graph=True)
+    f1.record(stream)
+    torch.cuda.synchronize()
+    ms_fwd = f0.elapsed_time(f1)
+    ens._destroy()
+    ens = fresh(eps4, delta)
+    torch.cuda.synchronize()
+    g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    g0.record(stream)
+    g = ens.value_and_grad(dt, T, cfg["ckpt"], target, cell_grads=False)
+    g1.record(stream)
+    torch.cuda.synchronize()
+    ms_vg = g0.elapsed_time(g1)
+    ens._destroy()
+    ms_fwd, ms_vg = max_over_ranks(pg, ms_fwd), max_over_ranks(pg, ms_vg)
+
+    if rank == 0:
+        peak, peak_kind = peaks()
+        bpc = BYTES_PER_CELL[dtype]
+        achieved = bpc * cells / (ms / args.steps / 1e3) / 1e9
+        cpu = None
+        if not args.no_cpu_baseline and world == 1:
+            c2 = dict(CONFIGS["c2"], cells=n, block=b, grains=1, noise=cfg["noise"], u0=delta[0], eps4=eps4[0],
+                      dt=dt)
+            rate, steps_run, threads = cpu_oracle_rate(c2, steps_budget_s=15.0, max_steps=2000)
+            cpu = {"value": rate, "unit": "Gcell-updates/s", "cores": threads, "kind": "port",
+                   "sample": f"{steps_run} steps of one {n}^2 instance (the instances are independent; the rate "
+                             "per cell-update is the same), OpenMP over blocks"}
+        esz = 8 if dtype == "f64" else 4
+        line = {
+            "metric": "Gcell-updates/s", "value": value, "unit": "Gcell-updates/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": dtype, "data": "synthetic",
+            "config": {"workload": cfg["workload"], "instances": ninst, "cells": n, "block": b,
+                       "noise": cfg["noise"], "parallelism": f"replicas{world}", "graph": True,
+                       "l2": "state larger than L2; no flush"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
+                         "algorithmic_bytes_per_cell": bpc},
+            "adjoint": {"steps": T, "checkpoint_every": cfg["ckpt"], "forward_ms": ms_fwd,
+                        "value_and_grad_ms": ms_vg, "cost_ratio": ms_vg / ms_fwd,
+                        "what": "value_and_grad = forward with checkpoints + loss + per segment: recompute and "
+                                "adjoint steps; cost_ratio = its time / the forward pass alone",
+                        "mean_loss": float(np.mean(g["loss"])),
+                        "mean_grad": {k: float(np.mean(g[k])) for k in ("lambda", "d_thermal", "eps4", "delta")}},
+            "cpu_baseline": cpu,
+            "e2e": {"value": world * cells * args.steps / (ms_e2e / 1e3) / 1e9, "unit": "Gcell-updates/s",
+                    "h2d_bytes_per_step": 2 * cells * 8 / args.steps, "d2h_bytes_per_step": cells * 8 / args.steps,
+                    "what": f"Ensemble.set phi and u from host + {args.steps} steps + Ensemble.get phi, "
+                            "host wall clock, bytes amortised per step"},
+            "gpu_launches": launches,
+            "clocks": {"sm_mhz": clk["sm_mhz"], "sm_max_mhz": clk["sm_max_mhz"], "reasons": clk["reasons"],
+                       "samples": clk["samples"]},
+        }
+        print(json.dumps(line), flush=True)
+    sched.close()
+    if pg is not None:
+        pg.destroy_process_group()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -332,6 +496,7 @@ def main():
     ap.add_argument("--noise", type=float, default=None, help="override the noise amplitude b")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
+    args.dtype_given = any(a == "--dtype" or a.startswith("--dtype=") for a in sys.argv[1:])
     args.warmup = max(args.warmup, 3)
     cfg = dict(CONFIGS[args.config])
     if args.noise is not None:
@@ -342,6 +507,9 @@ def main():
 
     if cfg.get("kind") in ("heat", "amr"):
         run_other(args, cfg)
+        return
+    if cfg.get("kind") == "ensemble":
+        run_ensemble(args, cfg)
         return
 
     import torch
