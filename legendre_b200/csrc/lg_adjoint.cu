@@ -41,10 +41,10 @@ namespace {
 
 constexpr int TW = 32;
 
-template <class T>
-__device__ __forceinline__ T recip(T x) {
-    return T(1) / x;
-}
+__device__ __forceinline__ double recip(double x) { return 1.0 / x; }
+// single precision: the correctly rounded hardware reciprocal (the FP32
+// adjoint is not matched bit for bit to anything)
+__device__ __forceinline__ float recip(float x) { return __frcp_rn(x); }
 
 // a(x, y), da(x, y) of KarmaRappelFlux::face and their partial derivatives
 // in x, y and eps4; x and y are the face's (derx, dery).
@@ -85,6 +85,34 @@ __device__ __forceinline__ FaceDer<T> face_der(T x, T y, T a_bar, T ae, T a12, T
     return f;
 }
 
+// A_c(hx, hy) of ModelC::center_anisotropy and dA/dhx, dA/dhy, dA/deps4
+template <class T>
+struct CentreDer {
+    T a, ax, ay, ae;
+};
+
+template <class T>
+__device__ __forceinline__ CentreDer<T> centre_der(T x, T y, T a_bar, T ae, T tol) {
+    CentreDer<T> c;
+    const T x2 = x * x, y2 = y * y;
+    const T s = x2 + y2;
+    if (s * s <= tol) {
+        c.a = a_bar;
+        c.ax = c.ay = T(0);
+        c.ae = T(-3);
+        return c;
+    }
+    const T is = recip(s);
+    const T is2 = is * is, is3 = is2 * is;
+    const T R = (x2 * x2 + y2 * y2) * is2;
+    const T k = T(4) * (x2 - y2) * is3 * ae;
+    c.a = a_bar + ae * R;
+    c.ax = k * x * y2;
+    c.ay = -k * y * x2;
+    c.ae = T(-3) + T(3) * R;
+    return c;
+}
+
 template <class T, int TH>
 struct Smem {
     static constexpr int W2 = TW + 4, H2 = TH + 4, N = W2 * H2;
@@ -94,12 +122,28 @@ struct Smem {
     T xj[N], xn[N], xt[N], xe[N];  // x faces: J, dJ/ddn (then Jbar dJ/ddn), dJ/ddt (then Jbar ...), dJ/deps
     T yj[N], yn[N], yt[N], ye[N];
     unsigned char out[N];  // bit 0: outside the instance in x, bit 1: in y
+    int64_t col[W2];       // offset terms of a window column / row (see stage)
+    int64_t row[H2];
+    unsigned char cout_[W2], rout[H2];
     double red[3][32];
 };
 
 __device__ __forceinline__ int reflect_clamp(int c, int n) {
     c = c < 0 ? -1 - c : (c >= n ? 2 * n - 1 - c : c);
     return c < 0 ? 0 : (c >= n ? n - 1 : c);
+}
+
+// the column (x) and row (y) terms of cell_offset: offset = inst * bpi * 2 *
+// slab_stride + col_term(X) + row_term(Y)
+__device__ __forceinline__ int64_t col_term(const Geo& g, int X) {
+    X = reflect_clamp(X, g.N0);
+    const int bx = X / g.n0;
+    return (int64_t)bx * 2 * g.slab_stride + (X - bx * g.n0 + 1);
+}
+__device__ __forceinline__ int64_t row_term(const Geo& g, int Y) {
+    Y = reflect_clamp(Y, g.N1);
+    const int by = Y / g.n1;
+    return (int64_t)by * g.nb0 * 2 * g.slab_stride + (int64_t)(Y - by * g.n1 + 1) * (g.n0 + 2);
 }
 
 // slab offset of field 0 of instance-global cell (X, Y), mirrored into the
@@ -157,16 +201,27 @@ __global__ void __launch_bounds__(256) adjoint_step_kernel(const T* __restrict__
         auto is_tile = [&](int cx, int cy) { return cx >= 2 && cx < 2 + w && cy >= 2 && cy < 2 + h; };
         auto region1 = [&](int cx, int cy) { return cx >= 1 && cx < W2 - 1 && cy >= 1 && cy < H2 - 1; };
 
-        // A. stage x_n on the window, the incoming cotangents on region 1
+        // A. stage x_n on the window, the incoming cotangents on region 1;
+        // the window's column and row offset terms are computed once
+        const int64_t base = (int64_t)inst * g.bpi * 2 * g.slab_stride;
+        if (threadIdx.x < W2) {
+            const int X = X0 - 2 + (int)threadIdx.x;
+            S.col[threadIdx.x] = col_term(g, X);
+            S.cout_[threadIdx.x] = (X < 0 || X >= g.N0) ? 1 : 0;
+        } else if (threadIdx.x < W2 + H2) {
+            const int r = threadIdx.x - W2, Y = Y0 - 2 + r;
+            S.row[r] = row_term(g, Y);
+            S.rout[r] = (Y < 0 || Y >= g.N1) ? 2 : 0;
+        }
+        __syncthreads();
         for (int k = threadIdx.x; k < N; k += blockDim.x) {
             const int cx = k % W2, cy = k / W2;
-            const int X = X0 - 2 + cx, Y = Y0 - 2 + cy;
-            const int ox = (X < 0 || X >= g.N0) ? 1 : 0, oy = (Y < 0 || Y >= g.N1) ? 2 : 0;
-            S.out[k] = (unsigned char)(ox | oy);
-            const int64_t o = cell_offset(g, inst, X, Y);
+            const int fl = S.cout_[cx] | S.rout[cy];
+            S.out[k] = (unsigned char)fl;
+            const int64_t o = base + S.col[cx] + S.row[cy];
             S.ph[k] = x[o];
             S.u[k] = x[o + g.slab_stride];
-            const bool in = (ox | oy) == 0 && region1(cx, cy);
+            const bool in = fl == 0 && region1(cx, cy);
             S.pb[k] = in ? lam_in[o] : T(0);
             S.ub[k] = in ? lam_in[o + g.slab_stride] : T(0);
             S.nb[k] = S.ax[k] = S.ay[k] = S.nu[k] = T(0);
@@ -218,13 +273,14 @@ __global__ void __launch_bounds__(256) adjoint_step_kernel(const T* __restrict__
             const T gp = ph * ph * ph - ph;
             const T Nn = -m.lambda * uc * pp + (flux - gp);
             const T cdx = S.ph[k + 1] - S.ph[k - 1], cdy = S.ph[k + W2] - S.ph[k - W2];
-            const FaceDer<T> c = face_der(T(0.5) * cdx, T(0.5) * cdy, m.c_a_bar, m.c_ae, T(0), m.c_tol);
+            const CentreDer<T> c = centre_der(T(0.5) * cdx, T(0.5) * cdy, m.c_a_bar, m.c_ae, m.c_tol);
             const T A = c.a;
-            const T iq = recip(A * A);
+            const T ia = recip(A);
+            const T iq = ia * ia;
             const T kphi = Nn * iq;
             const T mu = dt * (S.pb[k] + T(0.5) * S.ub[k]);
             const T nbar = mu * iq;
-            const T abar = T(-2) * mu * kphi / A;
+            const T abar = T(-2) * mu * kphi * ia;
             S.nb[k] = nbar;
             S.ax[k] = abar * T(0.5) * c.ax;
             S.ay[k] = abar * T(0.5) * c.ay;
@@ -286,21 +342,26 @@ __global__ void __launch_bounds__(256) adjoint_step_kernel(const T* __restrict__
         }
         __syncthreads();
 
-        // F. fold the ghost positions into their source cells and store
-        for (int k = threadIdx.x; k < N; k += blockDim.x) {
-            const int cx = k % W2, cy = k / W2;
-            if (!is_tile(cx, cy)) continue;
-            T pbar = S.pb[k], ubar = S.ub[k];
-            for (int dy = -1; dy <= 1; ++dy)
-                for (int dx = -1; dx <= 1; ++dx) {
-                    if (dx == 0 && dy == 0) continue;
-                    const int q = k + dx + dy * W2;
-                    if ((dx == 0 || (S.out[q] & 1)) && (dy == 0 || (S.out[q] & 2))) {
-                        pbar += S.pb[q];
-                        ubar += S.ub[q];
+        // F. fold the ghost positions into their source cells (tiles on an
+        // instance edge only) and store
+        const bool edge = X0 == 0 || Y0 == 0 || X0 + w == g.N0 || Y0 + h == g.N1;
+        for (int k = threadIdx.x; k < TW * TH; k += blockDim.x) {
+            const int tx = k % TW, ty = k / TW;
+            if (tx >= w || ty >= h) continue;
+            const int cx = tx + 2, cy = ty + 2, q0 = cx + cy * W2;
+            T pbar = S.pb[q0], ubar = S.ub[q0];
+            if (edge) {
+                for (int dy = -1; dy <= 1; ++dy)
+                    for (int dx = -1; dx <= 1; ++dx) {
+                        if (dx == 0 && dy == 0) continue;
+                        const int q = q0 + dx + dy * W2;
+                        if ((dx == 0 || (S.out[q] & 1)) && (dy == 0 || (S.out[q] & 2))) {
+                            pbar += S.pb[q];
+                            ubar += S.ub[q];
+                        }
                     }
-                }
-            const int64_t o = cell_offset(g, inst, X0 - 2 + cx, Y0 - 2 + cy);
+            }
+            const int64_t o = base + S.col[cx] + S.row[cy];
             lam_out[o] = pbar;
             lam_out[o + g.slab_stride] = ubar;
         }
