@@ -478,10 +478,14 @@ int lg_heat_fe_run(lg_state* st, int field, double kappa, double dt, int64_t nst
     const lg::SlabLayout L = layout_of(st, field);
     char key[256];
     snprintf(key, sizeof key, "heat|f=%d|k=%a|dt=%a", field, kappa, dt);
+    // 3-D: halos pulled from the neighbour blocks, ghosts filled once at the
+    // end; otherwise the push kernel, which keeps the ghosts valid each step
+    const bool pull = lg::heat3d_pull_supported(topo, L);
     auto step = [&]() -> int {
         const double* in = static_cast<const double*>(st->arena[st->cur]);
         double* out = static_cast<double*>(st->arena[st->cur ^ 1]);
-        cudaError_t e = lg::launch_heat_step(in, out, topo, L, field, kappa, dt, inv_h2, ctx->stream);
+        cudaError_t e = pull ? lg::launch_heat3d_pull(in, out, topo, L, field, kappa, dt, inv_h2, ctx->stream)
+                             : lg::launch_heat_step(in, out, topo, L, field, kappa, dt, inv_h2, ctx->stream);
         ctx->launches++;
         if (e != cudaSuccess) return cuda_fail(ctx, e, "heat step launch");
         st->cur ^= 1;
@@ -490,6 +494,10 @@ int lg_heat_fe_run(lg_state* st, int field, double kappa, double dt, int64_t nst
     };
     int rc = run_steps(st, key, nsteps, flags, step);
     if (rc != LG_OK) return rc;
+    if (pull && nsteps > 0) {
+        rc = fill_all_ghosts(st);
+        if (rc != LG_OK) return rc;
+    }
     if (nsteps & 1) {
         // graph replays keep parity; the remainder steps already flipped it
     }

@@ -5,6 +5,7 @@
 // and sum below rounds separately and `fma` appears exactly where the
 // reference calls `f64::mul_add`.  That is what makes the FP64 path
 // bit-identical to the reference's SerialScheduler.
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 
@@ -178,6 +179,82 @@ __global__ void __launch_bounds__(256) heat_step_kernel(const double* __restrict
     }
 }
 
+// asynchronous 8-byte global -> shared copy (completes at cp_async_wait)
+__device__ __forceinline__ void cp_async8(double* smem, const double* gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+// 3-D heat step with halos pulled from the neighbour blocks' interiors
+// (no ghost entries are read or written).  One CTA owns a z-range of ZC
+// planes of one block, threads on the (x, y) plane.  It first stages the
+// range with its one-cell face halo -- the z planes above and below and the
+// x and y rings of every plane -- in shared memory, every load issued before
+// any is used so that the whole range is in flight at once; halo values come
+// from the face-neighbour blocks or, at a mirror boundary, repeat the edge
+// cell (the zero-flux ghost, boundary.rs:63-80).  Then each thread updates
+// its column from shared memory.  Arithmetic and operand order as
+// heat_step_kernel, so the results are bit-identical.
+__global__ void __launch_bounds__(1024) heat3d_pull_kernel(const double* __restrict__ in, double* __restrict__ out,
+                                                           CartTopo topo, SlabLayout L, int field, double kappa,
+                                                           double dt, double ih0, double ih1, double ih2, int zc) {
+    extern __shared__ double stage[];
+    const int n0 = topo.n[0], n1 = topo.n[1], n2 = topo.n[2];
+    const int X2 = n0 + 2, PZ = (n0 + 2) * (n1 + 2);
+    const int x = threadIdx.x, y = threadIdx.y;
+    const int64_t sy = L.gdim[0], sz = (int64_t)L.gdim[0] * L.gdim[1];
+    const int nchunks = (n2 + zc - 1) / zc;
+    const int64_t items = (int64_t)topo.nblocks * nchunks;
+    auto off = [&](int xx, int yy, int zz) { return (int64_t)(xx + 1) + (yy + 1) * sy + (zz + 1) * sz; };
+    for (int64_t item = blockIdx.x; item < items; item += gridDim.x) {
+        const int b = (int)(item / nchunks);
+        const int z0 = (int)(item - (int64_t)b * nchunks) * zc, nz = min(zc, n2 - z0);
+        const int* nb = topo.nbr + b * 6;
+        const double* s = in + slab_base(L, b, field);
+        const double* sxl = nb[0] >= 0 ? in + slab_base(L, nb[0], field) : nullptr;
+        const double* sxr = nb[1] >= 0 ? in + slab_base(L, nb[1], field) : nullptr;
+        const double* syl = nb[2] >= 0 ? in + slab_base(L, nb[2], field) : nullptr;
+        const double* syr = nb[3] >= 0 ? in + slab_base(L, nb[3], field) : nullptr;
+        // plane r of the stage holds block plane z0 - 1 + r; every copy is
+        // issued before any is waited for
+        double* mine = stage + (x + 1) + (y + 1) * X2;
+        for (int r = 0; r < nz + 2; ++r) {
+            const int z = z0 - 1 + r;
+            const double* src;
+            if (z < 0)
+                src = nb[4] >= 0 ? in + slab_base(L, nb[4], field) + off(x, y, n2 - 1) : s + off(x, y, 0);
+            else if (z >= n2)
+                src = nb[5] >= 0 ? in + slab_base(L, nb[5], field) + off(x, y, 0) : s + off(x, y, n2 - 1);
+            else
+                src = s + off(x, y, z);
+            cp_async8(mine + r * PZ, src);
+        }
+        for (int r = 1; r <= nz; ++r) {
+            const int z = z0 - 1 + r;
+            double* pl = stage + r * PZ;
+            if (x == 0) cp_async8(pl + (y + 1) * X2, sxl ? sxl + off(n0 - 1, y, z) : s + off(0, y, z));
+            if (x == n0 - 1) cp_async8(pl + (n0 + 1) + (y + 1) * X2, sxr ? sxr + off(0, y, z) : s + off(n0 - 1, y, z));
+            if (y == 0) cp_async8(pl + x + 1, syl ? syl + off(x, n1 - 1, z) : s + off(x, 0, z));
+            if (y == n1 - 1) cp_async8(pl + (x + 1) + (n1 + 1) * X2, syr ? syr + off(x, 0, z) : s + off(x, n1 - 1, z));
+        }
+        cp_async_wait();
+        __syncthreads();
+        double* o = out + slab_base(L, b, field);
+        for (int r = 1; r <= nz; ++r) {
+            const double* q = mine + r * PZ;
+            const double uc = q[0];
+            double acc = 0.0;
+            acc += ((q[1] - (uc + uc)) + q[-1]) * ih0;
+            acc += ((q[X2] - (uc + uc)) + q[-X2]) * ih1;
+            acc += ((q[PZ] - (uc + uc)) + q[-PZ]) * ih2;
+            const double k = acc * kappa;
+            o[off(x, y, z0 - 1 + r)] = uc + dt * k;
+        }
+        __syncthreads();
+    }
+}
+
 // Reference-order Model C step, one thread per interior cell: the flux
 // kernel (finite_volume.rs:258-283), the local terms (phasefield.rs:395-404),
 // the u Laplacian and coupling (phasefield.rs:412-421), the Time driver
@@ -294,6 +371,37 @@ cudaError_t launch_halo_fill(void* arena, int elem_size, const CartTopo& topo, c
         halo_fill_kernel<double><<<grid, 256, 0, s>>>(static_cast<double*>(arena), topo, L, field, rs);
     else
         halo_fill_kernel<float><<<grid, 256, 0, s>>>(static_cast<float*>(arena), topo, L, field, rs);
+    return cudaGetLastError();
+}
+
+bool heat3d_pull_supported(const CartTopo& topo, const SlabLayout& L) {
+    return topo.D == 3 && L.ghost == 1 && topo.n[0] >= 1 && topo.n[1] >= 1 && topo.n[2] >= 1 &&
+           topo.n[0] * topo.n[1] <= 1024 && 3 * (topo.n[0] + 2) * (topo.n[1] + 2) * 8 <= 96 * 1024;
+}
+
+cudaError_t launch_heat3d_pull(const double* in, double* out, const CartTopo& topo, const SlabLayout& L, int field,
+                               double kappa, double dt, const double inv_h2[3], cudaStream_t s) {
+    // z-chunks per block: whole blocks when there are enough of them to fill
+    // the GPU several times, else chunks of at least 4 planes
+    // planes per CTA: at most 16 (and the stage at most 96 KB), fewer when
+    // whole blocks would not fill the GPU several times over
+    const int n2 = topo.n[2];
+    const int64_t plane = (int64_t)(topo.n[0] + 2) * (topo.n[1] + 2) * sizeof(double);
+    int zc = std::min(n2, 16);
+    while (zc > 1 && (zc + 2) * plane > 96 * 1024) --zc;
+    while (zc > 4 && (int64_t)topo.nblocks * ((n2 + zc - 1) / zc) < 148 * 8) zc = (zc + 1) / 2;
+    const int64_t items = (int64_t)topo.nblocks * ((n2 + zc - 1) / zc);
+    const unsigned grid = (unsigned)std::min<int64_t>(items, (int64_t)1 << 30);
+    const size_t smem = (size_t)(zc + 2) * plane;
+    static bool configured = false;
+    if (!configured) {
+        cudaError_t e = cudaFuncSetAttribute(heat3d_pull_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             96 * 1024 + 2 * 1024);
+        if (e != cudaSuccess) return e;
+        configured = true;
+    }
+    heat3d_pull_kernel<<<grid, dim3(topo.n[0], topo.n[1]), smem, s>>>(in, out, topo, L, field, kappa, dt, inv_h2[0],
+                                                                     inv_h2[1], inv_h2[2], zc);
     return cudaGetLastError();
 }
 

@@ -36,6 +36,14 @@ cudaError_t launch_halo_fill(void* arena, int elem_size, const CartTopo& topo, c
 cudaError_t launch_heat_step(const double* in, double* out, const CartTopo& topo, const SlabLayout& L, int field,
                              double kappa, double dt, const double inv_h2[3], cudaStream_t s);
 
+// (d) the same heat step for 3-D grids of ghost width 1, with every halo
+// value read from the neighbour blocks' interiors: `out` gets interiors only
+// (its ghost entries are left as they were).  Bit-identical to
+// launch_heat_step.  Needs n0 * n1 <= 1024.
+bool heat3d_pull_supported(const CartTopo& topo, const SlabLayout& L);
+cudaError_t launch_heat3d_pull(const double* in, double* out, const CartTopo& topo, const SlabLayout& L, int field,
+                               double kappa, double dt, const double inv_h2[3], cudaStream_t s);
+
 // (a) fused Model C Euler-Maruyama step, FP64, bit-exact to the reference.
 // Reads phi (field 0) and u (field 1) from `in`, writes both to `out` with
 // ghosts filled.  `tdev[slot]` holds the step's time (its bits are the noise
