@@ -123,12 +123,10 @@ cudaError_t launch_modelc_batch_f32(const float* in, float* out, const CartTopo&
                                     const void* params, const uint64_t* seeds, int bpi, double dt, double amp,
                                     double* tdev, int slot, int rows, cudaStream_t s) {
     TileArgs g{topo, L, dt, 0, tdev, slot, rows, 0, 0, 0};
-    g.params = params;
-    g.seeds = seeds;
-    g.bpi = bpi;
+    const BatchArgs bt{params, seeds, bpi};
     const float scale_amp = (float)(std::sqrt(dt) * amp);
-    if (amp != 0.0) return launch_strip_batch<float, OpsFast32, true, 3>(in, out, g, (float)dt, scale_amp, s);
-    return launch_strip_batch<float, OpsFast32, false, 3>(in, out, g, (float)dt, scale_amp, s);
+    if (amp != 0.0) return launch_strip_batch<float, OpsFast32, true, 3>(in, out, g, bt, (float)dt, scale_amp, s);
+    return launch_strip_batch<float, OpsFast32, false, 3>(in, out, g, bt, (float)dt, scale_amp, s);
 }
 
 }  // namespace lg

@@ -52,13 +52,16 @@ struct TileArgs {
     int strips;   // 32-column strips per block
     int chunks;   // row chunks per block
     int64_t units;
-    // batched instances (BATCH kernels): block b belongs to instance
-    // b / bpi, whose parameters are params[instance] (an Ops::Params array
-    // on the device) and whose Wiener seed is seeds[instance]; its noise
-    // keys use the instance-local block index b % bpi
-    const void* params = nullptr;
-    const uint64_t* seeds = nullptr;
-    int bpi = 0;
+};
+
+// Batched instances (BATCH kernels): block b belongs to instance b / bpi,
+// whose parameters are params[instance] (an Ops::Params array on the
+// device) and whose Wiener seed is seeds[instance]; its noise keys use the
+// instance-local block index b % bpi.
+struct BatchArgs {
+    const void* params;
+    const uint64_t* seeds;
+    int bpi;
 };
 
 template <class T>
@@ -123,12 +126,80 @@ __device__ __forceinline__ void strip_row(const typename Ops::Params& m, const T
     }
 }
 
+// One work unit of the strip kernel: the rows [r0, r1) of the 32-column
+// strip at c0 of block b, with the parameter record m (the kernel parameter,
+// or a batched instance's record) and the Wiener key of block key_block.
+template <class T, class Ops, bool NOISE, int NX, bool FULL, int PF>
+__device__ __forceinline__ void strip_unit(const typename Ops::Params& m, uint64_t seed, int key_block,
+                                           const TileArgs& g, const T* __restrict__ ph, const T* __restrict__ uu,
+                                           T* __restrict__ out, T* __restrict__ po, T* __restrict__ uo,
+                                           const Nbr2& nb, int r0, int r1, int lane, int col, bool valid,
+                                           int last_lane, int cr, bool edge_x, int n0, int n1, int sy, double tnow,
+                                           T dt, T scale_amp) {
+    constexpr int NB = PF + 3;
+    uint64_t block_key = 0;
+    if (NOISE)
+        block_key = wiener_block_key(seed, (uint64_t)__double_as_longlong(tnow), kWienerStream0,
+                                     (uint64_t)key_block);
+
+    int off = (col + 1) + (r0 + 1) * sy;  // slab offset of (col, r0)
+    Row3<T> w[NB];
+    T uw[NB];
+    T jb = T(0);
+    // window: rows r0-1 .. r0+PF in w[0..NB-2]; w[NB-1] is filled by the first row
+#pragma unroll
+    for (int q = 0; q < NB - 1; ++q) {
+        w[q] = Row3<T>{};
+        uw[q] = T(0);
+        const int r = r0 - 1 + q;
+        if (valid && r <= n1) {
+            const T* p = ph + off + (q - 1) * sy;
+            w[q] = {__ldg(p - 1), __ldg(p), __ldg(p + 1)};
+            uw[q] = __ldg(uu + off + (q - 1) * sy);
+        }
+    }
+    w[NB - 1] = Row3<T>{};
+    uw[NB - 1] = T(0);
+    // right-boundary face of the strip for rows r0 .. r0+31 (lane = row)
+    T bnd = T(0);
+    {
+        const int r = r0 + lane;
+        if (r < r1) {
+            const T* q = ph + (cr + 1) + (r + 1) * sy;  // (column cr, row r)
+            const T c0m = __ldg(q - sy), c1m = __ldg(q - sy + 1);
+            const T c00 = __ldg(q), c10 = __ldg(q + 1);
+            const T c0p = __ldg(q + sy), c1p = __ldg(q + sy + 1);
+            bnd = Ops::xface(m, c10 - c00, c1p - c1m, c0p, c0m);
+        }
+    }
+    // y face below the first row (between r0-1 and r0)
+    if (valid) jb = Ops::yface(m, w[1].b - w[0].b, w[1].c - w[1].a, w[0].c, w[0].a);
+
+#define LG_ROW(J, Q)                                                                                            \
+    strip_row<T, Ops, NOISE, NX, FULL, PF>(m, g, J, r0, lane, col, valid, last_lane, n0, n1, off, ph, uu, out, po,  \
+                                       uo, nb, edge_x, block_key, bnd, w[(Q) % NB], w[((Q) + 1) % NB],          \
+                                       w[((Q) + 2) % NB], w[((Q) + 2 + PF) % NB], uw[(Q) % NB],                \
+                                       uw[((Q) + 1) % NB], uw[((Q) + 2) % NB], uw[((Q) + 2 + PF) % NB], jb, dt, \
+                                       scale_amp);                                                              \
+    off += sy
+    int j = r0;
+    for (; j + NB <= r1; j += NB) {
+#pragma unroll
+        for (int q = 0; q < NB; ++q) { LG_ROW(j + q, q); }
+    }
+#pragma unroll
+    for (int q = 0; q < NB - 1; ++q) {
+        if (j + q < r1) { LG_ROW(j + q, q); }
+    }
+#undef LG_ROW
+}
+
 // Rows per work unit are at most 32, so one batch of boundary faces (lanes
 // across rows) serves the whole unit.
 template <class T, class Ops, bool NOISE, int MINB, int NX, int PF, bool BATCH = false>
 __global__ void __launch_bounds__(256, MINB)
     modelc_strip_kernel(const T* __restrict__ in, T* __restrict__ out, TileArgs g, typename Ops::Params m0, T dt,
-                        T scale_amp) {
+                        T scale_amp, BatchArgs bt) {
     constexpr bool FULL = NX > 0 && NX % 32 == 0;
     constexpr int NB = PF + 3;  // window rows: j-1, j, j+1 and PF rows of prefetch
     const CartTopo& topo = g.topo;
@@ -165,70 +236,16 @@ __global__ void __launch_bounds__(256, MINB)
         T* uo = out + slab_base(g.L, b, 1);
         Nbr2 nb;
         nb.load(topo, b);
-        typename Ops::Params m = m0;
-        uint64_t seed = g.seed;
-        int key_block = b;
-        if (BATCH) {
-            const int inst = b / g.bpi;
-            m = static_cast<const typename Ops::Params*>(g.params)[inst];
-            seed = g.seeds[inst];
-            key_block = b - inst * g.bpi;
+        if constexpr (BATCH) {
+            const int inst = b / bt.bpi;
+            const typename Ops::Params mi = static_cast<const typename Ops::Params*>(bt.params)[inst];
+            strip_unit<T, Ops, NOISE, NX, FULL, PF>(mi, bt.seeds[inst], b - inst * bt.bpi, g, ph, uu, out, po, uo, nb,
+                                                    r0, r1, lane, col, valid, last_lane, cr, edge_x, n0, n1, sy,
+                                                    tnow, dt, scale_amp);
+        } else {
+            strip_unit<T, Ops, NOISE, NX, FULL, PF>(m0, g.seed, b, g, ph, uu, out, po, uo, nb, r0, r1, lane, col,
+                                                    valid, last_lane, cr, edge_x, n0, n1, sy, tnow, dt, scale_amp);
         }
-        uint64_t block_key = 0;
-        if (NOISE)
-            block_key = wiener_block_key(seed, (uint64_t)__double_as_longlong(tnow), kWienerStream0,
-                                         (uint64_t)key_block);
-
-        int off = (col + 1) + (r0 + 1) * sy;  // slab offset of (col, r0)
-        Row3<T> w[NB];
-        T uw[NB];
-        T jb = T(0);
-        // window: rows r0-1 .. r0+PF in w[0..NB-2]; w[NB-1] is filled by the first row
-#pragma unroll
-        for (int q = 0; q < NB - 1; ++q) {
-            w[q] = Row3<T>{};
-            uw[q] = T(0);
-            const int r = r0 - 1 + q;
-            if (valid && r <= n1) {
-                const T* p = ph + off + (q - 1) * sy;
-                w[q] = {__ldg(p - 1), __ldg(p), __ldg(p + 1)};
-                uw[q] = __ldg(uu + off + (q - 1) * sy);
-            }
-        }
-        w[NB - 1] = Row3<T>{};
-        uw[NB - 1] = T(0);
-        // right-boundary face of the strip for rows r0 .. r0+31 (lane = row)
-        T bnd = T(0);
-        {
-            const int r = r0 + lane;
-            if (r < r1) {
-                const T* q = ph + (cr + 1) + (r + 1) * sy;  // (column cr, row r)
-                const T c0m = __ldg(q - sy), c1m = __ldg(q - sy + 1);
-                const T c00 = __ldg(q), c10 = __ldg(q + 1);
-                const T c0p = __ldg(q + sy), c1p = __ldg(q + sy + 1);
-                bnd = Ops::xface(m, c10 - c00, c1p - c1m, c0p, c0m);
-            }
-        }
-        // y face below the first row (between r0-1 and r0)
-        if (valid) jb = Ops::yface(m, w[1].b - w[0].b, w[1].c - w[1].a, w[0].c, w[0].a);
-
-#define LG_ROW(J, Q)                                                                                            \
-    strip_row<T, Ops, NOISE, NX, FULL, PF>(m, g, J, r0, lane, col, valid, last_lane, n0, n1, off, ph, uu, out, po,  \
-                                           uo, nb, edge_x, block_key, bnd, w[(Q) % NB], w[((Q) + 1) % NB],          \
-                                           w[((Q) + 2) % NB], w[((Q) + 2 + PF) % NB], uw[(Q) % NB],                \
-                                           uw[((Q) + 1) % NB], uw[((Q) + 2) % NB], uw[((Q) + 2 + PF) % NB], jb, dt, \
-                                           scale_amp);                                                              \
-    off += sy
-        int j = r0;
-        for (; j + NB <= r1; j += NB) {
-#pragma unroll
-            for (int q = 0; q < NB; ++q) { LG_ROW(j + q, q); }
-        }
-#pragma unroll
-        for (int q = 0; q < NB - 1; ++q) {
-            if (j + q < r1) { LG_ROW(j + q, q); }
-        }
-#undef LG_ROW
     }
 }
 
@@ -261,13 +278,13 @@ inline dim3 strip_grid(TileArgs& g) {
 // batched instances: block widths 64 (the ensemble configuration) and 32
 // get a compile-time row stride
 template <class T, class Ops, bool NOISE, int MINB>
-cudaError_t launch_strip_batch(const T* in, T* out, TileArgs g, T dt, T scale_amp, cudaStream_t s) {
+cudaError_t launch_strip_batch(const T* in, T* out, TileArgs g, BatchArgs bt, T dt, T scale_amp, cudaStream_t s) {
     const dim3 grid = strip_grid(g), block(256);
     const typename Ops::Params m{};
     switch (g.topo.n[0]) {
-        case 32: modelc_strip_kernel<T, Ops, NOISE, MINB, 32, 1, true><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp); break;
-        case 64: modelc_strip_kernel<T, Ops, NOISE, MINB, 64, 1, true><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp); break;
-        default: modelc_strip_kernel<T, Ops, NOISE, MINB, 0, 1, true><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp);
+        case 32: modelc_strip_kernel<T, Ops, NOISE, MINB, 32, 1, true><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp, bt); break;
+        case 64: modelc_strip_kernel<T, Ops, NOISE, MINB, 64, 1, true><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp, bt); break;
+        default: modelc_strip_kernel<T, Ops, NOISE, MINB, 0, 1, true><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp, bt);
     }
     return cudaGetLastError();
 }
@@ -284,12 +301,12 @@ cudaError_t launch_strip_minb(const T* in, T* out, TileArgs g, const typename Op
     const int64_t ctas = std::min<int64_t>((g.units + wpc - 1) / wpc, (int64_t)1 << 30);
     const dim3 grid((unsigned)ctas), block(wpc * 32);
     switch (n0) {  // block widths of the shipped configurations get a compile-time row stride
-        case 32: modelc_strip_kernel<T, Ops, NOISE, MINB, 32, PF><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp); break;
-        case 64: modelc_strip_kernel<T, Ops, NOISE, MINB, 64, PF><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp); break;
-        case 126: modelc_strip_kernel<T, Ops, NOISE, MINB, 126, PF><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp); break;
-        case 128: modelc_strip_kernel<T, Ops, NOISE, MINB, 128, PF><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp); break;
-        case 256: modelc_strip_kernel<T, Ops, NOISE, MINB, 256, PF><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp); break;
-        default: modelc_strip_kernel<T, Ops, NOISE, MINB, 0, PF><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp);
+        case 32: modelc_strip_kernel<T, Ops, NOISE, MINB, 32, PF><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp, BatchArgs{}); break;
+        case 64: modelc_strip_kernel<T, Ops, NOISE, MINB, 64, PF><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp, BatchArgs{}); break;
+        case 126: modelc_strip_kernel<T, Ops, NOISE, MINB, 126, PF><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp, BatchArgs{}); break;
+        case 128: modelc_strip_kernel<T, Ops, NOISE, MINB, 128, PF><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp, BatchArgs{}); break;
+        case 256: modelc_strip_kernel<T, Ops, NOISE, MINB, 256, PF><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp, BatchArgs{}); break;
+        default: modelc_strip_kernel<T, Ops, NOISE, MINB, 0, PF><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp, BatchArgs{});
     }
     return cudaGetLastError();
 }
