@@ -142,6 +142,16 @@ typedef struct lg_modelc_params {
  * (0 = library default). */
 int lg_modelc_em_run(lg_state* st, const lg_modelc_params* p, double dt, uint64_t seed, int64_t nsteps,
                      int variant, uint32_t flags);
+/* Autotuner of the fused Model C step: times every strip-kernel variant
+ * (2, 3 or 4 CTAs per SM by register budget x strip heights chosen by the
+ * library, 8, 16 or 32 rows) for `trial_steps` steps from a copy of the
+ * state, restores the state, its time and step index, and remembers the
+ * fastest for this context, block shape, block count, element type and noise
+ * setting: lg_modelc_em_run with variant 0 then uses it.  Returns it in
+ * *best_variant and its time per step in *best_ms (if non-null).  No
+ * counterpart in the reference, whose block size is the user's only knob. */
+int lg_modelc_autotune(lg_state* st, const lg_modelc_params* p, double dt, uint64_t seed, int trial_steps,
+                       int* best_variant, double* best_ms);
 
 /* Initial conditions, computed on the host exactly as the reference does and
  * uploaded.  `ModelC::initialize_grains` without orientations

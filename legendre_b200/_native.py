@@ -107,6 +107,7 @@ _SIGS = {
     "lg_fill_ghosts": (C.c_int, [_p, C.c_int]),
     "lg_heat_fe_run": (C.c_int, [_p, C.c_int, _d, _d, _i64, C.c_uint32]),
     "lg_modelc_em_run": (C.c_int, [_p, C.POINTER(ModelCParams), _d, _u64, _i64, C.c_int, C.c_uint32]),
+    "lg_modelc_autotune": (C.c_int, [_p, C.POINTER(ModelCParams), _d, _u64, C.c_int, C.POINTER(C.c_int), _pd]),
     "lg_modelc_initialize_grains": (C.c_int, [_p, _pd, _i64, _d]),
     "lg_heat_initialize_sine_noise": (C.c_int, [_p, C.c_int, _u64, _d]),
     "lg_standard_normal": (C.c_int, [_p, C.POINTER(C.c_uint64), _i64, _pd]),

@@ -249,3 +249,20 @@ class Simulation:
 
     def run(self, dt: float, nsteps: int, graph: bool = False, variant: int = 0) -> None:
         self.integrator.run(self, float(dt), int(nsteps), graph=graph, variant=variant)
+
+    def autotune(self, dt: float, trial_steps: int = 20):
+        """Pick the fastest Model C step variant for this grid and precision by
+        timing every candidate from a copy of the state (the state, its time
+        and step index are left as they were); later ``run`` calls with the
+        default variant use it.  Returns (variant, ms per step)."""
+        from .integrators import EulerMaruyama
+        from .physics import ModelC
+
+        if not isinstance(self.model, ModelC):
+            raise TypeError("the autotuner covers the Model C step")
+        seed = self.integrator.seed if isinstance(self.integrator, EulerMaruyama) else 0
+        p = self.model.params(flux_tol=self.disc.tol)
+        v, ms = C.c_int(), C.c_double()
+        N.check(N.lib.lg_modelc_autotune(self.state.handle, C.byref(p), float(dt), int(seed) & ((1 << 64) - 1),
+                                         int(trial_steps), C.byref(v), C.byref(ms)), self.scheduler.handle)
+        return v.value, ms.value

@@ -21,6 +21,7 @@ struct lg_ctx {
     bool own_stream = false;
     std::string err;
     int64_t launches = 0;
+    std::map<std::string, int> tuned;  // Model C variant chosen by lg_modelc_autotune, per shape
 };
 
 struct lg_grid {
@@ -181,6 +182,14 @@ int run_steps(lg_state* st, const std::string& key, int64_t nsteps, uint32_t fla
         if (rc != LG_OK) return rc;
     }
     return LG_OK;
+}
+
+// the autotuner's cache key: the grid's block shape and count, the element
+// type and whether the noise term is on
+std::string tune_key(const lg_state* st, bool noise) {
+    const lg_grid* g = st->grid;
+    return std::to_string(g->D) + "|" + std::to_string(g->block[0]) + "x" + std::to_string(g->block[1]) + "|" +
+           std::to_string(g->nblocks) + "|" + std::to_string(st->dtype) + "|" + (noise ? "n" : "q");
 }
 
 // Host-side time bookkeeping of `steps` steps: t += dt each
@@ -539,6 +548,10 @@ int lg_modelc_em_run(lg_state* st, const lg_modelc_params* p, double dt, uint64_
     LG_CUDA(ctx, cudaMemcpyAsync(st->d_t + st->tslot, &st->t, sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
     const lg::CartTopo topo = topo_of(st->grid);
     const lg::SlabLayout L = layout_of(st, 0);
+    if (variant == 0) {  // the autotuned choice for this shape, if any
+        auto it = ctx->tuned.find(tune_key(st, nz.on != 0));
+        if (it != ctx->tuned.end()) variant = it->second;
+    }
     char key[512];
     snprintf(key, sizeof key, "modelc|%a|%a|%a|%a|%a|%a|dt=%a|seed=%llu|v=%d", p->eps4, p->lambda, p->d_thermal,
              p->noise_amplitude, p->anisotropy_tol, p->flux_tol, dt, (unsigned long long)seed, variant);
@@ -572,6 +585,80 @@ int lg_modelc_em_run(lg_state* st, const lg_modelc_params* p, double dt, uint64_
     int rc = run_steps(st, key, nsteps, flags, step);
     if (rc != LG_OK) return rc;
     advance_time(st, dt, nsteps);
+    return LG_OK;
+}
+
+int lg_modelc_autotune(lg_state* st, const lg_modelc_params* p, double dt, uint64_t seed, int trial_steps,
+                       int* best_variant, double* best_ms) {
+    if (!st || !p || !best_variant || trial_steps < 1) return LG_ERR_INVALID;
+    lg_ctx* ctx = st->ctx;
+    if (st->grid->D != 2) return fail(ctx, LG_ERR_STATE, "the Model C autotuner needs a 2-D state");
+    cudaSetDevice(ctx->device);
+    if (!st->ghosts_valid) {
+        int rc = fill_all_ghosts(st);
+        if (rc != LG_OK) return rc;
+    }
+    // every candidate starts from a copy of the current state; the state,
+    // its time and its step index are restored afterwards
+    const size_t bytes = (size_t)st->grid->nblocks * st->nfields * st->slab_stride * st->esize;
+    void* saved = nullptr;
+    LG_CUDA(ctx, cudaMalloc(&saved, bytes));
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    const int cur0 = st->cur, slot0 = st->tslot;
+    const double t0 = st->t;
+    const int64_t k0 = st->step_index;
+    int rc = LG_OK;
+    cudaError_t ce = cudaMemcpyAsync(saved, st->arena[cur0], bytes, cudaMemcpyDeviceToDevice, ctx->stream);
+    if (ce != cudaSuccess) rc = cuda_fail(ctx, ce, "autotune state copy");
+    const std::string key = tune_key(st, p->noise_amplitude != 0.0);
+    ctx->tuned.erase(key);
+    int best = 0;
+    float best_t = 0.0f;
+    for (int kind : {2, 3, 4}) {
+        for (int rows : {0, 8, 16, 32}) {
+            if (rc != LG_OK) break;
+            const int v = kind + 1000 * rows;
+            ce = cudaMemcpyAsync(st->arena[cur0], saved, bytes, cudaMemcpyDeviceToDevice, ctx->stream);
+            if (ce != cudaSuccess) {
+                rc = cuda_fail(ctx, ce, "autotune state copy");
+                break;
+            }
+            st->cur = cur0;
+            st->tslot = slot0;
+            st->t = t0;
+            rc = lg_modelc_em_run(st, p, dt, seed, 2, v, 0);  // warm-up
+            if (rc != LG_OK) break;
+            cudaEventRecord(e0, ctx->stream);
+            rc = lg_modelc_em_run(st, p, dt, seed, trial_steps, v, 0);
+            cudaEventRecord(e1, ctx->stream);
+            if (rc != LG_OK) break;
+            cudaEventSynchronize(e1);
+            float ms = 0.0f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            if (best == 0 || ms < best_t) {
+                best = v;
+                best_t = ms;
+            }
+        }
+    }
+    if (rc == LG_OK) {
+        ce = cudaMemcpyAsync(st->arena[cur0], saved, bytes, cudaMemcpyDeviceToDevice, ctx->stream);
+        if (ce == cudaSuccess) ce = cudaStreamSynchronize(ctx->stream);
+        if (ce != cudaSuccess) rc = cuda_fail(ctx, ce, "autotune state restore");
+    }
+    cudaFree(saved);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    st->cur = cur0;
+    st->tslot = slot0;
+    st->t = t0;
+    st->step_index = k0;
+    if (rc != LG_OK) return rc;
+    ctx->tuned[key] = best;
+    *best_variant = best;
+    if (best_ms) *best_ms = best_t / trial_steps;
     return LG_OK;
 }
 

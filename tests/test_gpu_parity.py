@@ -262,3 +262,23 @@ def test_modelc_fp32_noisy_tracks_fp64_oracle(sched, orc):
     ref = os_.interior(0)
     assert np.sqrt(np.mean((phi - ref) ** 2)) < 1e-4
     assert np.max(np.abs(phi - ref)) < 2e-3
+
+
+@pytest.mark.parametrize("dtype", ["f64", "f32"])
+def test_autotune_restores_the_state_and_keeps_the_results(sched, orc, dtype):
+    # the tuner times every variant from a copy of the state and puts it back;
+    # runs with the chosen variant give the oracle's bits (FP64, no noise)
+    sim, os_, _ = _modelc_pair(sched, orc, [96, 64], [32, 32], [(10.0, 12.0, 4.0)], 0.0, 10, dtype=dtype)
+    before = [sim.state.download(f).copy() for f in ("phi", "u")]
+    t0, k0 = sim.time(), sim.step_index()
+    dt = sim.model.stable_dt(sim.grid.spacing)
+    variant, ms = sim.autotune(dt, trial_steps=5)
+    assert variant % 1000 in (2, 3, 4) and ms > 0.0
+    for f, b in zip(("phi", "u"), before):
+        assert np.array_equal(sim.state.download(f), b)
+    assert sim.time() == t0 and sim.step_index() == k0
+    if dtype == "f64":
+        sim.run(dt, 30, graph=True)
+        os_.modelc_run(orc.modelc_params(eps4=0.06, lam=3.19, noise=0.0), t0, dt, 7, 30, wiener=True, threads=4)
+        assert np.array_equal(sim.state.interior("phi"), os_.interior(0))
+        assert np.array_equal(sim.state.interior("u"), os_.interior(1))
