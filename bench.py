@@ -61,6 +61,22 @@ CONFIGS = {
 
 BYTES_PER_CELL = {"f64": 32, "f32": 16}  # read phi, u; write phi, u
 
+# DRAM bytes (read + write) per cell-update of the dominant kernel, from one
+# ncu capture each (profiles/): the strip kernel on 4096^2 (FP64 513 MB and
+# FP32 226 MB per 16.8M-cell launch) and the 3-D heat kernel on 256^3 (319 MB
+# per 16.8M cells; the 512^3 run has the same per-block work, so its traffic
+# scales with the cell count).  Other workloads report null.
+TRAFFIC_PER_CELL = {("c2", "f64"): 513.4e6 / 4096 ** 2, ("c2", "f32"): 226.3e6 / 4096 ** 2,
+                    ("c1big", "f64"): 318.7e6 / 256 ** 3}
+
+
+def traffic(args, cells_per_step):
+    """Measured DRAM bytes per launch of the dominant kernel, or None."""
+    if args.cells is not None or args.variant not in (0, 32002):
+        return None
+    per = TRAFFIC_PER_CELL.get((args.config, args.dtype))
+    return None if per is None else per * cells_per_step
+
 
 def peaks():
     p = ROOT / "MEASURED_PEAKS.json"
@@ -175,6 +191,54 @@ def initialize(sim, grid, model, grains, cfg, dtype, sched):
     for f in ("phi", "u"):
         sim.state.upload(f, tmp.download(f).astype(np.float32))
     tmp._destroy()
+
+
+def to_global(blocks, n, b):
+    """(num_blocks, b, b) block-major interiors -> (n, n), row-major."""
+    nb = n // b
+    return blocks.reshape(nb, nb, b, b).transpose(0, 2, 1, 3).reshape(n, n)
+
+
+def tip_position(phi, row, x0, h):
+    """x of the last zero crossing of phi along `row` to the right of x0
+    (linear interpolation between cell centres): the +x dendrite tip."""
+    line = phi[row]
+    i = int(x0 / h)
+    while i + 1 < line.size and line[i + 1] > 0.0:
+        i += 1
+    if i + 1 >= line.size or line[i] <= 0.0:
+        return float("nan")
+    return ((i + 0.5) + line[i] / (line[i] - line[i + 1])) * h
+
+
+def fp32_error(cfg, sched, steps):
+    """The FP32 path against the FP64 path (bit-identical to the CPU
+    oracle) from the same initial state and noise keys: phi L2 (RMS) and
+    L-inf after `steps` steps, solid fractions (phi > 0), and the +x tip
+    velocity of the grain nearest the domain centre over the second half."""
+    import numpy as np
+
+    n, b, h = cfg["cells"], cfg["block"], cfg["h"]
+    out = {}
+    for dtype in ("f64", "f32"):
+        sim, grid, model, grains = make_sim(cfg, dtype, sched)
+        initialize(sim, grid, model, grains, cfg, dtype, sched)
+        c = min(grains, key=lambda g: (g.center[0] - n * h / 2) ** 2 + (g.center[1] - n * h / 2) ** 2)
+        row = int(c.center[1] / h)
+        sim.run(cfg["dt"], steps // 2, graph=True)
+        p1 = to_global(sim.state.interior("phi").astype(np.float64), n, b)
+        sim.run(cfg["dt"], steps - steps // 2, graph=True)
+        p2 = to_global(sim.state.interior("phi").astype(np.float64), n, b)
+        v = (tip_position(p2, row, c.center[0], h) - tip_position(p1, row, c.center[0], h)) / (
+            (steps - steps // 2) * cfg["dt"])
+        out[dtype] = (p2, v, float(np.mean(p2 > 0.0)))
+        del sim
+    d = out["f32"][0] - out["f64"][0]
+    return {"steps": steps, "phi_l2": float(np.sqrt(np.mean(d * d))), "phi_linf": float(np.max(np.abs(d))),
+            "solid_fraction_f64": out["f64"][2], "solid_fraction_f32": out["f32"][2],
+            "tip_velocity_f64": out["f64"][1], "tip_velocity_f32": out["f32"][1],
+            "tip_velocity_rel_err": abs(out["f32"][1] - out["f64"][1]) / abs(out["f64"][1]),
+            "reference": "the FP64 path, bit-identical to the CPU oracle, from the same state and noise keys"}
 
 
 def cpu_oracle_rate(cfg, steps_budget_s: float, max_steps: int):
@@ -314,8 +378,8 @@ def run_other(args, cfg):
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": dict({"workload": cfg["workload"], "parallelism": f"replicas{world}", "graph": True}, **extra),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
-                         "algorithmic_bytes_per_cell": bytes_per_cell},
+                         "frac": achieved / peak, "traffic": traffic(args, cells) if cfg["kind"] == "heat" else None,
+                         "peak_kind": peak_kind, "algorithmic_bytes_per_cell": bytes_per_cell},
             "cpu_baseline": None, "e2e": None,
             "gpu_launches": sched.kernel_launches - launches0,
             "clocks": {"sm_mhz": clk["sm_mhz"], "sm_max_mhz": clk["sm_max_mhz"], "reasons": clk["reasons"],
@@ -495,12 +559,20 @@ def main():
     ap.add_argument("--variant", type=int, default=0)
     ap.add_argument("--noise", type=float, default=None, help="override the noise amplitude b")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cells", type=int, default=None, help="override the grid's cells per dimension (small cases)")
+    ap.add_argument("--instances", type=int, default=None, help="override the ensemble's instance count")
     args = ap.parse_args()
     args.dtype_given = any(a == "--dtype" or a.startswith("--dtype=") for a in sys.argv[1:])
     args.warmup = max(args.warmup, 3)
     cfg = dict(CONFIGS[args.config])
     if args.noise is not None:
         cfg["noise"] = args.noise
+    if args.cells is not None:
+        cfg["cells"] = args.cells
+        cfg["workload"] += f"_cells{args.cells}"
+    if args.instances is not None:
+        cfg["instances"] = args.instances
+        cfg["workload"] += f"_inst{args.instances}"
     if args.impl == "reference":
         run_reference(args, cfg)
         return
@@ -588,6 +660,9 @@ def main():
         peak, peak_kind = peaks()
         algo = BYTES_PER_CELL[args.dtype] * cells
         achieved = algo / (ms_per_step / 1e3) / 1e9
+        err = None
+        if args.dtype == "f32" and world == 1:
+            err = fp32_error(cfg, sched, min(args.steps, cfg["full_steps"]))
         cpu = None
         if not args.no_cpu_baseline and world == 1:
             rate, steps_run, threads = cpu_oracle_rate(cfg, steps_budget_s=15.0, max_steps=1000)
@@ -603,10 +678,11 @@ def main():
                        "l2": "state 2 fields x 2 buffers larger than L2; no flush",
                        "graph": True, "variant": args.variant, "autotuned_variant": tuned},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
+                         "frac": achieved / peak, "traffic": traffic(args, cells), "peak_kind": peak_kind,
                          "algorithmic_bytes_per_cell": BYTES_PER_CELL[args.dtype]},
             "cpu_baseline": cpu,
             "e2e": e2e,
+            "fp32_error": err,
             "gpu_launches": launches,
             "clocks": {"sm_mhz": clk["sm_mhz"], "sm_max_mhz": clk["sm_max_mhz"], "reasons": clk["reasons"],
                        "samples": clk["samples"]},
