@@ -264,9 +264,20 @@ __device__ __forceinline__ void modelc_tile(const TileArgs& a, const lg::MC<doub
     __syncthreads();
 }
 
+// Programmatic dependent launch: a step of the subcycling chain lets the
+// next launch start as soon as every CTA of this one is running, and waits
+// for its predecessor's completion (and memory) only before it reads data a
+// predecessor writes; table loads (tile descriptors, ghost and restriction
+// ops) are read-only and may precede the wait.  Without the launch
+// attribute both instructions are no-ops.
+__device__ __forceinline__ void pdl_release() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 template <bool NOISE>
 __global__ void __launch_bounds__(256) amr_modelc_tiles(TileArgs a, lg::MC<double> m) {
     __shared__ double sp[kWin * kWin], su[kWin * kWin];
+    pdl_release();
+    pdl_wait();
     const double t0 = a.tdev[a.slot];
     if (a.write_t && blockIdx.x == 0 && threadIdx.x == 0) a.tdev[a.slot ^ 1] = t0 + a.dt0;
     const double t = NOISE ? chain_time(t0, a.chain) : 0.0;
@@ -294,6 +305,8 @@ __device__ __forceinline__ void heat_tile(const TileArgs& a, double kappa, doubl
 
 __global__ void __launch_bounds__(256) amr_heat_tiles(TileArgs a, double kappa, double ih0, double ih1) {
     __shared__ double sp[kWin * kWin];
+    pdl_release();
+    pdl_wait();
     const double t0 = a.tdev[a.slot];
     if (a.write_t && blockIdx.x == 0 && threadIdx.x == 0) a.tdev[a.slot ^ 1] = t0 + a.dt0;
     for (int64_t ti = blockIdx.x; ti < a.ntiles; ti += gridDim.x) heat_tile(a, kappa, ih0, ih1, a.tiles[ti], sp);
@@ -316,7 +329,25 @@ __device__ __forceinline__ void restrict_ops(double* C, const double* F, const R
 
 __global__ void amr_restrict_kernel(double* C, const double* F, const RestrictOp* __restrict__ ops, int64_t nops,
                                     int r, double inv, int f0, int f1) {
+    pdl_release();
+    pdl_wait();
     restrict_ops(C, F, ops, nops, r, inv, f0, f1);
+}
+
+// launch with the programmatic-dependent-launch attribute (see pdl_release)
+template <class... KArgs, class... Args>
+cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, cudaStream_t st, Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, args...);
 }
 
 // ------------------------------------------------- persistent coarse step --
@@ -760,8 +791,9 @@ int launch_restrict(lg_amr_sim* s, int fine, int f0, int f1) {
     if (b == a) return LG_OK;
     const int r = (int)s->layout.ratios[fine - 1];
     const double inv = 1.0 / ((double)r * (double)r);
-    amr_restrict_kernel<<<grid_for(b - a, 256), 256, 0, lg::abi_stream(s->ctx)>>>(
-        s->arena[s->cur[fine - 1]], s->arena[s->cur[fine]], s->tab.restrict_ops + a, b - a, r, inv, f0, f1);
+    AMR_CUDA(s, launch_pdl(amr_restrict_kernel, dim3(grid_for(b - a, 256)), dim3(256), lg::abi_stream(s->ctx),
+                           s->arena[s->cur[fine - 1]], (const double*)s->arena[s->cur[fine]],
+                           (const RestrictOp*)(s->tab.restrict_ops + a), (int64_t)(b - a), r, inv, f0, f1));
     lg::abi_count_launch(s->ctx, 1);
     AMR_CUDA(s, cudaGetLastError());
     return LG_OK;
@@ -819,12 +851,13 @@ int launch_level(lg_amr_sim* s, int level, bool interp, double alpha, double dt,
     cudaStream_t st = lg::abi_stream(s->ctx);
     if (s->model == LG_MODEL_C) {
         if (s->mp.noise_amplitude != 0.0)
-            amr_modelc_tiles<true><<<g, threads, 0, st>>>(a, level_mc(s, level));
+            AMR_CUDA(s, launch_pdl(amr_modelc_tiles<true>, dim3(g), dim3(threads), st, a, level_mc(s, level)));
         else
-            amr_modelc_tiles<false><<<g, threads, 0, st>>>(a, level_mc(s, level));
+            AMR_CUDA(s, launch_pdl(amr_modelc_tiles<false>, dim3(g), dim3(threads), st, a, level_mc(s, level)));
     } else {
         const auto& h = s->layout.level_spacing[level];
-        amr_heat_tiles<<<g, threads, 0, st>>>(a, s->kappa, 1.0 / (h[0] * h[0]), 1.0 / (h[1] * h[1]));
+        AMR_CUDA(s, launch_pdl(amr_heat_tiles, dim3(g), dim3(threads), st, a, s->kappa, 1.0 / (h[0] * h[0]),
+                               1.0 / (h[1] * h[1])));
     }
     lg::abi_count_launch(s->ctx, 1);
     AMR_CUDA(s, cudaGetLastError());
