@@ -200,6 +200,10 @@ __global__ void __launch_bounds__(1024) heat3d_pull_kernel(const double* __restr
                                                            CartTopo topo, SlabLayout L, int field, double kappa,
                                                            double dt, double ih0, double ih1, double ih2, int zc) {
     extern __shared__ double stage[];
+    // programmatic dependent launch: the next step may launch now; this one
+    // waits for the previous step's grid (and its writes) before staging
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    asm volatile("griddepcontrol.wait;" ::: "memory");
     const int n0 = topo.n[0], n1 = topo.n[1], n2 = topo.n[2];
     const int X2 = n0 + 2, PZ = (n0 + 2) * (n1 + 2);
     const int x = threadIdx.x, y = threadIdx.y;
@@ -400,9 +404,18 @@ cudaError_t launch_heat3d_pull(const double* in, double* out, const CartTopo& to
         if (e != cudaSuccess) return e;
         configured = true;
     }
-    heat3d_pull_kernel<<<grid, dim3(topo.n[0], topo.n[1]), smem, s>>>(in, out, topo, L, field, kappa, dt, inv_h2[0],
-                                                                     inv_h2[1], inv_h2[2], zc);
-    return cudaGetLastError();
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(topo.n[0], topo.n[1]);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, heat3d_pull_kernel, in, out, topo, L, field, kappa, dt, inv_h2[0], inv_h2[1],
+                              inv_h2[2], zc);
 }
 
 cudaError_t launch_heat_step(const double* in, double* out, const CartTopo& topo, const SlabLayout& L, int field,
