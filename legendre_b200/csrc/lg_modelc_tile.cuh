@@ -77,8 +77,9 @@ constexpr unsigned kFull = 0xffffffffu;
 // receive the prefetch of row j+1+PF.  `off` is the slab offset of (col, j); ph/uu/po/uo
 // are the warp's slab bases.  NX > 0 fixes the block width (and the row
 // stride) at compile time; FULL means every lane owns a column.
-template <class T, class Ops, bool NOISE, int NX, bool FULL, int PF>
-__device__ __forceinline__ void strip_row(const typename Ops::Params& m, const TileArgs& g, int j, int r0, int lane,
+template <class T, class Ops, bool NOISE, int NX, bool FULL, int PF, bool TAIL>
+__device__ __forceinline__ void strip_row(const typename Ops::Params& m, const TileArgs& g, int j, int r0, int r1,
+                                          int lane,
                                           int col, bool valid, int last_lane, int n0, int n1, int off,
                                           const T* __restrict__ ph, const T* __restrict__ uu, T* __restrict__ out,
                                           T* __restrict__ po, T* __restrict__ uo, const Nbr2& nb, bool edge_x,
@@ -86,50 +87,53 @@ __device__ __forceinline__ void strip_row(const typename Ops::Params& m, const T
                                           const Row3<T>& C, Row3<T>& P, T UA, T UB, T UC, T& UP, T& jb, T dt,
                                           T scale_amp) {
     const int sy = NX > 0 ? NX + 2 : g.L.gdim[0];
-    const bool ok = FULL || valid;
+    // lanes past the block's last column (valid false) run the same code on
+    // a clamped column and only skip the stores: no branch splits the face,
+    // noise and cell arithmetic.  Unit heights are whole groups of NB rows,
+    // so the row loop has no separately unrolled tail; only blocks of fewer
+    // than NB rows (TAIL) run rows past the unit's end, without stores.
+    const bool live = !TAIL || j < r1;
+    const bool ok = (FULL || valid) && live;
+    if (j + 1 + PF <= n1) {
+        const T* q = ph + off + (1 + PF) * sy;
+        P.a = __ldg(q - 1);
+        P.b = __ldg(q);
+        P.c = __ldg(q + 1);
+        UP = __ldg(uu + off + (1 + PF) * sy);
+    }
     T ul = T(0), ur = T(0);
-    if (ok) {
-        if (j + 1 + PF <= n1) {
-            const T* q = ph + off + (1 + PF) * sy;
-            P.a = __ldg(q - 1);
-            P.b = __ldg(q);
-            P.c = __ldg(q + 1);
-            UP = __ldg(uu + off + (1 + PF) * sy);
-        }
+    if (live) {
         ul = __ldg(uu + off - 1);
         ur = __ldg(uu + off + 1);
     }
     T nval = T(0);
-    if (NOISE && ok) nval = Ops::noise(splitmix64(block_key ^ (uint64_t)(col + j * n0)));
-    T fl = T(0), jt = T(0);
-    if (ok) {
-        fl = Ops::xface(m, B.b - B.a, C.b - A.b, C.a, A.a);
-        jt = Ops::yface(m, C.b - B.b, C.c - C.a, B.c, B.a);
-    }
+    if (NOISE) nval = Ops::noise(splitmix64(block_key ^ (uint64_t)(col + j * n0)));
+    const T fl = Ops::xface(m, B.b - B.a, C.b - A.b, C.a, A.a);
+    const T jt = Ops::yface(m, C.b - B.b, C.c - C.a, B.c, B.a);
     // right face: the next lane's left face, or the strip's boundary face of this row
     T fr = __shfl_down_sync(kFull, fl, 1);
     const T fb = __shfl_sync(kFull, bnd, (j - r0) & 31);
     if (lane == last_lane) fr = fb;
+    T kphi, ku;
+    Ops::cell(m, fr, fl, jt, jb, B.b, B.c - B.a, C.b - A.b, UB, ul, ur, UC, UA, kphi, ku);
+    T phin = Ops::axpy(dt, kphi, B.b);
+    if (NOISE) phin = Ops::add_noise(phin, scale_amp, nval);
+    const T un = Ops::axpy(dt, ku, UB);
     if (ok) {
-        T kphi, ku;
-        Ops::cell(m, fr, fl, jt, jb, B.b, B.c - B.a, C.b - A.b, UB, ul, ur, UC, UA, kphi, ku);
-        T phin = Ops::axpy(dt, kphi, B.b);
-        if (NOISE) phin = Ops::add_noise(phin, scale_amp, nval);
-        const T un = Ops::axpy(dt, ku, UB);
         po[off] = phin;
         uo[off] = un;
         if (edge_x || j == 0 || j == n1 - 1) {  // warp-uniform: only warps on a block edge push ghosts
             push_ghosts_2d_g1(out, g.L, 0, nb, n0, n1, col, j, phin);
             push_ghosts_2d_g1(out, g.L, 1, nb, n0, n1, col, j, un);
         }
-        jb = jt;
     }
+    jb = jt;
 }
 
 // One work unit of the strip kernel: the rows [r0, r1) of the 32-column
 // strip at c0 of block b, with the parameter record m (the kernel parameter,
 // or a batched instance's record) and the Wiener key of block key_block.
-template <class T, class Ops, bool NOISE, int NX, bool FULL, int PF>
+template <class T, class Ops, bool NOISE, int NX, bool FULL, int PF, bool TAIL>
 __device__ __forceinline__ void strip_unit(const typename Ops::Params& m, uint64_t seed, int key_block,
                                            const TileArgs& g, const T* __restrict__ ph, const T* __restrict__ uu,
                                            T* __restrict__ out, T* __restrict__ po, T* __restrict__ uo,
@@ -142,7 +146,8 @@ __device__ __forceinline__ void strip_unit(const typename Ops::Params& m, uint64
         block_key = wiener_block_key(seed, (uint64_t)__double_as_longlong(tnow), kWienerStream0,
                                      (uint64_t)key_block);
 
-    int off = (col + 1) + (r0 + 1) * sy;  // slab offset of (col, r0)
+    // slab offset of (col, r0); a lane past the last column reads the last one
+    int off = ((FULL ? col : min(col, n0 - 1)) + 1) + (r0 + 1) * sy;
     Row3<T> w[NB];
     T uw[NB];
     T jb = T(0);
@@ -152,7 +157,7 @@ __device__ __forceinline__ void strip_unit(const typename Ops::Params& m, uint64
         w[q] = Row3<T>{};
         uw[q] = T(0);
         const int r = r0 - 1 + q;
-        if (valid && r <= n1) {
+        if (r <= n1) {
             const T* p = ph + off + (q - 1) * sy;
             w[q] = {__ldg(p - 1), __ldg(p), __ldg(p + 1)};
             uw[q] = __ldg(uu + off + (q - 1) * sy);
@@ -173,30 +178,25 @@ __device__ __forceinline__ void strip_unit(const typename Ops::Params& m, uint64
         }
     }
     // y face below the first row (between r0-1 and r0)
-    if (valid) jb = Ops::yface(m, w[1].b - w[0].b, w[1].c - w[1].a, w[0].c, w[0].a);
+    jb = Ops::yface(m, w[1].b - w[0].b, w[1].c - w[1].a, w[0].c, w[0].a);
 
 #define LG_ROW(J, Q)                                                                                            \
-    strip_row<T, Ops, NOISE, NX, FULL, PF>(m, g, J, r0, lane, col, valid, last_lane, n0, n1, off, ph, uu, out, po,  \
+    strip_row<T, Ops, NOISE, NX, FULL, PF, TAIL>(m, g, J, r0, r1, lane, col, valid, last_lane, n0, n1, off, ph, uu, out, po,  \
                                        uo, nb, edge_x, block_key, bnd, w[(Q) % NB], w[((Q) + 1) % NB],          \
                                        w[((Q) + 2) % NB], w[((Q) + 2 + PF) % NB], uw[(Q) % NB],                \
                                        uw[((Q) + 1) % NB], uw[((Q) + 2) % NB], uw[((Q) + 2 + PF) % NB], jb, dt, \
                                        scale_amp);                                                              \
     off += sy
-    int j = r0;
-    for (; j + NB <= r1; j += NB) {
+    for (int j = r0; j < r1; j += NB) {
 #pragma unroll
         for (int q = 0; q < NB; ++q) { LG_ROW(j + q, q); }
-    }
-#pragma unroll
-    for (int q = 0; q < NB - 1; ++q) {
-        if (j + q < r1) { LG_ROW(j + q, q); }
     }
 #undef LG_ROW
 }
 
 // Rows per work unit are at most 32, so one batch of boundary faces (lanes
 // across rows) serves the whole unit.
-template <class T, class Ops, bool NOISE, int MINB, int NX, int PF, bool BATCH = false>
+template <class T, class Ops, bool NOISE, int MINB, int NX, int PF, bool BATCH = false, bool TAIL = false>
 __global__ void __launch_bounds__(256, MINB)
     modelc_strip_kernel(const T* __restrict__ in, T* __restrict__ out, TileArgs g, typename Ops::Params m0, T dt,
                         T scale_amp, BatchArgs bt) {
@@ -221,8 +221,15 @@ __global__ void __launch_bounds__(256, MINB)
         const int s = (int)(unit % g.strips);
         const int k = (int)((unit / g.strips) % g.chunks);
         const int b = (int)(unit / ((int64_t)g.strips * g.chunks));
-        const int r0 = k * g.rows;
-        const int r1 = min(n1, r0 + g.rows);
+        // units are g.rows high (a multiple of NB unless TAIL); a block's
+        // last unit ends on its last row and may overlap the one before it,
+        // whose rows it then recomputes to the same bits
+        int r0 = k * g.rows;
+        int r1 = r0 + g.rows;
+        if (r1 > n1) {
+            r1 = n1;
+            if (!TAIL) r0 = n1 - g.rows;
+        }
         const int c0 = s * 32;
         const int col = c0 + lane;
         const bool valid = FULL || col < n0;
@@ -239,19 +246,21 @@ __global__ void __launch_bounds__(256, MINB)
         if constexpr (BATCH) {
             const int inst = b / bt.bpi;
             const typename Ops::Params mi = static_cast<const typename Ops::Params*>(bt.params)[inst];
-            strip_unit<T, Ops, NOISE, NX, FULL, PF>(mi, bt.seeds[inst], b - inst * bt.bpi, g, ph, uu, out, po, uo, nb,
+            strip_unit<T, Ops, NOISE, NX, FULL, PF, TAIL>(mi, bt.seeds[inst], b - inst * bt.bpi, g, ph, uu, out, po, uo, nb,
                                                     r0, r1, lane, col, valid, last_lane, cr, edge_x, n0, n1, sy,
                                                     tnow, dt, scale_amp);
         } else {
-            strip_unit<T, Ops, NOISE, NX, FULL, PF>(m0, g.seed, b, g, ph, uu, out, po, uo, nb, r0, r1, lane, col,
+            strip_unit<T, Ops, NOISE, NX, FULL, PF, TAIL>(m0, g.seed, b, g, ph, uu, out, po, uo, nb, r0, r1, lane, col,
                                                     valid, last_lane, cr, edge_x, n0, n1, sy, tnow, dt, scale_amp);
         }
     }
 }
 
-// Rows per work unit: at most 32 (one batch of boundary faces per unit);
-// fewer only when the grid would otherwise hold too few warps.
-inline int strip_rows(const CartTopo& topo, int strips, int rows) {
+// Rows per work unit: at most 32 (one batch of boundary faces per unit),
+// fewer only when the grid would otherwise hold too few warps, and a whole
+// number of groups of nb rows (the row loop's unroll) when the block has at
+// least nb rows.
+inline int strip_rows(const CartTopo& topo, int strips, int rows, int nb) {
     const int n1 = topo.n[1];
     if (rows <= 0) {
         const int64_t want_units = (int64_t)148 * 48 * 2;
@@ -260,27 +269,38 @@ inline int strip_rows(const CartTopo& topo, int strips, int rows) {
             (int)std::max<int64_t>(1, std::min<int64_t>(n1, (want_units + per_chunk - 1) / per_chunk));
         rows = std::max(8, (n1 + chunks - 1) / chunks);
     }
-    return std::max(1, std::min(std::min(rows, 32), n1));
+    rows = std::max(1, std::min(std::min(rows, 32), n1));
+    if (n1 >= nb) rows = std::max(nb, rows / nb * nb);
+    return rows;
 }
 
-// work decomposition of a launch: units of (block, strip, row chunk)
-inline dim3 strip_grid(TileArgs& g) {
+// work decomposition of a launch: units of (block, strip, row chunk); true
+// when the block is lower than the row group (the TAIL kernels)
+inline bool strip_plan(TileArgs& g, int nb) {
     const int n0 = g.topo.n[0], n1 = g.topo.n[1];
     g.strips = (n0 + 31) / 32;
-    g.rows = strip_rows(g.topo, g.strips, g.rows);
+    g.rows = strip_rows(g.topo, g.strips, g.rows, nb);
     g.chunks = (n1 + g.rows - 1) / g.rows;
     g.units = (int64_t)g.topo.nblocks * g.strips * g.chunks;
+    return n1 < nb;
+}
+
+inline dim3 strip_ctas(const TileArgs& g) {
     const int wpc = 8;
-    const int64_t ctas = std::min<int64_t>((g.units + wpc - 1) / wpc, (int64_t)1 << 30);
-    return dim3((unsigned)ctas);
+    return dim3((unsigned)std::min<int64_t>((g.units + wpc - 1) / wpc, (int64_t)1 << 30));
 }
 
 // batched instances: block widths 64 (the ensemble configuration) and 32
 // get a compile-time row stride
 template <class T, class Ops, bool NOISE, int MINB>
 cudaError_t launch_strip_batch(const T* in, T* out, TileArgs g, BatchArgs bt, T dt, T scale_amp, cudaStream_t s) {
-    const dim3 grid = strip_grid(g), block(256);
+    const bool tail = strip_plan(g, 1 + 3);
+    const dim3 grid = strip_ctas(g), block(256);
     const typename Ops::Params m{};
+    if (tail) {
+        modelc_strip_kernel<T, Ops, NOISE, MINB, 0, 1, true, true><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp, bt);
+        return cudaGetLastError();
+    }
     switch (g.topo.n[0]) {
         case 32: modelc_strip_kernel<T, Ops, NOISE, MINB, 32, 1, true><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp, bt); break;
         case 64: modelc_strip_kernel<T, Ops, NOISE, MINB, 64, 1, true><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp, bt); break;
@@ -292,15 +312,13 @@ cudaError_t launch_strip_batch(const T* in, T* out, TileArgs g, BatchArgs bt, T 
 template <class T, class Ops, bool NOISE, int MINB, int PF>
 cudaError_t launch_strip_minb(const T* in, T* out, TileArgs g, const typename Ops::Params& m, T dt, T scale_amp,
                               cudaStream_t s) {
-    const int n0 = g.topo.n[0], n1 = g.topo.n[1];
-    g.strips = (n0 + 31) / 32;
-    g.rows = strip_rows(g.topo, g.strips, g.rows);
-    g.chunks = (n1 + g.rows - 1) / g.rows;
-    g.units = (int64_t)g.topo.nblocks * g.strips * g.chunks;
-    const int wpc = 8;
-    const int64_t ctas = std::min<int64_t>((g.units + wpc - 1) / wpc, (int64_t)1 << 30);
-    const dim3 grid((unsigned)ctas), block(wpc * 32);
-    switch (n0) {  // block widths of the shipped configurations get a compile-time row stride
+    const bool tail = strip_plan(g, PF + 3);
+    const dim3 grid = strip_ctas(g), block(256);
+    if (tail) {
+        modelc_strip_kernel<T, Ops, NOISE, MINB, 0, PF, false, true><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp, BatchArgs{});
+        return cudaGetLastError();
+    }
+    switch (g.topo.n[0]) {  // block widths of the shipped configurations get a compile-time row stride
         case 32: modelc_strip_kernel<T, Ops, NOISE, MINB, 32, PF><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp, BatchArgs{}); break;
         case 64: modelc_strip_kernel<T, Ops, NOISE, MINB, 64, PF><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp, BatchArgs{}); break;
         case 126: modelc_strip_kernel<T, Ops, NOISE, MINB, 126, PF><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp, BatchArgs{}); break;

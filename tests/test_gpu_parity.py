@@ -255,6 +255,23 @@ def test_modelc_tile_ragged_blocks(sched, orc, block):
     assert np.array_equal(sim.state.interior("u"), os_.interior(1))
 
 
+@pytest.mark.parametrize("block", [[33, 20], [126, 6], [126, 40]])
+def test_modelc_tile_ragged_blocks_noisy(sched, orc, block):
+    # strips whose last lanes lie past the block edge: with noise, the strip
+    # kernel gives the bits of the one-thread-per-cell kernel
+    cells = [block[0] * 2, block[1] * 2]
+    grid = L.CartesianGrid(cells, block, [0.0, 0.0], [H, H])
+    model = L.ModelC(0.06, 3.19, 0.05)
+    sims = []
+    for variant in (2, 1):
+        sim = L.Simulation(grid, L.FiniteVolume(), model, L.EulerMaruyama(5), sched, L.CudaAllocator("f64"))
+        model.initialize_grains(grid, sim.state, [L.Grain((cells[0] * H / 2, cells[1] * H / 2), 2.0)], 0.7)
+        sim.run(model.stable_dt(grid.spacing), 30, variant=variant)
+        sims.append(sim)
+    for f in ("phi", "u"):
+        assert np.array_equal(sims[0].state.download(f), sims[1].state.download(f))
+
+
 def test_modelc_fp32_noisy_tracks_fp64_oracle(sched, orc):
     # same counter-based noise realization in both precisions
     sim, os_, _ = _modelc_pair(sched, orc, [64, 64], [32, 32], [(H, H, 10 * H)], 0.05, 300, dtype="f32")
