@@ -272,6 +272,12 @@ int lg_ensemble_run(lg_ensemble* e, double dt, int64_t nsteps, uint32_t flags);
  * x_T.  Parameter gradients accumulate in FP64 (FP32 ensembles included). */
 int lg_ensemble_value_and_grad(lg_ensemble* e, double dt, int64_t nsteps, int64_t ckpt_every, const double* target,
                                double* loss, double* grad_params, double* grad_phi0, double* grad_u0);
+/* The form of the step adjoint value_and_grad runs: LG_ADJOINT_STRIP (warp
+ * strips walking up the rows; the default) or LG_ADJOINT_TILE (shared-memory
+ * tiles with a two-cell halo).  Both give the same gradients up to rounding. */
+#define LG_ADJOINT_STRIP 0
+#define LG_ADJOINT_TILE 1
+int lg_ensemble_set_adjoint_kernel(lg_ensemble* e, int kernel);
 
 /* Standard normals of n keys on the device (`rng::standard_normal`,
  * src/util/rng.rs:43-49); host arrays in and out. */

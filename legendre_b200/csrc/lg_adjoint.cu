@@ -404,6 +404,312 @@ __global__ void __launch_bounds__(256) loss_seed_kernel(const T* __restrict__ x,
     }
 }
 
+// ------------------------------------------------------------ strip form --
+// The same step adjoint with one warp per work unit and no shared memory:
+// the warp owns 32 adjacent columns of one instance (lane l at column
+// X = 29 s - 1 + l) and walks up a run of rows.  Lanes 1..29 produce the
+// cotangents of their columns; lanes 0, 30 and 31 are the halo the
+// derivation needs (the cell-centred N^ and A^ of the neighbours of an
+// output cell, and the faces between them), so every face derivative is
+// evaluated once per lane and row and reaches the neighbouring lanes by
+// shuffles.
+//
+// Step r of the walk "completes" row r -- the x face left of each lane's
+// cell, the y face above it, the cell's N^, A^ and nu, and the face
+// cotangents that those make final -- and then gathers the cotangent of row
+// r - 1, whose stencil (rows r-2 .. r) is complete.  A unit that starts at
+// the instance's first row also gathers the ghost row below it, and one that
+// ends at the last row the ghost row above it; both fold into the adjacent
+// interior row, as the ghost columns X = -1 and X = N0 fold into columns 0
+// and N0 - 1 across lanes.  Quantities of cells outside the instance are
+// zero (selected, so that no value of a halo lane leaks in).
+constexpr int SW = 29;  // output columns per strip
+
+// Slab-offset row terms of consecutive rows: the division by the block
+// height happens only when the walk crosses a block edge or the instance
+// edge (where rows are mirrored).
+struct RowWalk {
+    int Y, yl;
+    int64_t term;
+    __device__ void init(const Geo& g, int y) {
+        Y = y;
+        term = row_term(g, y);
+        const int yc = reflect_clamp(y, g.N1);
+        yl = yc - (yc / g.n1) * g.n1;
+    }
+    __device__ void next(const Geo& g) {
+        ++Y;
+        ++yl;
+        if (Y <= 0 || Y >= g.N1 || yl == g.n1)
+            init(g, Y);
+        else
+            term += g.n0 + 2;
+    }
+};
+
+template <class T>
+__device__ __forceinline__ T shfl_up1(T v) {
+    return __shfl_up_sync(0xffffffffu, v, 1);
+}
+template <class T>
+__device__ __forceinline__ T shfl_dn1(T v) {
+    return __shfl_down_sync(0xffffffffu, v, 1);
+}
+
+template <class T>
+__device__ __forceinline__ double warp_sum(double v) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+template <class T>
+__global__ void __launch_bounds__(256) adjoint_strip_kernel(const T* __restrict__ x, const T* __restrict__ lam_in,
+                                                            T* __restrict__ lam_out,
+                                                            const AdjParams<T>* __restrict__ prm, Geo g, T dt,
+                                                            double* __restrict__ acc, int rows, int strips,
+                                                            int chunks) {
+    const int lane = threadIdx.x & 31;
+    const int64_t units = g.ninst * strips * chunks;
+    for (int64_t unit = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; unit < units;
+         unit += ((int64_t)gridDim.x * blockDim.x) >> 5) {
+        const int s = (int)(unit % strips);
+        const int k = (int)((unit / strips) % chunks);
+        const int64_t inst = unit / ((int64_t)strips * chunks);
+        const AdjParams<T> m = prm[inst];
+        const int X = s * SW - 1 + lane;
+        const bool xin = X >= 0 && X < g.N0;
+        const bool xo = xin && lane >= 1 && lane <= SW;  // this lane's column is an output of the unit
+        const int Y0 = k * rows, Y1 = min(g.N1, Y0 + rows);
+        const int gs = Y0 == 0 ? -1 : Y0;         // first gathered row (the ghost row below the instance)
+        const int ge = Y1 == g.N1 ? g.N1 : Y1 - 1;  // last gathered row (the ghost row above)
+        const int64_t base = inst * g.bpi * 2 * g.slab_stride;
+        const int64_t cC = base + col_term(g, X), cL = base + col_term(g, X - 1);
+        const int64_t ss = g.slab_stride;
+
+        // window rows r-1 (m), r (0), r+1 (p) at X-1 (a), X (b); X+1 by shuffle
+        // loads run one row ahead: step r reads the state of row r + 2 and
+        // the incoming cotangents of row r + 1
+        T pma, pmb, p0a, p0b, ppa, ppb, um, u0, up;
+        RowWalk rw;  // the last state row loaded
+        const int cs = gs - 1;
+        rw.init(g, cs - 1);
+        pma = x[cL + rw.term];
+        pmb = x[cC + rw.term];
+        um = x[cC + rw.term + ss];
+        const int64_t t_m = rw.term;
+        rw.next(g);
+        p0a = x[cL + rw.term];
+        p0b = x[cC + rw.term];
+        u0 = x[cC + rw.term + ss];
+        const int64_t t_0 = rw.term;
+        rw.next(g);
+        T nxa = x[cL + rw.term], nxb = x[cC + rw.term], nxu = x[cC + rw.term + ss];  // row cs + 1
+        T npb = T(0), nub = T(0);  // cotangents of row cs
+        if (xin && cs >= 0 && cs < g.N1) {
+            npb = lam_in[cC + t_0];
+            nub = lam_in[cC + t_0 + ss];
+        }
+        // y face (cs - 1, cs): its flux value for row cs
+        T yJ_prev;
+        {
+            const T mc = shfl_dn1(pmb), c0 = shfl_dn1(p0b);
+            const T dn = p0b - pmb;
+            const T dtr = T(0.25) * (((c0 - p0a) + mc) - pma);
+            const FaceDer<T> f = face_der(dtr, dn, m.f_a_bar, m.f_ae, m.f_a12, m.f_tol);
+            yJ_prev = f.a * (f.a * dn + f.da * dtr);
+        }
+        T yn_raw_prev = T(0), yt_raw_prev = T(0), ye_raw_prev = T(0);  // y face (r-1, r) before its cotangent
+        T nb_prev = T(0), pb_prev = T(0), ub_prev = T(0);                // row r-1
+        T xn_prev = T(0), xt_pm = T(0), xt_prev = T(0);  // xn of row r-1; xt of rows r-2, r-1
+        T yn_pm = T(0), yt_pm = T(0);                     // y face (r-2, r-1) with its cotangent
+        T ax_prev = T(0), ay_pm = T(0), ay_prev = T(0), nu_pm = T(0), nu_prev = T(0);
+        T gm_p = T(0), gm_u = T(0), gt_p = T(0), gt_u = T(0);  // ghost-row gathers below / the top row's gather
+        double acc_l = 0.0, acc_d = 0.0, acc_e = 0.0;
+        // row terms of rows r - 1, r and r + 1 (mirrored outside the instance,
+        // where no cotangent is loaded or stored)
+        int64_t rt_m = t_m, rt_0 = t_0, rt_p = rw.term;
+
+        for (int r = cs; r <= ge + 1; ++r) {
+            // ---- complete row r: row r + 1 arrived in the previous step;
+            // start the loads of the next one
+            ppa = nxa;
+            ppb = nxb;
+            up = nxu;
+            const T pb = npb, ub = nub;
+            rw.next(g);
+            nxa = x[cL + rw.term];
+            nxb = x[cC + rw.term];
+            nxu = x[cC + rw.term + ss];
+            npb = nub = T(0);
+            if (xin && r + 1 >= 0 && r + 1 < g.N1) {
+                npb = lam_in[cC + rt_p];
+                nub = lam_in[cC + rt_p + ss];
+            }
+            const bool rin = r >= 0 && r < g.N1;
+            const bool cin = rin && xin;
+            const bool orow = r >= Y0 && r < Y1;
+            const T p0c = shfl_dn1(p0b), ppc = shfl_dn1(ppb);
+            // x face left of X in row r
+            T xJ, xn_raw, xt_raw, xe_raw;
+            {
+                const T dn = p0b - p0a;
+                const T dtr = T(0.25) * (((ppb - pmb) + ppa) - pma);
+                const FaceDer<T> f = face_der(dn, dtr, m.f_a_bar, m.f_ae, m.f_a12, m.f_tol);
+                xJ = f.a * (f.a * dn - f.da * dtr);
+                xn_raw = T(2) * f.a * f.ax * dn + f.a * f.a - (f.ax * f.da + f.a * f.dax) * dtr;
+                xt_raw = T(2) * f.a * f.ay * dn - (f.ay * f.da + f.a * f.day) * dtr - f.a * f.da;
+                xe_raw = (T(2) * f.a * dn - f.da * dtr) * f.ae - f.a * dtr * f.dae;
+            }
+            // y face above X in row r (between rows r and r + 1)
+            T yJ, yn_raw, yt_raw, ye_raw;
+            {
+                const T dn = ppb - p0b;
+                const T dtr = T(0.25) * (((ppc - ppa) + p0c) - p0a);
+                const FaceDer<T> f = face_der(dtr, dn, m.f_a_bar, m.f_ae, m.f_a12, m.f_tol);
+                yJ = f.a * (f.a * dn + f.da * dtr);
+                yn_raw = T(2) * f.a * f.ay * dn + f.a * f.a + (f.ay * f.da + f.a * f.day) * dtr;
+                yt_raw = T(2) * f.a * f.ax * dn + (f.ax * f.da + f.a * f.dax) * dtr + f.a * f.da;
+                ye_raw = (T(2) * f.a * dn + f.da * dtr) * f.ae + f.a * dtr * f.dae;
+            }
+            // cell (X, r): N^, A^ and nu
+            const T xJr = shfl_dn1(xJ);
+            T nb, ax, ay, nu;
+            {
+                const T ph = p0b, uc = u0;
+                const T flux = ((xJr - xJ) + (yJ - yJ_prev)) * m.inv_h2_flux;
+                const T omp = T(1) - ph * ph;
+                const T pp = omp * omp;
+                const T gp = ph * ph * ph - ph;
+                const T Nn = -m.lambda * uc * pp + (flux - gp);
+                const CentreDer<T> c =
+                    centre_der(T(0.5) * (p0c - p0a), T(0.5) * (ppb - pmb), m.c_a_bar, m.c_ae, m.c_tol);
+                const T ia = recip(c.a);
+                const T iq = ia * ia;
+                const T kphi = Nn * iq;
+                const T mu = dt * (pb + T(0.5) * ub);
+                const T nbar = mu * iq;
+                const T abar = T(-2) * mu * kphi * ia;
+                nb = cin ? nbar : T(0);
+                ax = cin ? abar * T(0.5) * c.ax : T(0);
+                ay = cin ? abar * T(0.5) * c.ay : T(0);
+                nu = cin ? dt * m.d_thermal * ub : T(0);
+                const T uL = shfl_up1(u0), uR = shfl_dn1(u0);
+                if (xo && orow) {
+                    const T lap = ((uR - T(2) * uc) + uL) * m.ih0 + ((up - T(2) * uc) + um) * m.ih1;
+                    acc_l += (double)(nbar * (-uc * pp));
+                    acc_d += (double)(dt * ub * lap);
+                    acc_e += (double)(abar * c.ae);
+                }
+            }
+            // cotangent of the x face left of X (cells X-1 and X of row r)
+            T nbl = shfl_up1(nb);
+            if (lane == 0) nbl = T(0);  // lane 0 is a halo lane; its left face matters only outside the instance
+            const T jbx = (nbl - nb) * m.inv_h2_flux;
+            const T xn = xn_raw * jbx, xt = xt_raw * jbx;
+            // the face is counted by the cell on its right, or by the last cell for the face into the ghost column
+            if (orow && ((xo) || (X == g.N0 && lane >= 2 && lane <= SW + 1))) acc_e += (double)(jbx * xe_raw);
+            // cotangent of the y face (r-1, r)
+            const T jby = (nb_prev - nb) * m.inv_h2_flux;
+            const T yn_f = yn_raw_prev * jby, yt_f = yt_raw_prev * jby;
+            if (xo && (orow || (r == g.N1 && r - 1 >= Y0 && r - 1 < Y1))) acc_e += (double)(jby * ye_raw_prev);
+
+            // ---- gather row q = r - 1 (its stencil rows q-1 .. q+1 are complete)
+            const int q = r - 1;
+            if (q >= gs) {
+                const bool qin = q >= 0 && q < g.N1;
+                T pbar = T(0), ubar = T(0);
+                if (qin && xin) {
+                    const T ph = pmb, uc = um;
+                    const T omp = T(1) - ph * ph;
+                    const T dndphi = T(4) * m.lambda * uc * ph * omp + (T(1) - T(3) * ph * ph);
+                    pbar = pb_prev + nb_prev * dndphi;
+                    ubar = ub_prev - nb_prev * m.lambda * omp * omp - T(2) * (m.ih0 + m.ih1) * nu_prev;
+                }
+                const T xnR = shfl_dn1(xn_prev), xtR_m = shfl_dn1(xt_pm), xtR_p = shfl_dn1(xt);
+                pbar += xn_prev - xnR;
+                pbar += T(0.25) * ((xtR_m - xtR_p) + (xt_pm - xt));
+                pbar += yn_pm - yn_f;
+                T ytL = shfl_up1(yt_f), ytL_m = shfl_up1(yt_pm), axL = shfl_up1(ax_prev), nuL = shfl_up1(nu_prev);
+                if (lane == 0) ytL = ytL_m = axL = nuL = T(0);  // column X-2: outside whenever lane 0 is gathered
+                const T ytR = shfl_dn1(yt_f), ytR_m = shfl_dn1(yt_pm), axR = shfl_dn1(ax_prev),
+                        nuR = shfl_dn1(nu_prev);
+                pbar += T(0.25) * ((ytL - ytR) + (ytL_m - ytR_m));
+                pbar += (axL - axR) + (ay_pm - ay);
+                ubar += (nuL + nuR) * m.ih0 + (nu_pm + nu) * m.ih1;
+                // fold the ghost columns into columns 0 and N0 - 1
+                const T gpl = shfl_up1(pbar), gul = shfl_up1(ubar), gpr = shfl_dn1(pbar), gur = shfl_dn1(ubar);
+                if (X == 0 && lane >= 1) {
+                    pbar += gpl;
+                    ubar += gul;
+                }
+                if (X == g.N0 - 1 && lane <= 30) {
+                    pbar += gpr;
+                    ubar += gur;
+                }
+                // fold the ghost rows; store row q, or the top row once its ghost row is in
+                if (q == -1) {
+                    gm_p = pbar;
+                    gm_u = ubar;
+                } else if (q == g.N1) {
+                    if (xo) {
+                        const int64_t o = cC + row_term(g, g.N1 - 1);
+                        lam_out[o] = gt_p + pbar;
+                        lam_out[o + ss] = gt_u + ubar;
+                    }
+                } else {
+                    if (q == 0 && gs == -1) {
+                        pbar += gm_p;
+                        ubar += gm_u;
+                    }
+                    if (q == g.N1 - 1) {
+                        gt_p = pbar;
+                        gt_u = ubar;
+                    } else if (xo) {
+                        lam_out[cC + rt_m] = pbar;
+                        lam_out[cC + rt_m + ss] = ubar;
+                    }
+                }
+            }
+
+            // ---- shift the window
+            rt_m = rt_0;
+            rt_0 = rt_p;
+            rt_p = rw.term;
+            pma = p0a;
+            pmb = p0b;
+            p0a = ppa;
+            p0b = ppb;
+            um = u0;
+            u0 = up;
+            yJ_prev = yJ;
+            yn_raw_prev = yn_raw;
+            yt_raw_prev = yt_raw;
+            ye_raw_prev = ye_raw;
+            nb_prev = nb;
+            pb_prev = pb;
+            ub_prev = ub;
+            xn_prev = xn;
+            xt_pm = xt_prev;
+            xt_prev = xt;
+            yn_pm = yn_f;
+            yt_pm = yt_f;
+            ax_prev = ax;
+            ay_pm = ay_prev;
+            ay_prev = ay;
+            nu_pm = nu_prev;
+            nu_prev = nu;
+        }
+        acc_l = warp_sum<T>(acc_l);
+        acc_d = warp_sum<T>(acc_d);
+        acc_e = warp_sum<T>(acc_e);
+        if (lane == 0) {
+            acc[3 * unit + 0] += acc_l;
+            acc[3 * unit + 1] += acc_d;
+            acc[3 * unit + 2] += acc_e;
+        }
+    }
+}
+
 template <class T, int TH>
 cudaError_t launch_adjoint(const T* x, const T* lam_in, T* lam_out, const void* prm, Geo g, double dt, double* acc,
                            cudaStream_t s) {
@@ -423,12 +729,44 @@ cudaError_t launch_adjoint(const T* x, const T* lam_in, T* lam_out, const void* 
     return cudaGetLastError();
 }
 
+
+template <class T>
+cudaError_t launch_adjoint_strip(const T* x, const T* lam_in, T* lam_out, const void* prm, const Geo& g, double dt,
+                                 double* acc, cudaStream_t s) {
+    const int strips = adjoint_strips(g), rows = adjoint_strip_rows(g);
+    const int chunks = (g.N1 + rows - 1) / rows;
+    const int64_t units = g.ninst * strips * chunks;
+    const unsigned grid = (unsigned)std::min<int64_t>((units + 7) / 8, (int64_t)1 << 30);
+    adjoint_strip_kernel<T><<<grid, 256, 0, s>>>(x, lam_in, lam_out, static_cast<const AdjParams<T>*>(prm), g, (T)dt,
+                                                 acc, rows, strips, chunks);
+    return cudaGetLastError();
+}
+
 }  // namespace
 
 int adjoint_tile_rows(int dtype) { return dtype == 0 ? 8 : 16; }
 
-cudaError_t launch_adjoint_step(int dtype, const void* x, const void* lam_in, void* lam_out, const void* prm,
-                                const Geo& g, double dt, double* acc, cudaStream_t s) {
+int adjoint_strips(const Geo& g) { return (g.N0 + SW - 1) / SW; }
+
+// rows per strip unit: the whole instance height, halved while the launch
+// would hold fewer than 32 warps per SM (down to 16 rows); each unit
+// completes two rows beyond the ones it gathers
+int adjoint_strip_rows(const Geo& g) {
+    const int strips = adjoint_strips(g);
+    int rows = std::max(1, g.N1);
+    while (rows > 16 && g.ninst * strips * ((g.N1 + rows - 1) / rows) < (int64_t)148 * 32) rows = (rows + 1) / 2;
+    return rows;
+}
+
+cudaError_t launch_adjoint_step(int dtype, int kernel, const void* x, const void* lam_in, void* lam_out,
+                                const void* prm, const Geo& g, double dt, double* acc, cudaStream_t s) {
+    if (kernel == kAdjointStrip) {
+        if (dtype == 0)
+            return launch_adjoint_strip<double>((const double*)x, (const double*)lam_in, (double*)lam_out, prm, g, dt,
+                                                acc, s);
+        return launch_adjoint_strip<float>((const float*)x, (const float*)lam_in, (float*)lam_out, prm, g, dt, acc,
+                                           s);
+    }
     if (dtype == 0)
         return launch_adjoint<double, 8>((const double*)x, (const double*)lam_in, (double*)lam_out, prm, g, dt, acc,
                                          s);
@@ -450,7 +788,11 @@ cudaError_t launch_loss_seed(int dtype, const void* x, const double* target, voi
 
 int64_t loss_items(const Geo& g) { return (int64_t)g.ninst * ((g.N0 + TW - 1) / TW) * ((g.N1 + 7) / 8); }
 
-int64_t adjoint_items(int dtype, const Geo& g) {
+int64_t adjoint_items(int dtype, int kernel, const Geo& g) {
+    if (kernel == kAdjointStrip) {
+        const int rows = adjoint_strip_rows(g);
+        return g.ninst * adjoint_strips(g) * ((g.N1 + rows - 1) / rows);
+    }
     const int th = adjoint_tile_rows(dtype);
     return (int64_t)g.ninst * ((g.N0 + TW - 1) / TW) * ((g.N1 + th - 1) / th);
 }

@@ -30,13 +30,20 @@ struct AdjParams {
 size_t adj_params_size(int dtype);  // dtype: 0 FP64, 1 FP32
 void adj_params(int dtype, const ModelCDev& m, void* out);
 
+// the two forms of the step adjoint: warp strips (the default) and shared-
+// memory tiles; both compute the same cotangents up to rounding
+constexpr int kAdjointStrip = 0, kAdjointTile = 1;
+
 int adjoint_tile_rows(int dtype);
-int64_t adjoint_items(int dtype, const Geo& g);  // tiles; the accumulator holds 3 doubles per tile
+int adjoint_strips(const Geo& g);
+int adjoint_strip_rows(const Geo& g);
+// work items (tiles or strip units); the accumulator holds 3 doubles per item
+int64_t adjoint_items(int dtype, int kernel, const Geo& g);
 int64_t loss_items(const Geo& g);                // tiles of the loss kernel; one double each
 
-// cotangents of x_n from those of x_{n+1}; acc[3 tile + k] += the step's
-// dL/d(lambda, D, eps4) share of each tile
-cudaError_t launch_adjoint_step(int dtype, const void* x, const void* lam_in, void* lam_out, const void* prm,
+// cotangents of x_n from those of x_{n+1}; acc[3 item + k] += the step's
+// dL/d(lambda, D, eps4) share of each work item
+cudaError_t launch_adjoint_step(int dtype, int kernel, const void* x, const void* lam_in, void* lam_out, const void* prm,
                                 const Geo& g, double dt, double* acc, cudaStream_t s);
 // lam = (2 (phi - target), 0), loss[tile] = that tile's sum of squares
 cudaError_t launch_loss_seed(int dtype, const void* x, const double* target, void* lam, Geo g, double* loss,

@@ -59,8 +59,10 @@ struct lg_ensemble {
     std::vector<void*> ckpt, seg;
     void* adj[2] = {nullptr, nullptr};
     double* d_acc = nullptr;
+    int64_t acc_cap = 0;  // doubles held by d_acc
     double* d_loss = nullptr;
     double* d_target = nullptr;
+    int adj_kernel = lg::adj::kAdjointStrip;
 };
 
 namespace {
@@ -427,12 +429,18 @@ int lg_ensemble_value_and_grad(lg_ensemble* e, double dt, int64_t nsteps, int64_
     int rc = alloc_states(e, e->ckpt, (size_t)nseg);
     if (rc == LG_OK) rc = alloc_states(e, e->seg, (size_t)std::max<int64_t>(K - 1, 0));
     if (rc != LG_OK) return rc;
-    const int64_t acc_n = 3 * lg::adj::adjoint_items(kind, geo), loss_n = lg::adj::loss_items(geo);
+    const int64_t acc_n = 3 * lg::adj::adjoint_items(kind, e->adj_kernel, geo), loss_n = lg::adj::loss_items(geo);
     if (!e->adj[0]) {
         for (void*& q : e->adj) ENS_CUDA(e, cudaMalloc(&q, state_bytes(e)));
-        ENS_CUDA(e, cudaMalloc(&e->d_acc, acc_n * sizeof(double)));
         ENS_CUDA(e, cudaMalloc(&e->d_loss, loss_n * sizeof(double)));
         ENS_CUDA(e, cudaMalloc(&e->d_target, cells * sizeof(double)));
+    }
+    if (e->acc_cap < acc_n) {
+        cudaFree(e->d_acc);
+        e->d_acc = nullptr;
+        e->acc_cap = 0;
+        ENS_CUDA(e, cudaMalloc(&e->d_acc, acc_n * sizeof(double)));
+        e->acc_cap = acc_n;
     }
     ENS_CUDA(e, cudaMemcpyAsync(e->d_target, target, cells * sizeof(double), cudaMemcpyHostToDevice, st));
     ENS_CUDA(e, cudaMemsetAsync(e->d_acc, 0, acc_n * sizeof(double), st));
@@ -475,7 +483,7 @@ int lg_ensemble_value_and_grad(lg_ensemble* e, double dt, int64_t nsteps, int64_
         }
         for (int64_t i = len - 1; i >= 0; --i) {
             const void* x = i == 0 ? e->ckpt[(size_t)s] : e->seg[(size_t)(i - 1)];
-            ENS_CUDA(e, lg::adj::launch_adjoint_step(kind, x, e->adj[a], e->adj[a ^ 1], e->d_adj_params, geo, dt,
+            ENS_CUDA(e, lg::adj::launch_adjoint_step(kind, e->adj_kernel, x, e->adj[a], e->adj[a ^ 1], e->d_adj_params, geo, dt,
                                                      e->d_acc, st));
             lg::abi_count_launch(e->ctx, 1);
             a ^= 1;
@@ -514,6 +522,14 @@ int lg_ensemble_value_and_grad(lg_ensemble* e, double dt, int64_t nsteps, int64_
         grad_params[4 * i + 2] = g2;
         grad_params[4 * i + 3] = gd;
     }
+    return LG_OK;
+}
+
+int lg_ensemble_set_adjoint_kernel(lg_ensemble* e, int kernel) {
+    if (!e) return LG_ERR_INVALID;
+    if (kernel != LG_ADJOINT_STRIP && kernel != LG_ADJOINT_TILE)
+        return efail(e, LG_ERR_INVALID, "unknown adjoint kernel");
+    e->adj_kernel = kernel == LG_ADJOINT_STRIP ? lg::adj::kAdjointStrip : lg::adj::kAdjointTile;
     return LG_OK;
 }
 

@@ -84,9 +84,17 @@ class Ensemble:
         N.check(N.lib.lg_ensemble_run(self.handle, float(dt), int(nsteps), N.LG_RUN_GRAPH if graph else 0),
                 self.scheduler.handle)
 
-    def value_and_grad(self, dt: float, nsteps: int, ckpt_every: int, target, cell_grads: bool = True) -> dict:
+    ADJOINT_KERNELS = {"strip": 0, "tile": 1}
+
+    def value_and_grad(self, dt: float, nsteps: int, ckpt_every: int, target, cell_grads: bool = True,
+                       kernel: str = "strip") -> dict:
         """Loss and gradients of every instance (see the module docstring); the
-        state is left at the final step."""
+        state is left at the final step.  ``kernel`` picks the form of the
+        step adjoint: "strip" (warps walking up the rows) or "tile"
+        (shared-memory tiles); they agree up to rounding."""
+        if kernel not in self.ADJOINT_KERNELS:
+            raise ValueError("kernel is 'strip' or 'tile'")
+        N.check(N.lib.lg_ensemble_set_adjoint_kernel(self.handle, self.ADJOINT_KERNELS[kernel]), self.scheduler.handle)
         tgt = np.ascontiguousarray(np.broadcast_to(target, self.shape), dtype=np.float64)
         loss = np.empty(self.ninst)
         gp = np.empty((self.ninst, 4))

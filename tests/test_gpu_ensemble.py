@@ -187,3 +187,35 @@ def test_fp32_gradients_close_to_fp64(sched, problem):
         assert np.all(np.abs(g32[k] - g64[k]) <= 2e-3 * np.abs(g64[k]) + 1e-4 * np.abs(g64[k]).max()), k
     rel = np.linalg.norm(g32["phi0"] - g64["phi0"]) / np.linalg.norm(g64["phi0"])
     assert rel < 5e-3
+
+
+@pytest.mark.parametrize("dtype,rel", [("f64", 1e-10), ("f32", 2e-4)])
+@pytest.mark.parametrize("cells,block,ninst", [((32, 32), 16, 2), ((96, 80), 16, 3), ((64, 64), 64, 1)])
+def test_strip_and_tile_adjoints_agree(sched, dtype, rel, cells, block, ninst):
+    # the two forms of the step adjoint (warp strips, shared-memory tiles):
+    # several strips with a ragged last one, several row runs per instance,
+    # block edges inside the instance and instance edges on every side
+    nx, ny = cells
+    grid = L.CartesianGrid([nx, ny], [block, block], [0.0, 0.0], [H, H])
+    ys, xs = np.meshgrid((np.arange(ny) + 0.5) * H, (np.arange(nx) + 0.5) * H, indexing="ij")
+    phi0 = np.empty((ninst, ny, nx))
+    for i in range(ninst):
+        r = np.hypot(xs - nx * H * (0.4 + 0.05 * i), ys - ny * H * (0.55 - 0.04 * i))
+        phi0[i] = np.maximum(-1.0, -np.tanh((r - 4.0) / math.sqrt(2.0)))
+    eps4, seeds = [0.03 + 0.01 * i for i in range(ninst)], [20 + i for i in range(ninst)]
+    target = np.tanh(phi0 * 0.8)
+    out = {}
+    for kernel in ("tile", "strip"):
+        model = L.ModelC(0.05, LAM, 0.01)
+        model.d_thermal = D
+        ens = L.Ensemble(grid, model, eps4, seeds, sched, dtype=dtype)
+        ens.set("phi", phi0)
+        ens.set("u", -0.5)
+        out[kernel] = ens.value_and_grad(DT, 9, 4, target, kernel=kernel)
+        ens._destroy()
+    a, b = out["tile"], out["strip"]
+    assert np.array_equal(a["loss"], b["loss"])
+    for k in ("lambda", "d_thermal", "eps4", "delta"):
+        assert np.allclose(b[k], a[k], rtol=rel, atol=rel * np.abs(a[k]).max()), k
+    for k in ("phi0", "u0"):
+        assert np.linalg.norm(b[k] - a[k]) <= rel * np.linalg.norm(a[k]), k
