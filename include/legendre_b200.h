@@ -278,6 +278,11 @@ int lg_ensemble_value_and_grad(lg_ensemble* e, double dt, int64_t nsteps, int64_
 #define LG_ADJOINT_STRIP 0
 #define LG_ADJOINT_TILE 1
 int lg_ensemble_set_adjoint_kernel(lg_ensemble* e, int kernel);
+/* Device bytes value_and_grad may spend on a resident tail: the last
+ * segments whose every state fits are kept from the forward pass instead of
+ * being recomputed from their checkpoints (the gradients are the same bits).
+ * 0, the default, is pure checkpointing; 0 also frees the kept states. */
+int lg_ensemble_set_resident_budget(lg_ensemble* e, uint64_t bytes);
 
 /* Standard normals of n keys on the device (`rng::standard_normal`,
  * src/util/rng.rs:43-49); host arrays in and out. */

@@ -135,6 +135,7 @@ _SIGS = {
     "lg_ensemble_run": (C.c_int, [_p, _d, _i64, C.c_uint32]),
     "lg_ensemble_value_and_grad": (C.c_int, [_p, _d, _i64, _i64, _pd, _pd, _pd, _pd, _pd]),
     "lg_ensemble_set_adjoint_kernel": (C.c_int, [_p, C.c_int]),
+    "lg_ensemble_set_resident_budget": (C.c_int, [_p, C.c_uint64]),
     "lg_amr_tag_level_static": (C.c_int, [_p, C.c_int, C.c_int, _d, _pi64, _i64, _pi64]),
 }
 

@@ -42,9 +42,13 @@ namespace {
 constexpr int TW = 32;
 
 __device__ __forceinline__ double recip(double x) { return 1.0 / x; }
-// single precision: the correctly rounded hardware reciprocal (the FP32
-// adjoint is not matched bit for bit to anything)
-__device__ __forceinline__ float recip(float x) { return __frcp_rn(x); }
+// single precision: the hardware's approximate reciprocal (PTX rcp.approx,
+// within one ulp; the FP32 adjoint is not matched bit for bit to anything)
+__device__ __forceinline__ float recip(float x) {
+    float r;
+    asm("rcp.approx.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
 
 // a(x, y), da(x, y) of KarmaRappelFlux::face and their partial derivatives
 // in x, y and eps4; x and y are the face's (derx, dery).
@@ -524,6 +528,9 @@ __global__ void __launch_bounds__(256) adjoint_strip_kernel(const T* __restrict_
         T yn_pm = T(0), yt_pm = T(0);                     // y face (r-2, r-1) with its cotangent
         T ax_prev = T(0), ay_pm = T(0), ay_prev = T(0), nu_pm = T(0), nu_prev = T(0);
         T gm_p = T(0), gm_u = T(0), gt_p = T(0), gt_u = T(0);  // ghost-row gathers below / the top row's gather
+        // neighbour-lane copies kept for the next rows: xt of the right lane
+        // (rows r-2, r-1), yt of the face (r-2, r-1) of both neighbours
+        T xtR_pm = T(0), xtR_prev = T(0), ytL_pm = T(0), ytR_pm = T(0);
         double acc_l = 0.0, acc_d = 0.0, acc_e = 0.0;
         // row terms of rows r - 1, r and r + 1 (mirrored outside the instance,
         // where no cotangent is loaded or stored)
@@ -613,6 +620,12 @@ __global__ void __launch_bounds__(256) adjoint_strip_kernel(const T* __restrict_
             const T yn_f = yn_raw_prev * jby, yt_f = yt_raw_prev * jby;
             if (xo && (orow || (r == g.N1 && r - 1 >= Y0 && r - 1 < Y1))) acc_e += (double)(jby * ye_raw_prev);
 
+            // neighbour copies of this row's face terms (used now and by the next two gathers)
+            const T xtR = shfl_dn1(xt);
+            T ytL = shfl_up1(yt_f);
+            const T ytR = shfl_dn1(yt_f);
+            if (lane == 0) ytL = T(0);  // column X-2: outside whenever lane 0 is gathered
+
             // ---- gather row q = r - 1 (its stencil rows q-1 .. q+1 are complete)
             const int q = r - 1;
             if (q >= gs) {
@@ -625,14 +638,14 @@ __global__ void __launch_bounds__(256) adjoint_strip_kernel(const T* __restrict_
                     pbar = pb_prev + nb_prev * dndphi;
                     ubar = ub_prev - nb_prev * m.lambda * omp * omp - T(2) * (m.ih0 + m.ih1) * nu_prev;
                 }
-                const T xnR = shfl_dn1(xn_prev), xtR_m = shfl_dn1(xt_pm), xtR_p = shfl_dn1(xt);
+                const T xnR = shfl_dn1(xn_prev);
                 pbar += xn_prev - xnR;
-                pbar += T(0.25) * ((xtR_m - xtR_p) + (xt_pm - xt));
+                pbar += T(0.25) * ((xtR_pm - xtR) + (xt_pm - xt));
                 pbar += yn_pm - yn_f;
-                T ytL = shfl_up1(yt_f), ytL_m = shfl_up1(yt_pm), axL = shfl_up1(ax_prev), nuL = shfl_up1(nu_prev);
-                if (lane == 0) ytL = ytL_m = axL = nuL = T(0);  // column X-2: outside whenever lane 0 is gathered
-                const T ytR = shfl_dn1(yt_f), ytR_m = shfl_dn1(yt_pm), axR = shfl_dn1(ax_prev),
-                        nuR = shfl_dn1(nu_prev);
+                T axL = shfl_up1(ax_prev), nuL = shfl_up1(nu_prev);
+                if (lane == 0) axL = nuL = T(0);
+                const T axR = shfl_dn1(ax_prev), nuR = shfl_dn1(nu_prev);
+                const T ytL_m = ytL_pm, ytR_m = ytR_pm;
                 pbar += T(0.25) * ((ytL - ytR) + (ytL_m - ytR_m));
                 pbar += (axL - axR) + (ay_pm - ay);
                 ubar += (nuL + nuR) * m.ih0 + (nu_pm + nu) * m.ih1;
@@ -691,6 +704,10 @@ __global__ void __launch_bounds__(256) adjoint_strip_kernel(const T* __restrict_
             xn_prev = xn;
             xt_pm = xt_prev;
             xt_prev = xt;
+            xtR_pm = xtR_prev;
+            xtR_prev = xtR;
+            ytL_pm = ytL;
+            ytR_pm = ytR;
             yn_pm = yn_f;
             yt_pm = yt_f;
             ax_prev = ax;

@@ -57,6 +57,8 @@ struct lg_ensemble {
     std::map<std::string, std::pair<cudaGraphExec_t, int64_t>> graphs;  // exec, launches per replay
     // backward workspace
     std::vector<void*> ckpt, seg;
+    std::vector<void*> res;   // every state of the resident tail segments
+    uint64_t res_budget = 0;  // device bytes value_and_grad may keep states in
     void* adj[2] = {nullptr, nullptr};
     double* d_acc = nullptr;
     int64_t acc_cap = 0;  // doubles held by d_acc
@@ -170,8 +172,10 @@ int step_once(lg_ensemble* e, const void* in, void* out, double dt, int slot) {
 void free_workspace(lg_ensemble* e) {
     for (void* p : e->ckpt) cudaFree(p);
     for (void* p : e->seg) cudaFree(p);
+    for (void* p : e->res) cudaFree(p);
     e->ckpt.clear();
     e->seg.clear();
+    e->res.clear();
     for (void*& p : e->adj) {
         cudaFree(p);
         p = nullptr;
@@ -425,9 +429,21 @@ int lg_ensemble_value_and_grad(lg_ensemble* e, double dt, int64_t nsteps, int64_
     const int64_t nseg = (nsteps + K - 1) / K;
     const lg::adj::Geo geo = geo_of(e);
     const int64_t cells = e->ninst * e->N0 * e->N1;
-    // workspace: nseg checkpoints, K - 1 recomputed states, two cotangent buffers
-    int rc = alloc_states(e, e->ckpt, (size_t)nseg);
-    if (rc == LG_OK) rc = alloc_states(e, e->seg, (size_t)std::max<int64_t>(K - 1, 0));
+    // resident tail: the last segments whose every state fits in the budget
+    // keep them from the forward pass and skip their recomputation
+    int64_t nres = 0, used = 0;
+    for (int64_t s = nseg - 1; s >= 0; --s) {
+        const int64_t len = std::min(K, nsteps - s * K);
+        if ((uint64_t)(used + len) * (uint64_t)state_bytes(e) > e->res_budget) break;
+        used += len;
+        ++nres;
+    }
+    const int64_t first_res = nseg - nres, n_res0 = first_res * K;
+    // workspace: a checkpoint per recomputed segment, K - 1 recomputed
+    // states, the resident states, two cotangent buffers
+    int rc = alloc_states(e, e->ckpt, (size_t)first_res);
+    if (rc == LG_OK) rc = alloc_states(e, e->seg, (size_t)(first_res > 0 ? std::max<int64_t>(K - 1, 0) : 0));
+    if (rc == LG_OK) rc = alloc_states(e, e->res, (size_t)used);
     if (rc != LG_OK) return rc;
     const int64_t acc_n = 3 * lg::adj::adjoint_items(kind, e->adj_kernel, geo), loss_n = lg::adj::loss_items(geo);
     if (!e->adj[0]) {
@@ -446,19 +462,30 @@ int lg_ensemble_value_and_grad(lg_ensemble* e, double dt, int64_t nsteps, int64_
     ENS_CUDA(e, cudaMemsetAsync(e->d_acc, 0, acc_n * sizeof(double), st));
     for (void* q : e->adj) ENS_CUDA(e, cudaMemsetAsync(q, 0, state_bytes(e), st));
 
-    // forward pass with checkpoints; the times of the segment starts are kept
+    // forward pass: checkpoints of the recomputed segments; the resident
+    // segments' states are written in place (x_n in res[n - n_res0])
     std::vector<double> tseg((size_t)nseg);
     ENS_CUDA(e, cudaMemcpyAsync(e->d_t + e->tslot, &e->t, sizeof(double), cudaMemcpyHostToDevice, st));
     ENS_CUDA(e, cudaStreamSynchronize(st));
     for (int64_t n = 0; n < nsteps; ++n) {
-        if (n % K == 0) {
-            tseg[(size_t)(n / K)] = e->t;
-            ENS_CUDA(e, cudaMemcpyAsync(e->ckpt[(size_t)(n / K)], e->state[e->cur], state_bytes(e),
-                                        cudaMemcpyDeviceToDevice, st));
+        if (n % K == 0) tseg[(size_t)(n / K)] = e->t;
+        if (n < n_res0) {
+            if (n % K == 0)
+                ENS_CUDA(e, cudaMemcpyAsync(e->ckpt[(size_t)(n / K)], e->state[e->cur], state_bytes(e),
+                                            cudaMemcpyDeviceToDevice, st));
+            rc = step_once(e, e->state[e->cur], e->state[e->cur ^ 1], dt, e->tslot);
+            if (rc != LG_OK) return rc;
+            e->cur ^= 1;
+        } else {
+            const int64_t i = n - n_res0;
+            if (i == 0)
+                ENS_CUDA(e, cudaMemcpyAsync(e->res[0], e->state[e->cur], state_bytes(e), cudaMemcpyDeviceToDevice,
+                                            st));
+            const bool last = i + 1 == used;
+            rc = step_once(e, e->res[(size_t)i], last ? e->state[e->cur ^ 1] : e->res[(size_t)(i + 1)], dt, e->tslot);
+            if (rc != LG_OK) return rc;
+            if (last) e->cur ^= 1;
         }
-        rc = step_once(e, e->state[e->cur], e->state[e->cur ^ 1], dt, e->tslot);
-        if (rc != LG_OK) return rc;
-        e->cur ^= 1;
         e->tslot ^= 1;
         e->t += dt;
         e->step_index += 1;
@@ -471,6 +498,16 @@ int lg_ensemble_value_and_grad(lg_ensemble* e, double dt, int64_t nsteps, int64_
     double t_start = 0.0;
     for (int64_t s = nseg - 1; s >= 0; --s) {
         const int64_t len = std::min(K, nsteps - s * K);
+        if (s >= first_res) {  // resident: x_{sK+i} is res[sK + i - n_res0]
+            for (int64_t i = len - 1; i >= 0; --i) {
+                const void* x = e->res[(size_t)(s * K + i - n_res0)];
+                ENS_CUDA(e, lg::adj::launch_adjoint_step(kind, e->adj_kernel, x, e->adj[a], e->adj[a ^ 1],
+                                                         e->d_adj_params, geo, dt, e->d_acc, st));
+                lg::abi_count_launch(e->ctx, 1);
+                a ^= 1;
+            }
+            continue;
+        }
         t_start = tseg[(size_t)s];
         ENS_CUDA(e, cudaMemcpyAsync(e->d_t, &t_start, sizeof(double), cudaMemcpyHostToDevice, st));
         ENS_CUDA(e, cudaStreamSynchronize(st));  // the host scalar is rewritten for the next segment
@@ -483,8 +520,8 @@ int lg_ensemble_value_and_grad(lg_ensemble* e, double dt, int64_t nsteps, int64_
         }
         for (int64_t i = len - 1; i >= 0; --i) {
             const void* x = i == 0 ? e->ckpt[(size_t)s] : e->seg[(size_t)(i - 1)];
-            ENS_CUDA(e, lg::adj::launch_adjoint_step(kind, e->adj_kernel, x, e->adj[a], e->adj[a ^ 1], e->d_adj_params, geo, dt,
-                                                     e->d_acc, st));
+            ENS_CUDA(e, lg::adj::launch_adjoint_step(kind, e->adj_kernel, x, e->adj[a], e->adj[a ^ 1],
+                                                     e->d_adj_params, geo, dt, e->d_acc, st));
             lg::abi_count_launch(e->ctx, 1);
             a ^= 1;
         }
@@ -521,6 +558,16 @@ int lg_ensemble_value_and_grad(lg_ensemble* e, double dt, int64_t nsteps, int64_
         grad_params[4 * i + 1] = g1;
         grad_params[4 * i + 2] = g2;
         grad_params[4 * i + 3] = gd;
+    }
+    return LG_OK;
+}
+
+int lg_ensemble_set_resident_budget(lg_ensemble* e, uint64_t bytes) {
+    if (!e) return LG_ERR_INVALID;
+    e->res_budget = bytes;
+    if (bytes == 0) {  // give the resident states back
+        for (void* p : e->res) cudaFree(p);
+        e->res.clear();
     }
     return LG_OK;
 }

@@ -87,14 +87,18 @@ class Ensemble:
     ADJOINT_KERNELS = {"strip": 0, "tile": 1}
 
     def value_and_grad(self, dt: float, nsteps: int, ckpt_every: int, target, cell_grads: bool = True,
-                       kernel: str = "strip") -> dict:
+                       kernel: str = "strip", resident_bytes: int = 0) -> dict:
         """Loss and gradients of every instance (see the module docstring); the
         state is left at the final step.  ``kernel`` picks the form of the
         step adjoint: "strip" (warps walking up the rows) or "tile"
-        (shared-memory tiles); they agree up to rounding."""
+        (shared-memory tiles); they agree up to rounding.  With
+        ``resident_bytes`` > 0 the last segments whose states fit in that many
+        device bytes keep them from the forward pass instead of recomputing
+        them (same results, less work)."""
         if kernel not in self.ADJOINT_KERNELS:
             raise ValueError("kernel is 'strip' or 'tile'")
         N.check(N.lib.lg_ensemble_set_adjoint_kernel(self.handle, self.ADJOINT_KERNELS[kernel]), self.scheduler.handle)
+        N.check(N.lib.lg_ensemble_set_resident_budget(self.handle, int(resident_bytes)), self.scheduler.handle)
         tgt = np.ascontiguousarray(np.broadcast_to(target, self.shape), dtype=np.float64)
         loss = np.empty(self.ninst)
         gp = np.empty((self.ninst, 4))

@@ -219,3 +219,26 @@ def test_strip_and_tile_adjoints_agree(sched, dtype, rel, cells, block, ninst):
         assert np.allclose(b[k], a[k], rtol=rel, atol=rel * np.abs(a[k]).max()), k
     for k in ("phi0", "u0"):
         assert np.linalg.norm(b[k] - a[k]) <= rel * np.linalg.norm(a[k]), k
+
+
+@pytest.mark.parametrize("dtype", ["f64", "f32"])
+def test_resident_tail_gives_the_same_bits(sched, dtype):
+    # keeping the last segments' states instead of recomputing them changes
+    # no bit of the loss, the gradients or the final state, whether some or
+    # all segments stay
+    steps, ckpt = 11, 3  # segments of 3, 3, 3 and 2 steps
+    state_bytes = 2 * 2 * (BLOCK + 2) ** 2 * (N_ // BLOCK) ** 2 * (8 if dtype == "f64" else 4)
+    out = []
+    for states in (0, 2, 5, steps):
+        ens = make(sched, N_, BLOCK, EPS4, SEEDS, NOISE, dtype=dtype)
+        ens.set("phi", seeds_field(2, N_))
+        ens.set("u", -np.asarray(DELTA)[:, None, None] * np.ones((2, N_, N_)))
+        g = ens.value_and_grad(DT, steps, ckpt, seeds_field(2, N_) * 0.5, resident_bytes=states * state_bytes)
+        g["phi_T"] = ens.get("phi")
+        g["time"] = ens.time()
+        ens._destroy()
+        out.append(g)
+    for g in out[1:]:
+        for k in ("loss", "lambda", "d_thermal", "eps4", "delta", "phi0", "u0", "phi_T"):
+            assert np.array_equal(g[k], out[0][k]), k
+        assert g["time"] == out[0]["time"]
