@@ -284,6 +284,42 @@ int lg_ensemble_set_adjoint_kernel(lg_ensemble* e, int kernel);
  * 0, the default, is pure checkpointing; 0 also frees the kept states. */
 int lg_ensemble_set_resident_budget(lg_ensemble* e, uint64_t bytes);
 
+/* ---- Observation: snapshots off the stepping stream --------------------
+ * The device side of AsyncObserver (src/core/observer.rs:65-165): a ring of
+ * `nslots` snapshot slots of a state, each a device buffer and a pinned host
+ * buffer holding the interior cells of the chosen fields (1 to 8) in the row
+ * order of the reference's Parquet snapshots (src/io/parquet.rs:150-215):
+ * blocks in order, each block's interior cells dimension-0-fastest, one
+ * column of `rows` FP64 values per field (FP32 states are widened).
+ *
+ * lg_snapshot_ring_capture gathers the state as it stands after the work
+ * already enqueued on the state's stream into a free slot (one kernel on
+ * that stream) and copies the slot to the host on a stream of the ring's own
+ * after an event, so the stepping stream never waits for the host.  With no
+ * free slot it drops the snapshot and sets *slot = -1, as the reference's
+ * observer drops rather than blocks (observer.rs:17-25, 149-156).
+ * lg_snapshot_ring_poll hands out the oldest captured snapshot whose copy
+ * has finished, waiting up to timeout_ms (0: just look; LG_ERR_TIMEOUT if
+ * none); the caller reads `columns` (nfields x rows doubles) and gives the
+ * slot back with lg_snapshot_ring_release.  capture runs on the thread that
+ * steps the state; poll and release may run on another thread.  The state
+ * must outlive the ring. */
+typedef struct lg_snapshot_ring lg_snapshot_ring;
+int lg_snapshot_ring_create(lg_state* st, const int* fields, int nfields, int nslots, lg_snapshot_ring** out);
+int lg_snapshot_ring_destroy(lg_snapshot_ring* r);
+int lg_snapshot_ring_capture(lg_snapshot_ring* r, int64_t step, double t, int64_t epoch, int* slot);
+int lg_snapshot_ring_poll(lg_snapshot_ring* r, int timeout_ms, int* slot, int64_t* step, double* t, int64_t* epoch,
+                          const double** columns);
+int lg_snapshot_ring_release(lg_snapshot_ring* r, int slot);
+int lg_snapshot_ring_stats(lg_snapshot_ring* r, int64_t* captured, int64_t* dropped, int64_t* rows);
+/* Cell centres of a Cartesian grid in the same row order, one column of
+ * cells[0] x ... x cells[D-1] values per dimension: (block origin cell +
+ * index + 0.5) * spacing + origin as one fused multiply-add, the reference's
+ * cell_center (src/geometry/cartesian.rs:589-597).  Host only: it needs no
+ * device and no context. */
+int lg_cell_centers(int D, const int64_t* cells, const int64_t* block_cells, const double* origin,
+                    const double* spacing, double* out);
+
 /* Standard normals of n keys on the device (`rng::standard_normal`,
  * src/util/rng.rs:43-49); host arrays in and out. */
 int lg_standard_normal(lg_ctx* ctx, const uint64_t* keys, int64_t n, double* out);

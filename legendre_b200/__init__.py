@@ -9,12 +9,14 @@ from .geometry import CartesianGrid, GridError
 from .integrators import EulerMaruyama, FiniteDifference, FiniteVolume, ForwardEuler
 from .physics import A1, A2, Grain, Heat, ModelC, seed_positions
 from .ensemble import Ensemble
+from .observe import AsyncObserver, ParquetObserver, Snapshot, cell_centers
 from .amr import (AmrGrid, AmrSimulation, BergerOliger, CellBox, ClusterParams, GradientTagger, RegridPolicy,
                   Subcycling)
 
 __all__ = [
     "AmrGrid", "AmrSimulation", "BergerOliger", "CellBox", "ClusterParams", "GradientTagger", "RegridPolicy",
     "Subcycling",
+    "AsyncObserver", "ParquetObserver", "Snapshot", "cell_centers",
     "A1", "A2", "CartesianGrid", "CudaAllocator", "CudaScheduler", "DeviceState", "Ensemble", "EulerMaruyama",
     "FieldSpec",
     "FiniteDifference", "FiniteVolume", "ForwardEuler", "Grain", "GridError", "Heat", "LegendreError", "ModelC",

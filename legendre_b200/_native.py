@@ -136,6 +136,13 @@ _SIGS = {
     "lg_ensemble_value_and_grad": (C.c_int, [_p, _d, _i64, _i64, _pd, _pd, _pd, _pd, _pd]),
     "lg_ensemble_set_adjoint_kernel": (C.c_int, [_p, C.c_int]),
     "lg_ensemble_set_resident_budget": (C.c_int, [_p, C.c_uint64]),
+    "lg_snapshot_ring_create": (C.c_int, [_p, C.POINTER(C.c_int), C.c_int, C.c_int, C.POINTER(_p)]),
+    "lg_snapshot_ring_destroy": (C.c_int, [_p]),
+    "lg_snapshot_ring_capture": (C.c_int, [_p, _i64, _d, _i64, C.POINTER(C.c_int)]),
+    "lg_snapshot_ring_poll": (C.c_int, [_p, C.c_int, C.POINTER(C.c_int), _pi64, _pd, _pi64, C.POINTER(_pd)]),
+    "lg_snapshot_ring_release": (C.c_int, [_p, C.c_int]),
+    "lg_snapshot_ring_stats": (C.c_int, [_p, _pi64, _pi64, _pi64]),
+    "lg_cell_centers": (C.c_int, [C.c_int, _pi64, _pi64, _pd, _pd, _pd]),
     "lg_amr_tag_level_static": (C.c_int, [_p, C.c_int, C.c_int, _d, _pi64, _i64, _pi64]),
 }
 

@@ -39,6 +39,7 @@ SOURCES = [
     ("lg_amr.cu", ["-fmad=false"]),
     ("lg_adjoint.cu", []),      # not bit-matched to anything: contraction allowed
     ("lg_ensemble.cu", ["-fmad=false"]),
+    ("lg_observe.cu", ["-fmad=false"]),
 ]
 
 

@@ -234,6 +234,7 @@ class Simulation:
         self.alloc = alloc
         self.state = builder.build(grid, scheduler, alloc)
         integrator.validate(model, grid, disc)
+        self.observers = []
 
     def stable_dt(self) -> Optional[float]:
         return self.integrator.suggested_dt(self.model, self.grid)
@@ -247,8 +248,33 @@ class Simulation:
     def step(self, dt: float) -> None:
         self.run(dt, 1)
 
+    def add_observer(self, observer) -> None:
+        """Observers are called after the steps they fire on (step 1 and every
+        ``observer.every`` steps) with (step, t, epoch, grid, state), as
+        ``Simulation::step`` notifies them (simulation.rs:286-289)."""
+        self.observers.append(observer)
+
     def run(self, dt: float, nsteps: int, graph: bool = False, variant: int = 0) -> None:
-        self.integrator.run(self, float(dt), int(nsteps), graph=graph, variant=variant)
+        nsteps = int(nsteps)
+        if not self.observers:
+            self.integrator.run(self, float(dt), nsteps, graph=graph, variant=variant)
+            return
+        from .observe import fires
+
+        # run in stretches that end on the steps some observer fires on
+        done = 0
+        while done < nsteps:
+            k = self.step_index()
+            stop = nsteps - done
+            for s in range(1, stop + 1):
+                if any(fires(k + s, getattr(o, "every", 1)) for o in self.observers):
+                    stop = s
+                    break
+            self.integrator.run(self, float(dt), stop, graph=graph, variant=variant)
+            done += stop
+            step = self.step_index()
+            for o in self.observers:
+                o.observe(step, self.time(), 0, self.grid, self.state)
 
     def autotune(self, dt: float, trial_steps: int = 20):
         """Pick the fastest Model C step variant for this grid and precision by

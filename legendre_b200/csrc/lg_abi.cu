@@ -13,6 +13,7 @@
 #include <vector>
 
 #include "../../include/legendre_b200.h"
+#include "lg_state_view.h"
 #include "lg_kernels.h"
 
 struct lg_ctx {
@@ -204,6 +205,24 @@ void advance_time(lg_state* st, double dt, int64_t steps) {
 namespace lg {
 // context services for the other translation units of the library
 int abi_fail(lg_ctx* ctx, int code, const std::string& msg) { return fail(ctx, code, msg); }
+int abi_state_view(const lg_state* st, StateView* v) {
+    if (!st || !v) return LG_ERR_INVALID;
+    const lg_grid* g = st->grid;
+    v->ctx = st->ctx;
+    v->arena = st->arena[st->cur];
+    v->dtype = st->dtype;
+    v->esize = st->esize;
+    v->D = g->D;
+    v->nfields = st->nfields;
+    v->ghosts = st->ghosts.data();
+    v->slab_stride = st->slab_stride;
+    v->nblocks = g->nblocks;
+    for (int d = 0; d < 3; ++d) {
+        v->block[d] = g->block[d];
+        v->nb[d] = g->nb[d];
+    }
+    return LG_OK;
+}
 cudaStream_t abi_stream(lg_ctx* ctx) { return ctx->stream; }
 int abi_device(lg_ctx* ctx) { return ctx->device; }
 void abi_count_launch(lg_ctx* ctx, int64_t n) { ctx->launches += n; }

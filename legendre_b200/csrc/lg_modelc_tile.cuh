@@ -201,7 +201,6 @@ __global__ void __launch_bounds__(256, MINB)
     modelc_strip_kernel(const T* __restrict__ in, T* __restrict__ out, TileArgs g, typename Ops::Params m0, T dt,
                         T scale_amp, BatchArgs bt) {
     constexpr bool FULL = NX > 0 && NX % 32 == 0;
-    constexpr int NB = PF + 3;  // window rows: j-1, j, j+1 and PF rows of prefetch
     const CartTopo& topo = g.topo;
     const int n0 = NX > 0 ? NX : topo.n[0];
     const int n1 = topo.n[1];

@@ -1,0 +1,151 @@
+"""Snapshots through the device ring (AsyncObserver) on a GPU.
+
+* Every snapshot equals the state of a twin run at its step, bit for bit
+  (FP64, FP32 widened to FP64, 2-D Model C and 3-D heat), with step and time.
+* When the sink falls behind, snapshots are dropped and counted; the run
+  itself is unchanged bit for bit, and the snapshots that did go through are
+  the right ones.
+* Parquet files written behind the ring equal those of the synchronous
+  observer.
+"""
+import threading
+
+import numpy as np
+import pyarrow.parquet as pq
+import pytest
+
+import legendre_b200 as L
+from util import with_ghosts
+
+pytestmark = pytest.mark.gpu
+
+H = 0.4
+
+
+def modelc_sim(sched, dtype="f64", noise=0.02, cells=(64, 96), block=(32, 32), seed=3):
+    grid = L.CartesianGrid(list(cells), list(block), [0.0, 0.0], [H, H])
+    model = L.ModelC(0.05, 3.19, noise)
+    model.d_thermal = 2.0
+    sim = L.Simulation(grid, L.FiniteVolume(), model, L.EulerMaruyama(seed), sched, L.CudaAllocator(dtype))
+    init = sim if dtype == "f64" else L.Simulation(grid, L.FiniteVolume(), model, L.EulerMaruyama(seed), sched,
+                                                   L.CudaAllocator("f64"))
+    model.initialize_grains(grid, init.state, [L.Grain((cells[0] * H / 2, cells[1] * H / 2), 4.0)], 0.55)
+    if init is not sim:  # FP32: a cast copy of the FP64 initial state
+        for f in ("phi", "u"):
+            sim.state.upload(f, init.state.download(f).astype(np.float32))
+    return sim
+
+
+def heat_sim(sched, cells=(12, 8, 16), block=(4, 4, 8)):
+    grid = L.CartesianGrid(list(cells), list(block), [0.0] * 3, [0.1] * 3).with_periodic([True, False, True])
+    sim = L.Simulation(grid, L.FiniteDifference(), L.Heat(0.7), L.ForwardEuler(), sched, L.CudaAllocator("f64"))
+    rng = np.random.default_rng(5)
+    sim.state.upload("u", with_ghosts(rng.standard_normal((grid.num_blocks(),) + tuple(reversed(block))), 1))
+    return sim
+
+
+class Collect:
+    def __init__(self, gate=None):
+        self.snaps, self.finished, self.gate = [], False, gate
+
+    def consume(self, s):
+        if self.gate is not None:
+            self.gate.wait(30.0)
+        self.snaps.append((s.step, s.t, s.epoch, {k: v.copy() for k, v in s.columns.items()}))
+
+    def finish(self):
+        self.finished = True
+
+
+def twin_states(make, dt, steps, names):
+    """{step: (t, {name: interior in row order})} of a run without observers."""
+    sim = make()
+    out = {}
+    for k in range(1, steps + 1):
+        sim.run(dt, 1)
+        out[k] = (sim.time(), {n: sim.state.interior(f).astype(np.float64).reshape(-1) for n, f in names})
+    return sim, out
+
+
+@pytest.mark.parametrize("dtype", ["f64", "f32"])
+def test_snapshots_equal_the_state_at_their_steps(sched, dtype):
+    names = [("phi", "phi"), ("u", "u")]
+    make = lambda: modelc_sim(sched, dtype)
+    dt = 0.01
+    _, ref = twin_states(make, dt, 23, names)
+    sim = make()
+    sink = Collect()
+    obs = L.AsyncObserver(every=5, nslots=8, sinks=[sink], fields=names)
+    sim.add_observer(obs)
+    sim.run(dt, 23, graph=True)
+    obs.close()
+    assert sink.finished
+    assert [s[0] for s in sink.snaps] == [1, 5, 10, 15, 20]
+    assert obs.dropped_snapshots == 0
+    for step, t, epoch, cols in sink.snaps:
+        assert t == ref[step][0] and epoch == 0
+        for n, _ in names:
+            assert np.array_equal(cols[n], ref[step][1][n]), (step, n)
+
+
+def test_three_dimensional_snapshots(sched):
+    names = [("u", "u")]
+    make = lambda: heat_sim(sched)
+    dt = 0.15 * 0.01 / 0.7
+    _, ref = twin_states(make, dt, 9, names)
+    sim = make()
+    sink = Collect()
+    obs = L.AsyncObserver(every=3, nslots=4, sinks=[sink], fields=names)
+    sim.add_observer(obs)
+    sim.run(dt, 9)
+    obs.close()
+    assert [s[0] for s in sink.snaps] == [1, 3, 6, 9]
+    for step, t, _, cols in sink.snaps:
+        assert np.array_equal(cols["u"], ref[step][1]["u"])
+
+
+def test_a_slow_sink_drops_snapshots_not_steps(sched):
+    names = [("phi", "phi")]
+    make = lambda: modelc_sim(sched)
+    dt = 0.01
+    plain, ref = twin_states(make, dt, 40, names)
+    sim = make()
+    gate = threading.Event()
+    sink = Collect(gate)
+    obs = L.AsyncObserver(every=2, nslots=2, sinks=[sink], fields=names)
+    sim.add_observer(obs)
+    sim.run(dt, 40)
+    sched.sync()
+    gate.set()
+    obs.close()
+    captured, dropped = len(sink.snaps), None
+    fired = [1] + list(range(2, 41, 2))
+    assert captured >= 1 and captured < len(fired)
+    dropped = len(fired) - captured
+    steps = [s[0] for s in sink.snaps]
+    assert steps == sorted(steps) and set(steps) <= set(fired)
+    for step, t, _, cols in sink.snaps:
+        assert np.array_equal(cols["phi"], ref[step][1]["phi"])
+    assert dropped > 0
+    for f in ("phi", "u"):
+        assert np.array_equal(sim.state.download(f), plain.state.download(f))
+
+
+def test_parquet_behind_the_ring_equals_the_synchronous_writer(sched, tmp_path):
+    names = [("phi", "phi"), ("u", "u")]
+    dt = 0.01
+    a = modelc_sim(sched)
+    pa_ = L.ParquetObserver(a.grid, names, 1, tmp_path / "async")
+    obs = L.AsyncObserver(every=4, nslots=6, sinks=[pa_], fields=names)
+    a.add_observer(obs)
+    a.run(dt, 13, graph=True)
+    obs.close()
+    b = modelc_sim(sched)
+    b.add_observer(L.ParquetObserver(b.grid, names, 4, tmp_path / "sync"))
+    b.run(dt, 13)
+    files = sorted(p.name for p in (tmp_path / "sync").iterdir())
+    assert files == ["snap_0000001.parquet", "snap_0000004.parquet", "snap_0000008.parquet",
+                     "snap_0000012.parquet", "static_0000000.parquet"]
+    assert sorted(p.name for p in (tmp_path / "async").iterdir()) == files
+    for name in files:
+        assert pq.read_table(tmp_path / "async" / name).equals(pq.read_table(tmp_path / "sync" / name)), name
