@@ -584,6 +584,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cells", type=int, default=None, help="override the grid's cells per dimension (small cases)")
     ap.add_argument("--instances", type=int, default=None, help="override the ensemble's instance count")
+    ap.add_argument("--observe-every", type=int, default=0,
+                    help="also time the run with an AsyncObserver snapshotting phi and u every N steps")
     args = ap.parse_args()
     args.dtype_given = any(a == "--dtype" or a.startswith("--dtype=") for a in sys.argv[1:])
     args.warmup = max(args.warmup, 3)
@@ -679,6 +681,45 @@ def main():
            "what": f"lg_state_upload_field x2 from pinned host + {args.steps} steps + lg_state_download_field x2, "
                    "bytes amortised per step"}
 
+    # observed: the same K steps with an AsyncObserver taking snapshots of
+    # phi and u every N steps into a 3-slot ring; its sink reduces each one on
+    # the host (mean phi, solid fraction) while the device keeps stepping
+    observed = None
+    if args.observe_every > 0:
+        class StatsSink:
+            def __init__(self):
+                self.rows = []
+
+            def consume(self, snap):
+                phi = snap.columns["phi"]
+                self.rows.append((snap.step, float(phi.mean()), float((phi > 0).mean())))
+
+            def finish(self):
+                pass
+
+        sink = StatsSink()
+        obs = L.AsyncObserver(every=args.observe_every, nslots=3, sinks=[sink], fields=[("phi", "phi"), ("u", "u")])
+        sim.add_observer(obs)
+        sim.run(dt, args.observe_every, graph=True, variant=args.variant)  # binds the ring, warms the graphs
+        torch.cuda.synchronize()
+        barrier(pg)
+        e4 = torch.cuda.Event(enable_timing=True)
+        e5 = torch.cuda.Event(enable_timing=True)
+        e4.record(stream)
+        sim.run(dt, args.steps, graph=True, variant=args.variant)
+        e5.record(stream)
+        torch.cuda.synchronize()
+        ms_obs = max_over_ranks(pg, e4.elapsed_time(e5))
+        captured, dropped = obs.stats()
+        obs.close()
+        sim.observers.clear()
+        observed = {"every": args.observe_every, "slots": 3,
+                    "value": world * cells * args.steps / (ms_obs / 1e3) / 1e9, "unit": "Gcell-updates/s",
+                    "slowdown": ms_obs / ms - 1.0, "captured": captured, "dropped": dropped,
+                    "snapshot_bytes": 2 * cells * 8,
+                    "what": "device-timed K steps with the observer attached (gather kernel on the stepping "
+                            "stream, copy on the ring's stream, a host thread reducing each snapshot)"}
+
     if rank == 0:
         peak, peak_kind = peaks()
         algo = BYTES_PER_CELL[args.dtype] * cells
@@ -706,6 +747,7 @@ def main():
             "cpu_baseline": cpu,
             "e2e": e2e,
             "fp32_error": err,
+            "observer": observed,
             "gpu_launches": launches,
             "clocks": {"sm_mhz": clk["sm_mhz"], "sm_max_mhz": clk["sm_max_mhz"], "reasons": clk["reasons"],
                        "samples": clk["samples"]},

@@ -295,9 +295,13 @@ int lg_ensemble_set_resident_budget(lg_ensemble* e, uint64_t bytes);
  * lg_snapshot_ring_capture gathers the state as it stands after the work
  * already enqueued on the state's stream into a free slot (one kernel on
  * that stream) and copies the slot to the host on a stream of the ring's own
- * after an event, so the stepping stream never waits for the host.  With no
- * free slot it drops the snapshot and sets *slot = -1, as the reference's
- * observer drops rather than blocks (observer.rs:17-25, 149-156).
+ * after an event, so the stepping stream never waits for the host.  The
+ * calling thread first waits until the device has gathered the previous
+ * capture, so it runs at most one snapshot interval ahead of the device while
+ * the device keeps the work already enqueued.  With no free slot (the
+ * consumer has not finished with the earlier snapshots) it drops the
+ * snapshot and sets *slot = -1, as the reference's observer drops rather
+ * than blocks (observer.rs:17-25, 149-156).
  * lg_snapshot_ring_poll hands out the oldest captured snapshot whose copy
  * has finished, waiting up to timeout_ms (0: just look; LG_ERR_TIMEOUT if
  * none); the caller reads `columns` (nfields x rows doubles) and gives the

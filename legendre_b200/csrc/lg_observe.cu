@@ -8,7 +8,8 @@
 // field).  capture() gathers the current state into a free slot's device
 // buffer with one kernel on the state's stream, then copies it to the host
 // buffer on the ring's own stream after an event, so the stepping stream
-// never waits for the host.  A slot goes FREE -> IN_FLIGHT (capture) ->
+// never waits for the host (the host waits, at each capture, until the
+// device has reached the previous one).  A slot goes FREE -> IN_FLIGHT (capture) ->
 // HELD (poll, once its copy has finished) -> FREE (release).  With no free
 // slot the snapshot is dropped and counted, as the reference drops a
 // snapshot rather than block the solver (observer.rs:17-25, 149-156).
@@ -76,6 +77,7 @@ struct lg_snapshot_ring {
     std::vector<int64_t> step, epoch;
     std::vector<double> t;
     uint64_t next_seq = 0;
+    int last = -1;  // slot of the latest capture
     int64_t captured = 0, dropped = 0;
     std::mutex mu;
 };
@@ -161,6 +163,20 @@ int lg_snapshot_ring_destroy(lg_snapshot_ring* r) {
 int lg_snapshot_ring_capture(lg_snapshot_ring* r, int64_t step, double t, int64_t epoch, int* slot) {
     if (!r || !slot) return LG_ERR_INVALID;
     *slot = -1;
+    // pace the host: wait until the device has gathered the previous
+    // snapshot, so the caller runs at most one snapshot interval ahead of
+    // the device and a full ring means the consumer is behind (the device
+    // keeps the steps already enqueued)
+    cudaEvent_t prev = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(r->mu);
+        if (r->last >= 0) prev = r->packed[r->last];
+    }
+    if (prev) {
+        cudaSetDevice(r->device);
+        const cudaError_t w = cudaEventSynchronize(prev);
+        if (w != cudaSuccess) return rfail(r, LG_ERR_CUDA, std::string("snapshot pacing: ") + cudaGetErrorString(w));
+    }
     std::lock_guard<std::mutex> lock(r->mu);
     int i = 0;
     while (i < r->nslots && r->status[i] != kFree) ++i;
@@ -202,6 +218,7 @@ int lg_snapshot_ring_capture(lg_snapshot_ring* r, int64_t step, double t, int64_
     if (e == cudaSuccess) e = cudaEventRecord(r->copied[i], r->copy);
     if (e != cudaSuccess) return rfail(r, LG_ERR_CUDA, std::string("snapshot capture: ") + cudaGetErrorString(e));
     r->status[i] = kInFlight;
+    r->last = i;
     r->seq[i] = r->next_seq++;
     r->step[i] = step;
     r->t[i] = t;
