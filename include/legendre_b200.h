@@ -157,6 +157,19 @@ int lg_modelc_autotune(lg_state* st, const lg_modelc_params* p, double dt, uint6
  * uploaded.  `ModelC::initialize_grains` without orientations
  * (phasefield.rs:227-314): grains = n x (cx, cy, radius, orientation). */
 int lg_modelc_initialize_grains(lg_state* st, const double* grains, int64_t n, double u0);
+/* Multi-grain Model C (ModelC::with_orientations, phasefield.rs:118-125):
+ * theta0 is a static field of ghost width 0 beyond phi and u.
+ * lg_modelc_set_orientations takes theta0 from field `theta_field` of the
+ * state (copying it into both step buffers) and computes cos and sin theta0
+ * of every cell on the host, as the reference's sin_cos; from then on
+ * lg_modelc_em_run steps the oriented form, each cell's four faces with
+ * their anisotropy in its crystal frame (finite_volume.rs:178-235).  A
+ * negative theta_field returns to the axis-aligned step.
+ * lg_modelc_initialize_orientations writes theta0 by the nearest-seed
+ * Voronoi rule of initialize_grains (phasefield.rs:286-311; grains as x, y,
+ * radius, orientation) and sets it. */
+int lg_modelc_set_orientations(lg_state* st, int theta_field);
+int lg_modelc_initialize_orientations(lg_state* st, int theta_field, const double* grains, int64_t n);
 /* Heat initial condition of the 96^3 benchmark: sin(2 pi x) sin(2 pi y)
  * sin(2 pi z) + amp * (2 * unit_open(mix_key(seed, [gx, gy, gz])) - 1) at
  * cell centres (gx.. = global cell index); the reference has no such

@@ -109,6 +109,8 @@ _SIGS = {
     "lg_modelc_em_run": (C.c_int, [_p, C.POINTER(ModelCParams), _d, _u64, _i64, C.c_int, C.c_uint32]),
     "lg_modelc_autotune": (C.c_int, [_p, C.POINTER(ModelCParams), _d, _u64, C.c_int, C.POINTER(C.c_int), _pd]),
     "lg_modelc_initialize_grains": (C.c_int, [_p, _pd, _i64, _d]),
+    "lg_modelc_set_orientations": (C.c_int, [_p, C.c_int]),
+    "lg_modelc_initialize_orientations": (C.c_int, [_p, C.c_int, _pd, _i64]),
     "lg_heat_initialize_sine_noise": (C.c_int, [_p, C.c_int, _u64, _d]),
     "lg_standard_normal": (C.c_int, [_p, C.POINTER(C.c_uint64), _i64, _pd]),
     "lg_amr_sim_create": (C.c_int, [_p, _pi64, _pi64, _pd, _pd, C.POINTER(C.c_uint32), C.c_int, _pi64, _i64, C.c_int,

@@ -7,6 +7,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <limits>
 #include <map>
 #include <string>
 #include <thread>
@@ -59,6 +60,10 @@ struct lg_state {
     int64_t step_index = 0;
     bool ghosts_valid = false;
     std::map<std::string, GraphEntry> graphs;
+    // multi-grain Model C: the theta0 field and cos/sin theta0 of every
+    // interior cell on the device (cos block-major, then sin), state dtype
+    int theta_field = -1;
+    void* orient = nullptr;
 };
 
 namespace {
@@ -417,6 +422,7 @@ int lg_state_destroy(lg_state* st) {
     cudaFree(st->arena[0]);
     cudaFree(st->arena[1]);
     cudaFree(st->d_t);
+    cudaFree(st->orient);
     delete st;
     return LG_OK;
 }
@@ -572,8 +578,10 @@ int lg_modelc_em_run(lg_state* st, const lg_modelc_params* p, double dt, uint64_
         if (it != ctx->tuned.end()) variant = it->second;
     }
     char key[512];
-    snprintf(key, sizeof key, "modelc|%a|%a|%a|%a|%a|%a|dt=%a|seed=%llu|v=%d", p->eps4, p->lambda, p->d_thermal,
-             p->noise_amplitude, p->anisotropy_tol, p->flux_tol, dt, (unsigned long long)seed, variant);
+    snprintf(key, sizeof key, "modelc|%a|%a|%a|%a|%a|%a|dt=%a|seed=%llu|v=%d|orient=%p", p->eps4, p->lambda,
+             p->d_thermal, p->noise_amplitude, p->anisotropy_tol, p->flux_tol, dt, (unsigned long long)seed, variant,
+             st->orient);
+    const int64_t ncells = st->grid->nblocks * st->grid->block[0] * st->grid->block[1];
     // variant = kind + 1000 * rows: kind 0 library default, 1 one thread per
     // cell in reference order, 2/3/4 warp strips with 2/3/4 CTAs per SM;
     // rows fixes the strip height
@@ -585,7 +593,15 @@ int lg_modelc_em_run(lg_state* st, const lg_modelc_params* p, double dt, uint64_
         cudaError_t e;
         const void* in = st->arena[st->cur];
         void* out = st->arena[st->cur ^ 1];
-        if (st->dtype == LG_F64)
+        if (st->orient)  // multi-grain: the oriented strip step, whatever the variant's kind
+            e = st->dtype == LG_F64
+                    ? lg::launch_modelc_oriented_f64(static_cast<const double*>(in), static_cast<double*>(out), topo,
+                                                     L, m, dt, nz, st->d_t, st->tslot,
+                                                     static_cast<const double*>(st->orient), ncells, rows, ctx->stream)
+                    : lg::launch_modelc_oriented_f32(static_cast<const float*>(in), static_cast<float*>(out), topo, L,
+                                                     m, dt, nz, st->d_t, st->tslot,
+                                                     static_cast<const float*>(st->orient), ncells, rows, ctx->stream);
+        else if (st->dtype == LG_F64)
             e = tile ? lg::launch_modelc_tile_f64(static_cast<const double*>(in), static_cast<double*>(out), topo, L,
                                                   m, dt, nz, st->d_t, st->tslot, rows, minb, ctx->stream)
                      : lg::launch_modelc_step_f64(static_cast<const double*>(in), static_cast<double*>(out), topo, L,
@@ -742,6 +758,138 @@ int lg_modelc_initialize_grains(lg_state* st, const double* grains, int64_t n, d
     int rc = lg_state_upload_field(st, 0, phi.data(), (int64_t)phi.size());
     if (rc != LG_OK) return rc;
     return lg_state_upload_field(st, 1, u.data(), (int64_t)u.size());
+}
+
+int lg_modelc_set_orientations(lg_state* st, int theta_field) {
+    if (!st) return LG_ERR_INVALID;
+    lg_ctx* ctx = st->ctx;
+    cudaSetDevice(ctx->device);
+    if (theta_field < 0) {  // back to the axis-aligned step
+        LG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+        cudaFree(st->orient);
+        st->orient = nullptr;
+        st->theta_field = -1;
+        return LG_OK;
+    }
+    const lg_grid* g = st->grid;
+    if (g->D != 2 || st->nfields < 3 || st->ghosts[0] != 1 || st->ghosts[1] != 1)
+        return fail(ctx, LG_ERR_STATE, "multi-grain Model C needs a 2-D state with phi, u and theta0");
+    if (theta_field < 2 || theta_field >= st->nfields || st->ghosts[theta_field] != 0)
+        return fail(ctx, LG_ERR_INVALID, "theta0 must be a field beyond phi and u with ghost width 0");
+    const int64_t bc = g->block[0] * g->block[1], ncells = g->nblocks * bc;
+    // theta0 of the current arena to the host, and into the other arena (the
+    // step writes phi and u only, so both buffers keep the static field)
+    const size_t pitch = (size_t)st->nfields * st->slab_stride * st->esize, width = (size_t)bc * st->esize;
+    const size_t off = (size_t)theta_field * st->slab_stride * st->esize;
+    std::vector<char> raw((size_t)ncells * st->esize);
+    const char* cur = static_cast<const char*>(st->arena[st->cur]) + off;
+    char* other = static_cast<char*>(st->arena[st->cur ^ 1]) + off;
+    LG_CUDA(ctx, cudaMemcpy2DAsync(raw.data(), width, cur, pitch, width, g->nblocks, cudaMemcpyDeviceToHost,
+                                   ctx->stream));
+    LG_CUDA(ctx, cudaMemcpy2DAsync(other, pitch, cur, pitch, width, g->nblocks, cudaMemcpyDeviceToDevice,
+                                   ctx->stream));
+    LG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    // (s0, c0) = theta0.sin_cos() on the host, as the reference evaluates it
+    // (phasefield.rs:383, finite_volume.rs:202)
+    const size_t tbytes = 2 * (size_t)ncells * st->esize;
+    std::vector<char> trig(tbytes);
+    for (int64_t k = 0; k < ncells; ++k) {
+        const double th = st->dtype == LG_F64 ? reinterpret_cast<const double*>(raw.data())[k]
+                                              : (double)reinterpret_cast<const float*>(raw.data())[k];
+        const double c0 = std::cos(th), s0 = std::sin(th);
+        if (st->dtype == LG_F64) {
+            reinterpret_cast<double*>(trig.data())[k] = c0;
+            reinterpret_cast<double*>(trig.data())[ncells + k] = s0;
+        } else {
+            reinterpret_cast<float*>(trig.data())[k] = (float)c0;
+            reinterpret_cast<float*>(trig.data())[ncells + k] = (float)s0;
+        }
+    }
+    cudaFree(st->orient);
+    st->orient = nullptr;
+    st->theta_field = -1;
+    LG_CUDA(ctx, cudaMalloc(&st->orient, tbytes));
+    LG_CUDA(ctx, cudaMemcpy(st->orient, trig.data(), tbytes, cudaMemcpyHostToDevice));
+    st->theta_field = theta_field;
+    return LG_OK;
+}
+
+int lg_modelc_initialize_orientations(lg_state* st, int theta_field, const double* grains, int64_t n) {
+    if (!st || (n > 0 && !grains)) return LG_ERR_INVALID;
+    lg_ctx* ctx = st->ctx;
+    const lg_grid* g = st->grid;
+    if (g->D != 2 || theta_field < 2 || theta_field >= st->nfields || st->ghosts[theta_field] != 0)
+        return fail(ctx, LG_ERR_INVALID, "theta0 must be a field beyond phi and u with ghost width 0");
+    const int64_t nx = g->block[0], ny = g->block[1], bc = nx * ny;
+    std::vector<double> theta((size_t)(bc * g->nblocks), 0.0);
+    auto center = [&](int64_t b, int64_t i, int64_t j, double* out) {
+        int64_t c0 = b % g->nb[0], c1 = b / g->nb[0];
+        out[0] = std::fma(((double)(c0 * nx) + (double)i) + 0.5, g->spacing[0], g->origin[0]);
+        out[1] = std::fma(((double)(c1 * ny) + (double)j) + 0.5, g->spacing[1], g->origin[1]);
+    };
+    // ModelC::initialize_grains, theta0 by nearest-seed Voronoi
+    // (phasefield.rs:286-311): per block the candidates are the grains whose
+    // box distance is at most the smallest farthest-corner distance; a cell
+    // takes the first candidate minimising fma(dy, dy, dx * dx)
+    auto work = [&](int64_t b0, int64_t b1) {
+        for (int64_t b = b0; b < b1; ++b) {
+            double hx = g->spacing[0], hy = g->spacing[1], c0[2], c1[2];
+            center(b, 0, 0, c0);
+            center(b, nx - 1, ny - 1, c1);
+            double lo[2] = {std::fma(0.5, -hx, c0[0]), std::fma(0.5, -hy, c0[1])};
+            double hi[2] = {std::fma(0.5, hx, c1[0]), std::fma(0.5, hy, c1[1])};
+            double threshold = std::numeric_limits<double>::max();
+            for (int64_t k = 0; k < n; ++k) {
+                double cx = grains[4 * k], cy = grains[4 * k + 1];
+                double dx = std::max(std::fabs(cx - lo[0]), std::fabs(cx - hi[0]));
+                double dy = std::max(std::fabs(cy - lo[1]), std::fabs(cy - hi[1]));
+                threshold = std::min(threshold, std::hypot(dx, dy));
+            }
+            std::vector<int64_t> cand;
+            for (int64_t k = 0; k < n; ++k) {
+                double cx = grains[4 * k], cy = grains[4 * k + 1];
+                double dx = std::max(std::max(lo[0] - cx, cx - hi[0]), 0.0);
+                double dy = std::max(std::max(lo[1] - cy, cy - hi[1]), 0.0);
+                if (std::hypot(dx, dy) <= threshold) cand.push_back(k);
+            }
+            double* th = theta.data() + b * bc;
+            for (int64_t j = 0; j < ny; ++j)
+                for (int64_t i = 0; i < nx; ++i) {
+                    double xy[2];
+                    center(b, i, j, xy);
+                    double best = 0.0, bd = 0.0;
+                    bool any = false;
+                    for (int64_t k : cand) {
+                        double dx = xy[0] - grains[4 * k], dy = xy[1] - grains[4 * k + 1];
+                        double d = std::fma(dy, dy, dx * dx);
+                        if (!any || d < bd) {
+                            any = true;
+                            bd = d;
+                            best = grains[4 * k + 3];
+                        }
+                    }
+                    th[i + j * nx] = any ? best : 0.0;
+                }
+        }
+    };
+    unsigned nt = std::max(1u, std::min(64u, std::thread::hardware_concurrency()));
+    if (g->nblocks < 4) nt = 1;
+    std::vector<std::thread> pool;
+    int64_t per = (g->nblocks + nt - 1) / nt;
+    for (unsigned k = 0; k < nt; ++k) {
+        int64_t b0 = k * per, b1 = std::min<int64_t>(g->nblocks, b0 + per);
+        if (b0 < b1) pool.emplace_back(work, b0, b1);
+    }
+    for (auto& t : pool) t.join();
+    int rc;
+    if (st->dtype == LG_F64) {
+        rc = lg_state_upload_field(st, theta_field, theta.data(), (int64_t)theta.size());
+    } else {
+        std::vector<float> tf(theta.begin(), theta.end());
+        rc = lg_state_upload_field(st, theta_field, tf.data(), (int64_t)tf.size());
+    }
+    if (rc != LG_OK) return rc;
+    return lg_modelc_set_orientations(st, theta_field);
 }
 
 int lg_heat_initialize_sine_noise(lg_state* st, int field, uint64_t seed, double amp) {

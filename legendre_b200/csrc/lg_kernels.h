@@ -69,6 +69,17 @@ cudaError_t launch_modelc_tile_f64(const double* in, double* out, const CartTopo
 cudaError_t launch_modelc_tile_f32(const float* in, float* out, const CartTopo& topo, const SlabLayout& L,
                                    const ModelCDev& m, double dt, const NoiseDev& nz, double* tdev, int slot,
                                    int rows, int minb, cudaStream_t s);
+// The multi-grain step (lg_modelc.cu, lg_modelc_f32.cu): the strip schedule
+// with every cell's four faces in its own crystal frame; `trig` holds cos
+// theta0 of the ncells interior cells (blocks in order, dimension 0 fastest)
+// then sin theta0, in the state's element type.  FP64 is bit-identical to
+// the reference's apply_oriented path.
+cudaError_t launch_modelc_oriented_f64(const double* in, double* out, const CartTopo& topo, const SlabLayout& L,
+                                       const ModelCDev& m, double dt, const NoiseDev& nz, double* tdev, int slot,
+                                       const double* trig, int64_t ncells, int rows, cudaStream_t s);
+cudaError_t launch_modelc_oriented_f32(const float* in, float* out, const CartTopo& topo, const SlabLayout& L,
+                                       const ModelCDev& m, double dt, const NoiseDev& nz, double* tdev, int slot,
+                                       const float* trig, int64_t ncells, int rows, cudaStream_t s);
 
 // Batched instances (an ensemble of independent grids of one geometry):
 // block b of the topology belongs to instance b / bpi, with the parameter

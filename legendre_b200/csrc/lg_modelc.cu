@@ -22,6 +22,17 @@ cudaError_t launch_modelc_tile_f64(const double* in, double* out, const CartTopo
     return launch_strip_ops<double, OpsExact<double>, false, 1>(in, out, g, mc, dt, scale_amp, minb, s);
 }
 
+cudaError_t launch_modelc_oriented_f64(const double* in, double* out, const CartTopo& topo, const SlabLayout& L,
+                                       const ModelCDev& m, double dt, const NoiseDev& nz, double* tdev, int slot,
+                                       const double* trig, int64_t ncells, int rows, cudaStream_t s) {
+    TileArgs g{topo, L, dt, nz.seed, tdev, slot, rows, 0, 0, 0};
+    const MC<double> mc = to_mc<double>(m);
+    const double scale_amp = std::sqrt(dt) * nz.amp;
+    const OrientArgs oa{trig, ncells};
+    if (nz.on) return launch_strip_oriented<double, OpsExact<double>, true, 2>(in, out, g, mc, dt, scale_amp, oa, s);
+    return launch_strip_oriented<double, OpsExact<double>, false, 2>(in, out, g, mc, dt, scale_amp, oa, s);
+}
+
 size_t modelc_record_size_f64() { return sizeof(MC<double>); }
 void modelc_record_f64(const ModelCDev& m, void* out) { *static_cast<MC<double>*>(out) = to_mc<double>(m); }
 

@@ -64,6 +64,14 @@ struct BatchArgs {
     int bpi;
 };
 
+// Multi-grain kernels (ORIENT): cos theta0 of every interior cell, blocks in
+// order and each block's cells dimension-0-fastest, followed by sin theta0
+// in the same order (ncells values each), in the kernel's element type.
+struct OrientArgs {
+    const void* trig;
+    int64_t ncells;
+};
+
 template <class T>
 struct Row3 {
     T a, b, c;  // columns c-1, c, c+1
@@ -77,7 +85,7 @@ constexpr unsigned kFull = 0xffffffffu;
 // receive the prefetch of row j+1+PF.  `off` is the slab offset of (col, j); ph/uu/po/uo
 // are the warp's slab bases.  NX > 0 fixes the block width (and the row
 // stride) at compile time; FULL means every lane owns a column.
-template <class T, class Ops, bool NOISE, int NX, bool FULL, int PF, bool TAIL>
+template <class T, class Ops, bool NOISE, int NX, bool FULL, int PF, bool TAIL, bool ORIENT>
 __device__ __forceinline__ void strip_row(const typename Ops::Params& m, const TileArgs& g, int j, int r0, int r1,
                                           int lane,
                                           int col, bool valid, int last_lane, int n0, int n1, int off,
@@ -85,7 +93,7 @@ __device__ __forceinline__ void strip_row(const typename Ops::Params& m, const T
                                           T* __restrict__ po, T* __restrict__ uo, const Nbr2& nb, bool edge_x,
                                           uint64_t block_key, T bnd, const Row3<T>& A, const Row3<T>& B,
                                           const Row3<T>& C, Row3<T>& P, T UA, T UB, T UC, T& UP, T& jb, T dt,
-                                          T scale_amp) {
+                                          T scale_amp, const T* __restrict__ trig_b, int64_t ncells) {
     const int sy = NX > 0 ? NX + 2 : g.L.gdim[0];
     // lanes past the block's last column (valid false) run the same code on
     // a clamped column and only skip the stores: no branch splits the face,
@@ -108,6 +116,30 @@ __device__ __forceinline__ void strip_row(const typename Ops::Params& m, const T
     }
     T nval = T(0);
     if (NOISE) nval = Ops::noise(splitmix64(block_key ^ (uint64_t)(col + j * n0)));
+    if constexpr (ORIENT) {
+        // multi-grain: the cell's four faces in its own crystal frame, no
+        // face shared with a neighbour (finite_volume.rs:196-234)
+        T c0 = T(1), s0 = T(0);
+        if (live) {
+            const int64_t ci = (int64_t)j * n0 + (FULL ? col : min(col, n0 - 1));
+            c0 = __ldg(trig_b + ci);
+            s0 = __ldg(trig_b + ncells + ci);
+        }
+        T kphi, ku;
+        Ops::oriented_cell(m, A.a, A.b, A.c, B.a, B.b, B.c, C.a, C.b, C.c, c0, s0, UB, ul, ur, UC, UA, kphi, ku);
+        T phin = Ops::axpy(dt, kphi, B.b);
+        if (NOISE) phin = Ops::add_noise(phin, scale_amp, nval);
+        const T un = Ops::axpy(dt, ku, UB);
+        if (ok) {
+            po[off] = phin;
+            uo[off] = un;
+            if (edge_x || j == 0 || j == n1 - 1) {
+                push_ghosts_2d_g1(out, g.L, 0, nb, n0, n1, col, j, phin);
+                push_ghosts_2d_g1(out, g.L, 1, nb, n0, n1, col, j, un);
+            }
+        }
+        return;
+    }
     const T fl = Ops::xface(m, B.b - B.a, C.b - A.b, C.a, A.a);
     const T jt = Ops::yface(m, C.b - B.b, C.c - C.a, B.c, B.a);
     // right face: the next lane's left face, or the strip's boundary face of this row
@@ -133,13 +165,13 @@ __device__ __forceinline__ void strip_row(const typename Ops::Params& m, const T
 // One work unit of the strip kernel: the rows [r0, r1) of the 32-column
 // strip at c0 of block b, with the parameter record m (the kernel parameter,
 // or a batched instance's record) and the Wiener key of block key_block.
-template <class T, class Ops, bool NOISE, int NX, bool FULL, int PF, bool TAIL>
+template <class T, class Ops, bool NOISE, int NX, bool FULL, int PF, bool TAIL, bool ORIENT>
 __device__ __forceinline__ void strip_unit(const typename Ops::Params& m, uint64_t seed, int key_block,
                                            const TileArgs& g, const T* __restrict__ ph, const T* __restrict__ uu,
                                            T* __restrict__ out, T* __restrict__ po, T* __restrict__ uo,
                                            const Nbr2& nb, int r0, int r1, int lane, int col, bool valid,
                                            int last_lane, int cr, bool edge_x, int n0, int n1, int sy, double tnow,
-                                           T dt, T scale_amp) {
+                                           T dt, T scale_amp, const T* __restrict__ trig_b, int64_t ncells) {
     constexpr int NB = PF + 3;
     uint64_t block_key = 0;
     if (NOISE)
@@ -167,7 +199,7 @@ __device__ __forceinline__ void strip_unit(const typename Ops::Params& m, uint64
     uw[NB - 1] = T(0);
     // right-boundary face of the strip for rows r0 .. r0+31 (lane = row)
     T bnd = T(0);
-    {
+    if constexpr (!ORIENT) {
         const int r = r0 + lane;
         if (r < r1) {
             const T* q = ph + (cr + 1) + (r + 1) * sy;  // (column cr, row r)
@@ -178,14 +210,14 @@ __device__ __forceinline__ void strip_unit(const typename Ops::Params& m, uint64
         }
     }
     // y face below the first row (between r0-1 and r0)
-    jb = Ops::yface(m, w[1].b - w[0].b, w[1].c - w[1].a, w[0].c, w[0].a);
+    if constexpr (!ORIENT) jb = Ops::yface(m, w[1].b - w[0].b, w[1].c - w[1].a, w[0].c, w[0].a);
 
 #define LG_ROW(J, Q)                                                                                            \
-    strip_row<T, Ops, NOISE, NX, FULL, PF, TAIL>(m, g, J, r0, r1, lane, col, valid, last_lane, n0, n1, off, ph, uu, out, po,  \
+    strip_row<T, Ops, NOISE, NX, FULL, PF, TAIL, ORIENT>(m, g, J, r0, r1, lane, col, valid, last_lane, n0, n1, off, ph, uu, out, po,  \
                                        uo, nb, edge_x, block_key, bnd, w[(Q) % NB], w[((Q) + 1) % NB],          \
                                        w[((Q) + 2) % NB], w[((Q) + 2 + PF) % NB], uw[(Q) % NB],                \
                                        uw[((Q) + 1) % NB], uw[((Q) + 2) % NB], uw[((Q) + 2 + PF) % NB], jb, dt, \
-                                       scale_amp);                                                              \
+                                       scale_amp, trig_b, ncells);                                                              \
     off += sy
     for (int j = r0; j < r1; j += NB) {
 #pragma unroll
@@ -196,10 +228,11 @@ __device__ __forceinline__ void strip_unit(const typename Ops::Params& m, uint64
 
 // Rows per work unit are at most 32, so one batch of boundary faces (lanes
 // across rows) serves the whole unit.
-template <class T, class Ops, bool NOISE, int MINB, int NX, int PF, bool BATCH = false, bool TAIL = false>
+template <class T, class Ops, bool NOISE, int MINB, int NX, int PF, bool BATCH = false, bool TAIL = false,
+          bool ORIENT = false>
 __global__ void __launch_bounds__(256, MINB)
     modelc_strip_kernel(const T* __restrict__ in, T* __restrict__ out, TileArgs g, typename Ops::Params m0, T dt,
-                        T scale_amp, BatchArgs bt) {
+                        T scale_amp, BatchArgs bt, OrientArgs oa) {
     constexpr bool FULL = NX > 0 && NX % 32 == 0;
     const CartTopo& topo = g.topo;
     const int n0 = NX > 0 ? NX : topo.n[0];
@@ -245,12 +278,15 @@ __global__ void __launch_bounds__(256, MINB)
         if constexpr (BATCH) {
             const int inst = b / bt.bpi;
             const typename Ops::Params mi = static_cast<const typename Ops::Params*>(bt.params)[inst];
-            strip_unit<T, Ops, NOISE, NX, FULL, PF, TAIL>(mi, bt.seeds[inst], b - inst * bt.bpi, g, ph, uu, out, po, uo, nb,
-                                                    r0, r1, lane, col, valid, last_lane, cr, edge_x, n0, n1, sy,
-                                                    tnow, dt, scale_amp);
+            strip_unit<T, Ops, NOISE, NX, FULL, PF, TAIL, ORIENT>(
+                mi, bt.seeds[inst], b - inst * bt.bpi, g, ph, uu, out, po, uo, nb, r0, r1, lane, col, valid, last_lane,
+                cr, edge_x, n0, n1, sy, tnow, dt, scale_amp, nullptr, 0);
         } else {
-            strip_unit<T, Ops, NOISE, NX, FULL, PF, TAIL>(m0, g.seed, b, g, ph, uu, out, po, uo, nb, r0, r1, lane, col,
-                                                    valid, last_lane, cr, edge_x, n0, n1, sy, tnow, dt, scale_amp);
+            // multi-grain: this block's cos theta0 (sin theta0 follows ncells later)
+            const T* trig_b = ORIENT ? static_cast<const T*>(oa.trig) + (int64_t)b * n0 * n1 : nullptr;
+            strip_unit<T, Ops, NOISE, NX, FULL, PF, TAIL, ORIENT>(m0, g.seed, b, g, ph, uu, out, po, uo, nb, r0, r1,
+                                                                  lane, col, valid, last_lane, cr, edge_x, n0, n1, sy,
+                                                                  tnow, dt, scale_amp, trig_b, oa.ncells);
         }
     }
 }
@@ -297,13 +333,13 @@ cudaError_t launch_strip_batch(const T* in, T* out, TileArgs g, BatchArgs bt, T 
     const dim3 grid = strip_ctas(g), block(256);
     const typename Ops::Params m{};
     if (tail) {
-        modelc_strip_kernel<T, Ops, NOISE, MINB, 0, 1, true, true><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp, bt);
+        modelc_strip_kernel<T, Ops, NOISE, MINB, 0, 1, true, true><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp, bt, OrientArgs{});
         return cudaGetLastError();
     }
     switch (g.topo.n[0]) {
-        case 32: modelc_strip_kernel<T, Ops, NOISE, MINB, 32, 1, true><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp, bt); break;
-        case 64: modelc_strip_kernel<T, Ops, NOISE, MINB, 64, 1, true><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp, bt); break;
-        default: modelc_strip_kernel<T, Ops, NOISE, MINB, 0, 1, true><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp, bt);
+        case 32: modelc_strip_kernel<T, Ops, NOISE, MINB, 32, 1, true><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp, bt, OrientArgs{}); break;
+        case 64: modelc_strip_kernel<T, Ops, NOISE, MINB, 64, 1, true><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp, bt, OrientArgs{}); break;
+        default: modelc_strip_kernel<T, Ops, NOISE, MINB, 0, 1, true><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp, bt, OrientArgs{});
     }
     return cudaGetLastError();
 }
@@ -314,16 +350,35 @@ cudaError_t launch_strip_minb(const T* in, T* out, TileArgs g, const typename Op
     const bool tail = strip_plan(g, PF + 3);
     const dim3 grid = strip_ctas(g), block(256);
     if (tail) {
-        modelc_strip_kernel<T, Ops, NOISE, MINB, 0, PF, false, true><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp, BatchArgs{});
+        modelc_strip_kernel<T, Ops, NOISE, MINB, 0, PF, false, true><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp, BatchArgs{}, OrientArgs{});
         return cudaGetLastError();
     }
     switch (g.topo.n[0]) {  // block widths of the shipped configurations get a compile-time row stride
-        case 32: modelc_strip_kernel<T, Ops, NOISE, MINB, 32, PF><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp, BatchArgs{}); break;
-        case 64: modelc_strip_kernel<T, Ops, NOISE, MINB, 64, PF><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp, BatchArgs{}); break;
-        case 126: modelc_strip_kernel<T, Ops, NOISE, MINB, 126, PF><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp, BatchArgs{}); break;
-        case 128: modelc_strip_kernel<T, Ops, NOISE, MINB, 128, PF><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp, BatchArgs{}); break;
-        case 256: modelc_strip_kernel<T, Ops, NOISE, MINB, 256, PF><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp, BatchArgs{}); break;
-        default: modelc_strip_kernel<T, Ops, NOISE, MINB, 0, PF><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp, BatchArgs{});
+        case 32: modelc_strip_kernel<T, Ops, NOISE, MINB, 32, PF><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp, BatchArgs{}, OrientArgs{}); break;
+        case 64: modelc_strip_kernel<T, Ops, NOISE, MINB, 64, PF><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp, BatchArgs{}, OrientArgs{}); break;
+        case 126: modelc_strip_kernel<T, Ops, NOISE, MINB, 126, PF><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp, BatchArgs{}, OrientArgs{}); break;
+        case 128: modelc_strip_kernel<T, Ops, NOISE, MINB, 128, PF><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp, BatchArgs{}, OrientArgs{}); break;
+        case 256: modelc_strip_kernel<T, Ops, NOISE, MINB, 256, PF><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp, BatchArgs{}, OrientArgs{}); break;
+        default: modelc_strip_kernel<T, Ops, NOISE, MINB, 0, PF><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp, BatchArgs{}, OrientArgs{});
+    }
+    return cudaGetLastError();
+}
+
+// the multi-grain step: block widths 126 (the 101.6M-cell configuration)
+// and 256 get a compile-time row stride
+template <class T, class Ops, bool NOISE, int MINB>
+cudaError_t launch_strip_oriented(const T* in, T* out, TileArgs g, const typename Ops::Params& m, T dt, T scale_amp,
+                                  OrientArgs oa, cudaStream_t s) {
+    const bool tail = strip_plan(g, 1 + 3);
+    const dim3 grid = strip_ctas(g), block(256);
+    if (tail) {
+        modelc_strip_kernel<T, Ops, NOISE, MINB, 0, 1, false, true, true><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp, BatchArgs{}, oa);
+        return cudaGetLastError();
+    }
+    switch (g.topo.n[0]) {
+        case 126: modelc_strip_kernel<T, Ops, NOISE, MINB, 126, 1, false, false, true><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp, BatchArgs{}, oa); break;
+        case 256: modelc_strip_kernel<T, Ops, NOISE, MINB, 256, 1, false, false, true><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp, BatchArgs{}, oa); break;
+        default: modelc_strip_kernel<T, Ops, NOISE, MINB, 0, 1, false, false, true><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp, BatchArgs{}, oa);
     }
     return cudaGetLastError();
 }

@@ -48,6 +48,7 @@ class ModelC:
         self.orientations = False
         self.phi = None
         self.u = None
+        self.theta = None
 
     @classmethod
     def classic(cls, noise_amplitude: float = 0.0) -> "ModelC":
@@ -61,6 +62,10 @@ class ModelC:
         """phi moved by Time and Wiener(0), u by Time, both ghost 1 (phasefield.rs:335-349)."""
         self.phi = builder.register_driven("phi", 1, [TIME, wiener(0)])
         self.u = builder.register("u", 1)
+        if self.orientations:
+            # the static crystal orientation theta0, read at cell centres only
+            # (ghost width 0; phasefield.rs:342-348)
+            self.theta = builder.register_static("theta0", 0)
 
     def stable_dt(self, spacing) -> Optional[float]:
         """0.2 h^2 / D (phasefield.rs:446-449)."""
@@ -72,6 +77,19 @@ class ModelC:
                               flux_tol)
 
     # ------------------------------------------------------ initial state
+    def with_orientations(self) -> "ModelC":
+        """Per-grain crystal orientations (phasefield.rs:118-125): a static
+        theta0 field, and every face's anisotropy taken in its cell's crystal
+        frame.  Set theta0 with ``initialize_grains`` (nearest-seed Voronoi)
+        or upload it and call ``set_orientations``."""
+        self.orientations = True
+        return self
+
+    def set_orientations(self, state) -> None:
+        """Use the theta0 now in ``state`` for the following steps (cos and
+        sin theta0 are computed once, on the host, as the reference does)."""
+        N.check(N.lib.lg_modelc_set_orientations(state.handle, state._index("theta0")), state.scheduler.handle)
+
     def initialize(self, grid, state, seed_center, seed_radius: float, u0: float) -> None:
         """Single tanh seed in an undercooled melt (phasefield.rs:180-189)."""
         self.initialize_seeds(grid, state, [(seed_center, seed_radius)], u0)
@@ -82,14 +100,17 @@ class ModelC:
     def initialize_grains(self, grid, state, grains: Sequence[Grain], u0: float) -> None:
         """phi = max over seeds of -tanh((r - r0)/sqrt 2), u = -u0 (phasefield.rs:227-314),
         computed on the host exactly as the reference does, then uploaded."""
-        if any(g.orientation != 0.0 for g in grains):
-            raise NotImplementedError("per-grain orientations are not on the device path")
+        if any(g.orientation != 0.0 for g in grains) and not self.orientations:
+            raise ValueError("per-grain orientations need ModelC.with_orientations()")
         arr = np.array([[g.center[0], g.center[1], g.radius, g.orientation] for g in grains], dtype=np.float64)
         if state.alloc.dtype != "f64":
             raise ValueError("initialize_grains targets an FP64 state; upload a cast copy for FP32")
         ptr = arr.ctypes.data_as(C.POINTER(C.c_double)) if len(grains) else None
         N.check(N.lib.lg_modelc_initialize_grains(state.handle, ptr, len(grains), float(u0)),
                 state.scheduler.handle)
+        if self.orientations:  # theta0 by nearest-seed Voronoi (phasefield.rs:286-311)
+            N.check(N.lib.lg_modelc_initialize_orientations(state.handle, state._index("theta0"), ptr, len(grains)),
+                    state.scheduler.handle)
 
 
 def seed_positions(cells: int, h: float, nseeds: int, seed: int, radius: Optional[float] = None):

@@ -17,6 +17,8 @@
 // mirroring `RayonScheduler` (src/core/scheduler.rs:65-84): blocks are
 // disjoint, so results are identical for every thread count.
 
+#include <limits>
+
 #include "oracle_core.hpp"
 
 namespace {
@@ -195,7 +197,7 @@ double heat_run(const Grid& grid, State& st, int f, double kappa, double t, doub
 // EulerMaruyama::step (src/integrators/euler_maruyama.rs:34-75) with
 // ModelC<Wiener<1>> (noise != 0) or ModelC<NoNoise>, fields phi=0, u=1.
 double modelc_run(const Grid& grid, State& st, const ModelC& m, double t, double dt, uint64_t seed,
-                  int64_t steps, bool wiener, int nthreads) {
+                  int64_t steps, bool wiener, int nthreads, int theta_field = -1) {
     const int64_t nb = grid.num_blocks();
     const int64_t len = grid.block_len(1);
     // Stage buffers (simulation.rs:187-202): Tendency(Time) carries phi and
@@ -209,8 +211,12 @@ double modelc_run(const Grid& grid, State& st, const ModelC& m, double t, double
         fill_ghosts_mirror(grid, st, 1);
         const Ext e = ext_of(grid);
         parallel_blocks(nb, nthreads, [&](int64_t b) {
-            modelc_drift_block(e, grid.spacing, m, st.slab[b][0].data(), st.slab[b][1].data(), kphi[b].data(),
-                               ku[b].data());
+            if (theta_field >= 0)
+                modelc_drift_block_oriented(e, grid.spacing, m, st.slab[b][0].data(), st.slab[b][1].data(),
+                                            st.slab[b][theta_field].data(), kphi[b].data(), ku[b].data());
+            else
+                modelc_drift_block(e, grid.spacing, m, st.slab[b][0].data(), st.slab[b][1].data(), kphi[b].data(),
+                                   ku[b].data());
         });
         if (wiener) {
             // eval_tendency_impl: fill_zero then amp_phi = b on the interior
@@ -268,6 +274,56 @@ void modelc_initialize_grains(const Grid& grid, State& st, const double* grains,
             phi[grid.linearize(idx, 1)] = v;
         });
         for_each_interior(grid, [&](const int64_t* idx) { u[grid.linearize(idx, 1)] = -u0; });
+    }
+}
+
+// phasefield.rs:286-311: theta0 by nearest-seed Voronoi.  Per block, the
+// candidates are the grains whose box distance is at most the smallest
+// farthest-corner distance of any grain; each cell takes the orientation of
+// the candidate minimising fma(dy, dy, dx * dx) (the first one on ties, as
+// min_by), or 0 without candidates.  Written into field f (ghost width 0).
+void modelc_initialize_orientations(const Grid& grid, State& st, int f, const double* grains, int64_t n) {
+    const int64_t nx = grid.block[0], ny = grid.block[1];
+    for (int64_t b = 0; b < grid.num_blocks(); ++b) {
+        double hx = grid.spacing[0], hy = grid.spacing[1];
+        int64_t i0[3] = {0, 0, 0}, i1[3] = {nx - 1, ny - 1, 0};
+        double c0[3], c1[3];
+        grid.cell_center(b, i0, c0);
+        grid.cell_center(b, i1, c1);
+        double lo[2] = {std::fma(0.5, -hx, c0[0]), std::fma(0.5, -hy, c0[1])};
+        double hi[2] = {std::fma(0.5, hx, c1[0]), std::fma(0.5, hy, c1[1])};
+        auto dist_box = [&](double cx, double cy) {
+            double dx = std::max(std::max(lo[0] - cx, cx - hi[0]), 0.0);
+            double dy = std::max(std::max(lo[1] - cy, cy - hi[1]), 0.0);
+            return std::hypot(dx, dy);
+        };
+        auto dist_far = [&](double cx, double cy) {
+            double dx = std::max(std::fabs(cx - lo[0]), std::fabs(cx - hi[0]));
+            double dy = std::max(std::fabs(cy - lo[1]), std::fabs(cy - hi[1]));
+            return std::hypot(dx, dy);
+        };
+        double threshold = std::numeric_limits<double>::max();
+        for (int64_t k = 0; k < n; ++k) threshold = std::min(threshold, dist_far(grains[4 * k], grains[4 * k + 1]));
+        std::vector<int64_t> cand;
+        for (int64_t k = 0; k < n; ++k)
+            if (dist_box(grains[4 * k], grains[4 * k + 1]) <= threshold) cand.push_back(k);
+        std::vector<double>& th = st.slab[b][f];
+        for_each_interior(grid, [&](const int64_t* idx) {
+            double xy[3];
+            grid.cell_center(b, idx, xy);
+            double best = 0.0, bd = 0.0;
+            bool any = false;
+            for (int64_t k : cand) {
+                double dx = xy[0] - grains[4 * k], dy = xy[1] - grains[4 * k + 1];
+                double d = std::fma(dy, dy, dx * dx);
+                if (!any || d < bd) {  // strict: the first minimum stays (total_cmp on finite values)
+                    any = true;
+                    bd = d;
+                    best = grains[4 * k + 3];
+                }
+            }
+            th[grid.linearize(idx, 0)] = any ? best : 0.0;
+        });
     }
 }
 
@@ -376,6 +432,18 @@ void orc_modelc_drift(const void* grid, void* s, const orc_modelc_params* p, dou
         std::memcpy(kphi_out + b * len, kp.data(), len * sizeof(double));
         std::memcpy(ku_out + b * len, ku.data(), len * sizeof(double));
     }
+}
+
+double orc_modelc_run_oriented(const void* grid, void* s, const orc_modelc_params* p, int theta_field, double t0,
+                               double dt, uint64_t seed, int64_t steps, int wiener, int nthreads) {
+    ModelC m = make_model(p);
+    return modelc_run(*static_cast<const Grid*>(grid), *static_cast<State*>(s), m, t0, dt, seed, steps,
+                      wiener != 0, nthreads, theta_field);
+}
+
+void orc_modelc_initialize_orientations(const void* grid, void* s, int theta_field, const double* grains,
+                                        int64_t n) {
+    modelc_initialize_orientations(*static_cast<const Grid*>(grid), *static_cast<State*>(s), theta_field, grains, n);
 }
 
 void orc_modelc_initialize_grains(const void* grid, void* s, const double* grains, int64_t n, double u0) {

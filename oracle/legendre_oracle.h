@@ -53,6 +53,11 @@ double orc_modelc_run(const void* grid, void* s, const orc_modelc_params* p, dou
                       int64_t steps, int wiener, int nthreads);
 void orc_modelc_drift(const void* grid, void* s, const orc_modelc_params* p, double* kphi_out, double* ku_out);
 void orc_modelc_initialize_grains(const void* grid, void* s, const double* grains, int64_t n, double u0);
+/* the multi-grain form: theta0 in field `theta_field` (ghost width 0) */
+double orc_modelc_run_oriented(const void* grid, void* s, const orc_modelc_params* p, int theta_field, double t0,
+                               double dt, uint64_t seed, int64_t steps, int wiener, int nthreads);
+void orc_modelc_initialize_orientations(const void* grid, void* s, int theta_field, const double* grains,
+                                        int64_t n);
 int orc_num_threads_available(void);
 
 #ifdef __cplusplus

@@ -244,6 +244,72 @@ inline void modelc_drift_block(const Ext& e, const double* h, const ModelC& m, c
     });
 }
 
+// The multi-grain form: KarmaRappelFlux::apply_oriented (finite_volume.rs:
+// 178-235) with every face's anisotropy taken in the crystal frame of the
+// cell's own orientation theta0 (read at the cell centre, ghost width 0),
+// rotate() at finite_volume.rs:238-242, and the local terms with
+// center_anisotropy_rotated (finite_volume.rs:159-172, phasefield.rs:378-392).
+// (s0, c0) = theta0.sin_cos(): glibc sin and cos, as Rust's f64::sin_cos.
+inline void modelc_drift_block_oriented(const Ext& e, const double* h, const ModelC& m, const double* p,
+                                        const double* u, const double* theta, double* kphi, double* ku) {
+    const int g = 1;
+    const int64_t sx = 1, sy = e.n[0] + 2 * g;
+    double inv_h2 = 1.0 / (h[0] * h[1]);
+    double quarter = 0.25;
+    auto rotate = [](double c0, double s0, double dx, double dy, double* rx, double* ry) {
+        *rx = c0 * dx + s0 * dy;
+        *ry = c0 * dy - s0 * dx;
+    };
+    for_each_interior(e, [&](const int64_t* idx) {
+        int64_t o = e.lin(idx, g);
+        double th = theta[e.lin(idx, 0)];
+        double s0 = std::sin(th), c0 = std::cos(th);
+        auto P = [&](int di, int dj) { return p[o + di * sx + dj * sy]; };
+        double derx_r = P(1, 0) - P(0, 0);
+        double derx_l = P(0, 0) - P(-1, 0);
+        double derx_t = quarter * (P(1, 1) - P(-1, 1) + P(1, 0) - P(-1, 0));
+        double derx_b = quarter * (P(1, 0) - P(-1, 0) + P(1, -1) - P(-1, -1));
+        double dery_t = P(0, 1) - P(0, 0);
+        double dery_b = P(0, 0) - P(0, -1);
+        double dery_r = quarter * (P(1, 1) - P(1, -1) + P(0, 1) - P(0, -1));
+        double dery_l = quarter * (P(0, 1) - P(0, -1) + P(-1, 1) - P(-1, -1));
+        double rx, ry, a_r, da_r, a_l, da_l, a_t, da_t, a_b, da_b;
+        rotate(c0, s0, derx_r, dery_r, &rx, &ry);
+        kr_face(m, rx, ry, &a_r, &da_r);
+        rotate(c0, s0, derx_l, dery_l, &rx, &ry);
+        kr_face(m, rx, ry, &a_l, &da_l);
+        rotate(c0, s0, derx_t, dery_t, &rx, &ry);
+        kr_face(m, rx, ry, &a_t, &da_t);
+        rotate(c0, s0, derx_b, dery_b, &rx, &ry);
+        kr_face(m, rx, ry, &a_b, &da_b);
+        double j_r = a_r * (a_r * derx_r - da_r * dery_r);
+        double j_l = a_l * (a_l * derx_l - da_l * dery_l);
+        double j_t = a_t * (a_t * dery_t + da_t * derx_t);
+        double j_b = a_b * (a_b * dery_b + da_b * derx_b);
+        kphi[o] = (j_r - j_l + j_t - j_b) * inv_h2;
+    });
+    for_each_interior(e, [&](const int64_t* idx) {
+        int64_t o = e.lin(idx, g);
+        double th = theta[e.lin(idx, 0)];
+        double s0 = std::sin(th), c0 = std::cos(th);
+        double pv = p[o];
+        double g_prime = std::fma(pv * pv, pv, -pv);
+        double one_m_p2 = std::fma(pv, -pv, 1.0);
+        double p_prime = one_m_p2 * one_m_p2;
+        double dx = 0.5 * (p[o + sx] - p[o - sx]);
+        double dy = 0.5 * (p[o + sy] - p[o - sy]);
+        double rx, ry, a, da;
+        rotate(c0, s0, dx, dy, &rx, &ry);
+        kr_face(m, rx, ry, &a, &da);  // the flux's face(): flux constants
+        kphi[o] = std::fma(m.lambda * u[o], -p_prime, kphi[o] - g_prime) / (a * a);
+    });
+    central_laplacian(e, h, u, ku, g);
+    for_each_interior(e, [&](const int64_t* idx) {
+        int64_t o = e.lin(idx, g);
+        ku[o] = std::fma(ku[o], m.d_thermal, 0.5 * kphi[o]);
+    });
+}
+
 // ------------------------------------------------------------ drivers -----
 // Driver::Time (driver.rs:210-217): x += dt * v over every slab entry
 inline void apply_time(std::vector<double>& x, const std::vector<double>& v, double dt) {

@@ -51,6 +51,8 @@ def _load():
         "orc_modelc_run": (d, [p, p, C.POINTER(Params), d, d, u64, i64, C.c_int, C.c_int]),
         "orc_modelc_drift": (None, [p, p, C.POINTER(Params), pd, pd]),
         "orc_modelc_initialize_grains": (None, [p, p, pd, i64, d]),
+        "orc_modelc_run_oriented": (d, [p, p, C.POINTER(Params), C.c_int, d, d, u64, i64, C.c_int, C.c_int]),
+        "orc_modelc_initialize_orientations": (None, [p, p, C.c_int, pd, i64]),
         "orc_num_threads_available": (C.c_int, []),
     }
     for name, (res, args) in sigs.items():
@@ -156,6 +158,16 @@ class State:
 
     def modelc_run(self, params: Params, t0, dt, seed, steps, wiener, threads=1):
         return lib.orc_modelc_run(self.grid.h, self.h, C.byref(params), t0, dt, seed, steps, int(wiener), threads)
+
+    def modelc_run_oriented(self, params: Params, theta_field, t0, dt, seed, steps, wiener, threads=1):
+        return lib.orc_modelc_run_oriented(self.grid.h, self.h, C.byref(params), theta_field, t0, dt, seed, steps,
+                                           int(wiener), threads)
+
+    def initialize_orientations(self, theta_field, grains):
+        """grains: (x, y, radius, orientation) tuples."""
+        arr = np.array([[g[0], g[1], g[2], g[3]] for g in grains], dtype=np.float64)
+        lib.orc_modelc_initialize_orientations(self.grid.h, self.h, theta_field,
+                                               arr.ctypes.data_as(C.POINTER(C.c_double)), len(grains))
 
     def modelc_drift(self, params: Params):
         n = self.grid.num_blocks() * self.grid.block_len(1)
