@@ -38,6 +38,14 @@ CONFIGS = {
     "c3": dict(workload="model_c_10080sq", cells=10080, block=126, h=0.4, dt=0.008, d_thermal=2.0,
                lam=2.0 / 0.6267, eps4=0.05, u0=0.5, grains=64, radius=8.0, noise=0.01, seed=42,
                full_steps=10000),
+    # the reference's flagship run (README: model_c --cells 10080 --block 126
+    # --seeds 1000 --orient --noise 0.02): classic Model C (eps4 0.06, lambda
+    # 3.19, D = 0.6267 lambda), 1000 grains of r = 10 h with orientations
+    # unit_open(mix_key(42, [i, 2])) pi/2, theta0 by nearest seed, u0 = 0.7,
+    # b = 0.02, dt = 0.2 h^2 / D
+    "c3o": dict(workload="model_c_10080sq_1000grains_oriented", cells=10080, block=126, h=0.4,
+                dt=0.2 * 0.4 * 0.4 / (0.6267 * 3.19), d_thermal=0.6267 * 3.19, lam=3.19, eps4=0.06, u0=0.7,
+                grains=1000, radius=4.0, noise=0.02, seed=42, orient=True, full_steps=21865),
     # 3-D heat, 96^3 periodic as 6^3 blocks of 16^3, dt = 0.15 h^2, sine + seeded noise
     "c1": dict(kind="heat", workload="heat_96cube", cells=96, block=16, kappa=1.0, seed=42, amp=1e-3,
                full_steps=2000, noise=0.0),
@@ -172,9 +180,11 @@ def make_sim(cfg, dtype, sched, seed_offset=0):
     grid = L.CartesianGrid([n, n], [b, b], [0.0, 0.0], [h, h])
     model = L.ModelC(cfg["eps4"], cfg["lam"], cfg["noise"])
     model.d_thermal = cfg["d_thermal"]
+    if cfg.get("orient"):
+        model.with_orientations()
     sim = L.Simulation(grid, L.FiniteVolume(), model, L.EulerMaruyama(cfg["seed"] + seed_offset), sched,
                        L.CudaAllocator(dtype))
-    grains = L.seed_positions(n, h, cfg["grains"], cfg["seed"], radius=cfg["radius"])
+    grains = L.seed_positions(n, h, cfg["grains"], cfg["seed"], radius=cfg["radius"], orient=cfg.get("orient", False))
     return sim, grid, model, grains
 
 
@@ -188,9 +198,11 @@ def initialize(sim, grid, model, grains, cfg, dtype, sched):
         return
     tmp = L.DeviceState(grid, sched, L.CudaAllocator("f64"), sim.state.specs)
     model.initialize_grains(grid, tmp, grains, cfg["u0"])
-    for f in ("phi", "u"):
-        sim.state.upload(f, tmp.download(f).astype(np.float32))
+    for spec in sim.state.specs:
+        sim.state.upload(spec.name, tmp.download(spec.name).astype(np.float32))
     tmp._destroy()
+    if model.orientations:
+        model.set_orientations(sim.state)
 
 
 def to_global(blocks, n, b):
@@ -251,17 +263,26 @@ def cpu_oracle_rate(cfg, steps_budget_s: float, max_steps: int):
 
     n, b, h = cfg["cells"], cfg["block"], cfg["h"]
     og = orc.Grid([n, n], [b, b], [0.0, 0.0], [h, h])
-    st = orc.State(og, [1, 1])
-    grains = seed_positions(n, h, cfg["grains"], cfg["seed"], radius=cfg["radius"])
+    orient = bool(cfg.get("orient"))
+    st = orc.State(og, [1, 1, 0] if orient else [1, 1])
+    grains = seed_positions(n, h, cfg["grains"], cfg["seed"], radius=cfg["radius"], orient=orient)
     st.initialize_grains([(g.center[0], g.center[1], g.radius) for g in grains], cfg["u0"])
+    if orient:
+        st.initialize_orientations(2, [(g.center[0], g.center[1], g.radius, g.orientation) for g in grains])
     p = orc.modelc_params(eps4=cfg["eps4"], lam=cfg["lam"], d_thermal=cfg["d_thermal"], noise=cfg["noise"])
     threads = int(orc.lib.orc_num_threads_available())
+
+    def run(t, k):
+        if orient:
+            return st.modelc_run_oriented(p, 2, t, cfg["dt"], cfg["seed"], k, True, threads)
+        return st.modelc_run(p, t, cfg["dt"], cfg["seed"], k, True, threads)
+
     t0 = time.perf_counter()
-    t = st.modelc_run(p, 0.0, cfg["dt"], cfg["seed"], 1, True, threads)
+    t = run(0.0, 1)
     one = time.perf_counter() - t0
     steps = max(1, min(max_steps, int(steps_budget_s / max(one, 1e-6))))
     t0 = time.perf_counter()
-    st.modelc_run(p, t, cfg["dt"], cfg["seed"], steps, True, threads)
+    run(t, steps)
     el = time.perf_counter() - t0
     return n * n * steps / el / 1e9, steps, threads
 
@@ -722,7 +743,9 @@ def main():
 
     if rank == 0:
         peak, peak_kind = peaks()
-        algo = BYTES_PER_CELL[args.dtype] * cells
+        # the multi-grain step also reads cos and sin theta0 of every cell
+        bpc = BYTES_PER_CELL[args.dtype] + (2 * (8 if args.dtype == "f64" else 4) if cfg.get("orient") else 0)
+        algo = bpc * cells
         achieved = algo / (ms_per_step / 1e3) / 1e9
         err = None
         if args.dtype == "f32" and world == 1:
@@ -743,7 +766,7 @@ def main():
                        "graph": True, "variant": args.variant, "autotuned_variant": tuned},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic(args, cells), "peak_kind": peak_kind,
-                         "algorithmic_bytes_per_cell": BYTES_PER_CELL[args.dtype]},
+                         "algorithmic_bytes_per_cell": bpc},
             "cpu_baseline": cpu,
             "e2e": e2e,
             "fp32_error": err,
