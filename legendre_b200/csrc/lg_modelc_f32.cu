@@ -68,38 +68,34 @@ struct OpsFast32 {
         const float lap = ((ur + ul) - 2.0f * uc) * m.ih0 + ((up + um) - 2.0f * uc) * m.ih1;
         ku = lap * m.d_thermal + 0.5f * kphi;
     }
-    // the multi-grain cell: four faces in the cell's crystal frame, each with
-    // one reciprocal (see OpsExact::oriented_cell for the reference form)
-    static __device__ __forceinline__ float oface(const Fast32& m, float rx, float ry, float& da) {
+    // multi-grain faces and cell (see OpsExact::oxface for the reference form):
+    // one reciprocal per face
+    static __device__ __forceinline__ float oaniso(const Fast32& m, float rx, float ry, float& da) {
         float a, inv;
         aniso(rx, ry, m.f_a_bar, m.f_a1pe, m.f_2ae, m.f_tol, a, inv);
         da = -m.f_a12 * rx * ry * (rx * rx - ry * ry) * inv;
         return a;
     }
-    static __device__ __forceinline__ void oriented_cell(const Fast32& m, float Aa, float Ab, float Ac, float Ba,
-                                                         float Bb, float Bc, float Ca, float Cb, float Cc, float c0,
-                                                         float s0, float uc, float ul, float ur, float up, float um,
-                                                         float& kphi, float& ku) {
-        const float derx_r = Bc - Bb, derx_l = Bb - Ba;
-        const float derx_t = 0.25f * ((Cc - Ca) + (Bc - Ba)), derx_b = 0.25f * ((Bc - Ba) + (Ac - Aa));
-        const float dery_t = Cb - Bb, dery_b = Bb - Ab;
-        const float dery_r = 0.25f * ((Cc - Ac) + (Cb - Ab)), dery_l = 0.25f * ((Cb - Ab) + (Ca - Aa));
-        float da_r, da_l, da_t, da_b;
-        const float a_r = oface(m, c0 * derx_r + s0 * dery_r, c0 * dery_r - s0 * derx_r, da_r);
-        const float a_l = oface(m, c0 * derx_l + s0 * dery_l, c0 * dery_l - s0 * derx_l, da_l);
-        const float a_t = oface(m, c0 * derx_t + s0 * dery_t, c0 * dery_t - s0 * derx_t, da_t);
-        const float a_b = oface(m, c0 * derx_b + s0 * dery_b, c0 * dery_b - s0 * derx_b, da_b);
-        const float jr = a_r * (a_r * derx_r - da_r * dery_r);
-        const float jl = a_l * (a_l * derx_l - da_l * dery_l);
-        const float jt = a_t * (a_t * dery_t + da_t * derx_t);
-        const float jb = a_b * (a_b * dery_b + da_b * derx_b);
+    static __device__ __forceinline__ float oxface(const Fast32& m, float c0, float s0, float derx, float dery) {
+        float da;
+        const float a = oaniso(m, c0 * derx + s0 * dery, c0 * dery - s0 * derx, da);
+        return a * (a * derx - da * dery);
+    }
+    static __device__ __forceinline__ float oyface(const Fast32& m, float c0, float s0, float derx, float dery) {
+        float da;
+        const float a = oaniso(m, c0 * derx + s0 * dery, c0 * dery - s0 * derx, da);
+        return a * (a * dery + da * derx);
+    }
+    static __device__ __forceinline__ void ocell(const Fast32& m, float jr, float jl, float jt, float jb, float p,
+                                                 float cdx, float cdy, float c0, float s0, float uc, float ul, float ur,
+                                                 float up, float um, float& kphi, float& ku) {
         const float flux = ((jr - jl) + (jt - jb)) * m.inv_h2_flux;
-        const float g_prime = Bb * Bb * Bb - Bb;
-        const float one_m_p2 = 1.0f - Bb * Bb;
+        const float g_prime = p * p * p - p;
+        const float one_m_p2 = 1.0f - p * p;
         const float p_prime = one_m_p2 * one_m_p2;
-        const float dx = 0.5f * (Bc - Ba), dy = 0.5f * (Cb - Ab);
+        const float dx = 0.5f * cdx, dy = 0.5f * cdy;
         float dac;
-        const float a = oface(m, c0 * dx + s0 * dy, c0 * dy - s0 * dx, dac);
+        const float a = oaniso(m, c0 * dx + s0 * dy, c0 * dy - s0 * dx, dac);
         kphi = ((flux - g_prime) - m.lambda * uc * p_prime) * rcp_approx(a * a);
         const float lap = ((ur + ul) - 2.0f * uc) * m.ih0 + ((up + um) - 2.0f * uc) * m.ih1;
         ku = lap * m.d_thermal + 0.5f * kphi;

@@ -101,34 +101,29 @@ struct OpsExact {
         acc += ((up - (uc + uc)) + um) * m.ih1;
         ku = fma_t(acc, m.d_thermal, T(0.5) * kphi);
     }
-    // The multi-grain cell (finite_volume.rs:196-234, phasefield.rs:378-392):
-    // the four faces of cell (i, j) from its 3x3 neighbourhood -- rows A (j-1),
-    // B (j), C (j+1), columns a (i-1), b (i), c (i+1) -- each with its
-    // anisotropy in the crystal frame (c0, s0) = (cos, sin) theta0 of the cell,
-    // fluxes in the lab frame; the centre anisotropy rotated likewise, with
-    // the flux's constants (center_anisotropy_rotated).
-    static __device__ __forceinline__ void oriented_cell(const MC<T>& m, T Aa, T Ab, T Ac, T Ba, T Bb, T Bc, T Ca,
-                                                         T Cb, T Cc, T c0, T s0, T uc, T ul, T ur, T up, T um,
-                                                         T& kphi, T& ku) {
-        const T q = T(0.25);
-        const T derx_r = Bc - Bb, derx_l = Bb - Ba;
-        const T derx_t = q * (Cc - Ca + Bc - Ba), derx_b = q * (Bc - Ba + Ac - Aa);
-        const T dery_t = Cb - Bb, dery_b = Bb - Ab;
-        const T dery_r = q * (Cc - Ac + Cb - Ab), dery_l = q * (Cb - Ab + Ca - Aa);
-        T a_r, da_r, a_l, da_l, a_t, da_t, a_b, da_b;
-        kr_face(m, c0 * derx_r + s0 * dery_r, c0 * dery_r - s0 * derx_r, a_r, da_r);
-        kr_face(m, c0 * derx_l + s0 * dery_l, c0 * dery_l - s0 * derx_l, a_l, da_l);
-        kr_face(m, c0 * derx_t + s0 * dery_t, c0 * dery_t - s0 * derx_t, a_t, da_t);
-        kr_face(m, c0 * derx_b + s0 * dery_b, c0 * dery_b - s0 * derx_b, a_b, da_b);
-        const T jr = a_r * (a_r * derx_r - da_r * dery_r);
-        const T jl = a_l * (a_l * derx_l - da_l * dery_l);
-        const T jt = a_t * (a_t * dery_t + da_t * derx_t);
-        const T jb = a_b * (a_b * dery_b + da_b * derx_b);
+    // Multi-grain faces and cell (finite_volume.rs:196-234, phasefield.rs:
+    // 378-392): a face's anisotropy in the crystal frame (c0, s0) = (cos, sin)
+    // theta0 of the cell being updated, the flux in the lab frame; the centre
+    // anisotropy rotated likewise with the flux's constants
+    // (center_anisotropy_rotated).  derx/dery are the face's lab-frame
+    // differences in the reference's operand order.
+    static __device__ __forceinline__ T oxface(const MC<T>& m, T c0, T s0, T derx, T dery) {
+        T a, da;
+        kr_face(m, c0 * derx + s0 * dery, c0 * dery - s0 * derx, a, da);
+        return a * (a * derx - da * dery);
+    }
+    static __device__ __forceinline__ T oyface(const MC<T>& m, T c0, T s0, T derx, T dery) {
+        T a, da;
+        kr_face(m, c0 * derx + s0 * dery, c0 * dery - s0 * derx, a, da);
+        return a * (a * dery + da * derx);
+    }
+    static __device__ __forceinline__ void ocell(const MC<T>& m, T jr, T jl, T jt, T jb, T p, T cdx, T cdy, T c0, T s0,
+                                                 T uc, T ul, T ur, T up, T um, T& kphi, T& ku) {
         const T flux = (jr - jl + jt - jb) * m.inv_h2_flux;
-        const T g_prime = fma_t(Bb * Bb, Bb, -Bb);
-        const T one_m_p2 = fma_t(Bb, -Bb, T(1));
+        const T g_prime = fma_t(p * p, p, -p);
+        const T one_m_p2 = fma_t(p, -p, T(1));
         const T p_prime = one_m_p2 * one_m_p2;
-        const T dx = T(0.5) * (Bc - Ba), dy = T(0.5) * (Cb - Ab);
+        const T dx = T(0.5) * cdx, dy = T(0.5) * cdy;
         T a, da;
         kr_face(m, c0 * dx + s0 * dy, c0 * dy - s0 * dx, a, da);
         kphi = fma_t(m.lambda * uc, -p_prime, flux - g_prime) / (a * a);

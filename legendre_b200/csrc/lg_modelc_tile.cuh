@@ -79,6 +79,9 @@ struct Row3 {
 
 constexpr unsigned kFull = 0xffffffffu;
 
+__device__ __forceinline__ bool same_bits(double a, double b) { return __double_as_longlong(a) == __double_as_longlong(b); }
+__device__ __forceinline__ bool same_bits(float a, float b) { return __float_as_int(a) == __float_as_int(b); }
+
 // One row: x face left of the lane's column, y face above cell (c, j), the
 // cell update, stores and ghost pushes.  A, B, C = phi rows j-1, j, j+1 at
 // columns c-1, c, c+1; UA, UB, UC = u at column c for the same rows; P / UP
@@ -93,7 +96,8 @@ __device__ __forceinline__ void strip_row(const typename Ops::Params& m, const T
                                           T* __restrict__ po, T* __restrict__ uo, const Nbr2& nb, bool edge_x,
                                           uint64_t block_key, T bnd, const Row3<T>& A, const Row3<T>& B,
                                           const Row3<T>& C, Row3<T>& P, T UA, T UB, T UC, T& UP, T& jb, T dt,
-                                          T scale_amp, const T* __restrict__ trig_b, int64_t ncells) {
+                                          T scale_amp, const T* __restrict__ trig_b, int64_t ncells, T& cprev,
+                                          T& sprev) {
     const int sy = NX > 0 ? NX + 2 : g.L.gdim[0];
     // lanes past the block's last column (valid false) run the same code on
     // a clamped column and only skip the stores: no branch splits the face,
@@ -117,16 +121,35 @@ __device__ __forceinline__ void strip_row(const typename Ops::Params& m, const T
     T nval = T(0);
     if (NOISE) nval = Ops::noise(splitmix64(block_key ^ (uint64_t)(col + j * n0)));
     if constexpr (ORIENT) {
-        // multi-grain: the cell's four faces in its own crystal frame, no
-        // face shared with a neighbour (finite_volume.rs:196-234)
+        // multi-grain: every face's anisotropy in the frame of the cell being
+        // updated.  Within a grain two neighbours share theta0, and the
+        // reference evaluates their common face from the same differences in
+        // the same order, so it is computed once: the left face comes from
+        // this lane, the right face from the next lane (or the strip's
+        // boundary batch), the bottom face from the previous row.  Where the
+        // neighbour's cos/sin theta0 differ (grain boundaries), the face is
+        // evaluated again in this cell's frame.
         T c0 = T(1), s0 = T(0);
         if (live) {
             const int64_t ci = (int64_t)j * n0 + (FULL ? col : min(col, n0 - 1));
             c0 = __ldg(trig_b + ci);
             s0 = __ldg(trig_b + ncells + ci);
         }
+        const T q = T(0.25);
+        const T jl = Ops::oxface(m, c0, s0, B.b - B.a, q * (C.b - A.b + C.a - A.a));
+        const T jt = Ops::oyface(m, c0, s0, q * (C.c - C.a + B.c - B.a), C.b - B.b);
+        T jr = __shfl_down_sync(kFull, jl, 1);
+        const T c0n = __shfl_down_sync(kFull, c0, 1), s0n = __shfl_down_sync(kFull, s0, 1);
+        const T fb = __shfl_sync(kFull, bnd, (j - r0) & 31);
+        if (lane == last_lane)
+            jr = fb;
+        else if (!(same_bits(c0n, c0) && same_bits(s0n, s0)))
+            jr = Ops::oxface(m, c0, s0, B.c - B.b, q * (C.c - A.c + C.b - A.b));
+        T jbot = jb;
+        if (!(same_bits(cprev, c0) && same_bits(sprev, s0)))
+            jbot = Ops::oyface(m, c0, s0, q * (B.c - B.a + A.c - A.a), B.b - A.b);
         T kphi, ku;
-        Ops::oriented_cell(m, A.a, A.b, A.c, B.a, B.b, B.c, C.a, C.b, C.c, c0, s0, UB, ul, ur, UC, UA, kphi, ku);
+        Ops::ocell(m, jr, jl, jt, jbot, B.b, B.c - B.a, C.b - A.b, c0, s0, UB, ul, ur, UC, UA, kphi, ku);
         T phin = Ops::axpy(dt, kphi, B.b);
         if (NOISE) phin = Ops::add_noise(phin, scale_amp, nval);
         const T un = Ops::axpy(dt, ku, UB);
@@ -138,6 +161,9 @@ __device__ __forceinline__ void strip_row(const typename Ops::Params& m, const T
                 push_ghosts_2d_g1(out, g.L, 1, nb, n0, n1, col, j, un);
             }
         }
+        jb = jt;
+        cprev = c0;
+        sprev = s0;
         return;
     }
     const T fl = Ops::xface(m, B.b - B.a, C.b - A.b, C.a, A.a);
@@ -208,16 +234,35 @@ __device__ __forceinline__ void strip_unit(const typename Ops::Params& m, uint64
             const T c0p = __ldg(q + sy), c1p = __ldg(q + sy + 1);
             bnd = Ops::xface(m, c10 - c00, c1p - c1m, c0p, c0m);
         }
+    } else {  // the same faces in the frame of the strip's last cell of each row
+        const int r = r0 + lane;
+        if (r < r1) {
+            const T* q = ph + (cr + 1) + (r + 1) * sy;
+            const T c0m = __ldg(q - sy), c1m = __ldg(q - sy + 1);
+            const T c00 = __ldg(q), c10 = __ldg(q + 1);
+            const T c0p = __ldg(q + sy), c1p = __ldg(q + sy + 1);
+            const int64_t ci = (int64_t)r * n0 + cr;
+            bnd = Ops::oxface(m, __ldg(trig_b + ci), __ldg(trig_b + ncells + ci), c10 - c00,
+                              T(0.25) * (c1p - c1m + c0p - c0m));
+        }
     }
     // y face below the first row (between r0-1 and r0)
-    if constexpr (!ORIENT) jb = Ops::yface(m, w[1].b - w[0].b, w[1].c - w[1].a, w[0].c, w[0].a);
+    T cpv = T(0), spv = T(0);  // cos/sin theta0 of the previous row's cell (multi-grain)
+    if constexpr (!ORIENT) {
+        jb = Ops::yface(m, w[1].b - w[0].b, w[1].c - w[1].a, w[0].c, w[0].a);
+    } else {  // bottom face of the first row in its own frame
+        const int64_t ci = (int64_t)r0 * n0 + (FULL ? col : min(col, n0 - 1));
+        cpv = __ldg(trig_b + ci);
+        spv = __ldg(trig_b + ncells + ci);
+        jb = Ops::oyface(m, cpv, spv, T(0.25) * (w[1].c - w[1].a + w[0].c - w[0].a), w[1].b - w[0].b);
+    }
 
 #define LG_ROW(J, Q)                                                                                            \
     strip_row<T, Ops, NOISE, NX, FULL, PF, TAIL, ORIENT>(m, g, J, r0, r1, lane, col, valid, last_lane, n0, n1, off, ph, uu, out, po,  \
                                        uo, nb, edge_x, block_key, bnd, w[(Q) % NB], w[((Q) + 1) % NB],          \
                                        w[((Q) + 2) % NB], w[((Q) + 2 + PF) % NB], uw[(Q) % NB],                \
                                        uw[((Q) + 1) % NB], uw[((Q) + 2) % NB], uw[((Q) + 2 + PF) % NB], jb, dt, \
-                                       scale_amp, trig_b, ncells);                                                              \
+                                       scale_amp, trig_b, ncells, cpv, spv);                                                              \
     off += sy
     for (int j = r0; j < r1; j += NB) {
 #pragma unroll
