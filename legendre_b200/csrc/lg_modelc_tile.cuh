@@ -97,7 +97,7 @@ __device__ __forceinline__ void strip_row(const typename Ops::Params& m, const T
                                           uint64_t block_key, T bnd, const Row3<T>& A, const Row3<T>& B,
                                           const Row3<T>& C, Row3<T>& P, T UA, T UB, T UC, T& UP, T& jb, T dt,
                                           T scale_amp, const T* __restrict__ trig_b, int64_t ncells, T& cprev,
-                                          T& sprev) {
+                                          T& sprev, T& cnext, T& snext) {
     const int sy = NX > 0 ? NX + 2 : g.L.gdim[0];
     // lanes past the block's last column (valid false) run the same code on
     // a clamped column and only skip the stores: no branch splits the face,
@@ -129,11 +129,12 @@ __device__ __forceinline__ void strip_row(const typename Ops::Params& m, const T
         // boundary batch), the bottom face from the previous row.  Where the
         // neighbour's cos/sin theta0 differ (grain boundaries), the face is
         // evaluated again in this cell's frame.
-        T c0 = T(1), s0 = T(0);
-        if (live) {
-            const int64_t ci = (int64_t)j * n0 + (FULL ? col : min(col, n0 - 1));
-            c0 = __ldg(trig_b + ci);
-            s0 = __ldg(trig_b + ncells + ci);
+        // this row's frame arrived with the previous row; fetch the next one
+        const T c0 = cnext, s0 = snext;
+        if (j + 1 < n1) {
+            const int64_t ci = (int64_t)(j + 1) * n0 + (FULL ? col : min(col, n0 - 1));
+            cnext = __ldg(trig_b + ci);
+            snext = __ldg(trig_b + ncells + ci);
         }
         const T q = T(0.25);
         const T jl = Ops::oxface(m, c0, s0, B.b - B.a, q * (C.b - A.b + C.a - A.a));
@@ -248,12 +249,13 @@ __device__ __forceinline__ void strip_unit(const typename Ops::Params& m, uint64
     }
     // y face below the first row (between r0-1 and r0)
     T cpv = T(0), spv = T(0);  // cos/sin theta0 of the previous row's cell (multi-grain)
+    T cnx = T(0), snx = T(0);  // and of the row about to be stepped
     if constexpr (!ORIENT) {
         jb = Ops::yface(m, w[1].b - w[0].b, w[1].c - w[1].a, w[0].c, w[0].a);
     } else {  // bottom face of the first row in its own frame
         const int64_t ci = (int64_t)r0 * n0 + (FULL ? col : min(col, n0 - 1));
-        cpv = __ldg(trig_b + ci);
-        spv = __ldg(trig_b + ncells + ci);
+        cpv = cnx = __ldg(trig_b + ci);
+        spv = snx = __ldg(trig_b + ncells + ci);
         jb = Ops::oyface(m, cpv, spv, T(0.25) * (w[1].c - w[1].a + w[0].c - w[0].a), w[1].b - w[0].b);
     }
 
@@ -262,7 +264,7 @@ __device__ __forceinline__ void strip_unit(const typename Ops::Params& m, uint64
                                        uo, nb, edge_x, block_key, bnd, w[(Q) % NB], w[((Q) + 1) % NB],          \
                                        w[((Q) + 2) % NB], w[((Q) + 2 + PF) % NB], uw[(Q) % NB],                \
                                        uw[((Q) + 1) % NB], uw[((Q) + 2) % NB], uw[((Q) + 2 + PF) % NB], jb, dt, \
-                                       scale_amp, trig_b, ncells, cpv, spv);                                                              \
+                                       scale_amp, trig_b, ncells, cpv, spv, cnx, snx);                                                              \
     off += sy
     for (int j = r0; j < r1; j += NB) {
 #pragma unroll
