@@ -170,6 +170,16 @@ int lg_modelc_initialize_grains(lg_state* st, const double* grains, int64_t n, d
  * radius, orientation) and sets it. */
 int lg_modelc_set_orientations(lg_state* st, int theta_field);
 int lg_modelc_initialize_orientations(lg_state* st, int theta_field, const double* grains, int64_t n);
+/* RungeKutta4 (src/integrators/rk4.rs:22-79): classic fourth-order steps of
+ * the heat model on `field` (any dimension, FP64) and of Model C (2-D,
+ * axis-aligned or multi-grain, FP64 or FP32), deterministic models only (the
+ * reference pairs RK4 with NoNoise): a non-zero noise amplitude is refused.
+ * Each step is four stage launches, k_i of the stage input written beside
+ * y + c_i k_i, the last one applying y += dt/6 k1, dt/3 k2, dt/3 k3, dt/6 k4
+ * in the reference's order; FP64 is bit-identical to the reference.  The
+ * first run allocates five more arenas of the state's size. */
+int lg_heat_rk4_run(lg_state* st, int field, double kappa, double dt, int64_t nsteps, uint32_t flags);
+int lg_modelc_rk4_run(lg_state* st, const lg_modelc_params* p, double dt, int64_t nsteps, uint32_t flags);
 /* Heat initial condition of the 96^3 benchmark: sin(2 pi x) sin(2 pi y)
  * sin(2 pi z) + amp * (2 * unit_open(mix_key(seed, [gx, gy, gz])) - 1) at
  * cell centres (gx.. = global cell index); the reference has no such

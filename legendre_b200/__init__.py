@@ -6,7 +6,7 @@ Importing the package loads ``liblegendre_b200.so`` (built in-tree by
 from ._native import LegendreError, exported_symbols  # noqa: F401  (loads the library)
 from .core import CudaAllocator, CudaScheduler, DeviceState, FieldSpec, Simulation, StateBuilder, TIME, wiener
 from .geometry import CartesianGrid, GridError
-from .integrators import EulerMaruyama, FiniteDifference, FiniteVolume, ForwardEuler
+from .integrators import EulerMaruyama, FiniteDifference, FiniteVolume, ForwardEuler, RungeKutta4
 from .physics import A1, A2, Grain, Heat, ModelC, seed_positions
 from .ensemble import Ensemble
 from .observe import AsyncObserver, ParquetObserver, Snapshot, cell_centers
@@ -20,5 +20,5 @@ __all__ = [
     "A1", "A2", "CartesianGrid", "CudaAllocator", "CudaScheduler", "DeviceState", "Ensemble", "EulerMaruyama",
     "FieldSpec",
     "FiniteDifference", "FiniteVolume", "ForwardEuler", "Grain", "GridError", "Heat", "LegendreError", "ModelC",
-    "Simulation", "StateBuilder", "TIME", "seed_positions", "wiener",
+    "RungeKutta4", "Simulation", "StateBuilder", "TIME", "seed_positions", "wiener",
 ]

@@ -110,6 +110,8 @@ _SIGS = {
     "lg_modelc_autotune": (C.c_int, [_p, C.POINTER(ModelCParams), _d, _u64, C.c_int, C.POINTER(C.c_int), _pd]),
     "lg_modelc_initialize_grains": (C.c_int, [_p, _pd, _i64, _d]),
     "lg_modelc_set_orientations": (C.c_int, [_p, C.c_int]),
+    "lg_heat_rk4_run": (C.c_int, [_p, C.c_int, _d, _d, _i64, C.c_uint32]),
+    "lg_modelc_rk4_run": (C.c_int, [_p, C.POINTER(ModelCParams), _d, _i64, C.c_uint32]),
     "lg_modelc_initialize_orientations": (C.c_int, [_p, C.c_int, _pd, _i64]),
     "lg_heat_initialize_sine_noise": (C.c_int, [_p, C.c_int, _u64, _d]),
     "lg_standard_normal": (C.c_int, [_p, C.POINTER(C.c_uint64), _i64, _pd]),

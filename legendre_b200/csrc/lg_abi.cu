@@ -64,6 +64,9 @@ struct lg_state {
     // interior cell on the device (cos block-major, then sin), state dtype
     int theta_field = -1;
     void* orient = nullptr;
+    // RungeKutta4 workspace (allocated at the first RK4 run): k1, k2, k3 and
+    // two stage states, each an arena of the state's layout
+    void* rk[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
 };
 
 namespace {
@@ -423,6 +426,7 @@ int lg_state_destroy(lg_state* st) {
     cudaFree(st->arena[1]);
     cudaFree(st->d_t);
     cudaFree(st->orient);
+    for (void* q : st->rk) cudaFree(q);
     delete st;
     return LG_OK;
 }
@@ -758,6 +762,151 @@ int lg_modelc_initialize_grains(lg_state* st, const double* grains, int64_t n, d
     int rc = lg_state_upload_field(st, 0, phi.data(), (int64_t)phi.size());
     if (rc != LG_OK) return rc;
     return lg_state_upload_field(st, 1, u.data(), (int64_t)u.size());
+}
+
+// the RungeKutta4 workspace: five arenas of the state's layout, zeroed
+static int rk_workspace(lg_state* st) {
+    if (st->rk[0]) return LG_OK;
+    const size_t bytes = (size_t)st->grid->nblocks * st->nfields * st->slab_stride * st->esize;
+    for (void*& q : st->rk) {
+        cudaError_t e = cudaMalloc(&q, bytes);
+        if (e == cudaSuccess) e = cudaMemsetAsync(q, 0, bytes, st->ctx->stream);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            for (void*& r : st->rk) {
+                cudaFree(r);
+                r = nullptr;
+            }
+            return fail(st->ctx, LG_ERR_NOMEM, "RungeKutta4 workspace: out of device memory");
+        }
+    }
+    return LG_OK;
+}
+
+int lg_heat_rk4_run(lg_state* st, int field, double kappa, double dt, int64_t nsteps, uint32_t flags) {
+    if (!st) return LG_ERR_INVALID;
+    lg_ctx* ctx = st->ctx;
+    if (st->dtype != LG_F64) return fail(ctx, LG_ERR_STATE, "the heat path is FP64");
+    if (field < 0 || field >= st->nfields || st->ghosts[field] != 1)
+        return fail(ctx, LG_ERR_STATE, "heat field must exist and have ghost width 1");
+    if (nsteps < 0) return fail(ctx, LG_ERR_INVALID, "negative step count");
+    cudaSetDevice(ctx->device);
+    int rc = rk_workspace(st);
+    if (rc != LG_OK) return rc;
+    if (!st->ghosts_valid) {
+        rc = fill_all_ghosts(st);
+        if (rc != LG_OK) return rc;
+    }
+    double inv_h2[3] = {0, 0, 0};
+    for (int d = 0; d < st->grid->D; ++d) inv_h2[d] = 1.0 / (st->grid->spacing[d] * st->grid->spacing[d]);
+    const lg::CartTopo topo = topo_of(st->grid);
+    const lg::SlabLayout L = layout_of(st, field);
+    const double half_dt = 0.5 * dt, sixth = dt / 6.0, third = dt / 3.0;  // rk4.rs:57, 74-75
+    char key[256];
+    snprintf(key, sizeof key, "heat-rk4|f=%d|k=%a|dt=%a", field, kappa, dt);
+    double* k1 = static_cast<double*>(st->rk[0]);
+    double* k2 = static_cast<double*>(st->rk[1]);
+    double* k3 = static_cast<double*>(st->rk[2]);
+    double* t0 = static_cast<double*>(st->rk[3]);
+    double* t1 = static_cast<double*>(st->rk[4]);
+    auto step = [&]() -> int {
+        const double* y = static_cast<const double*>(st->arena[st->cur]);
+        double* out = static_cast<double*>(st->arena[st->cur ^ 1]);
+        cudaError_t e = lg::launch_heat_rk_stage(1, y, t0, y, k1, nullptr, nullptr, nullptr, topo, L, field, kappa,
+                                                 inv_h2, half_dt, 0.0, 0.0, ctx->stream);
+        if (e == cudaSuccess)
+            e = lg::launch_heat_rk_stage(1, t0, t1, y, k2, nullptr, nullptr, nullptr, topo, L, field, kappa, inv_h2,
+                                         half_dt, 0.0, 0.0, ctx->stream);
+        if (e == cudaSuccess)
+            e = lg::launch_heat_rk_stage(1, t1, t0, y, k3, nullptr, nullptr, nullptr, topo, L, field, kappa, inv_h2,
+                                         dt, 0.0, 0.0, ctx->stream);
+        if (e == cudaSuccess)
+            e = lg::launch_heat_rk_stage(2, t0, out, y, nullptr, k1, k2, k3, topo, L, field, kappa, inv_h2, 0.0,
+                                         sixth, third, ctx->stream);
+        ctx->launches += 4;
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "heat RK4 stage launch");
+        st->cur ^= 1;
+        st->tslot ^= 1;
+        return LG_OK;
+    };
+    rc = run_steps(st, key, nsteps, flags, step);
+    if (rc != LG_OK) return rc;
+    advance_time(st, dt, nsteps);
+    return LG_OK;
+}
+
+int lg_modelc_rk4_run(lg_state* st, const lg_modelc_params* p, double dt, int64_t nsteps, uint32_t flags) {
+    if (!st || !p) return LG_ERR_INVALID;
+    lg_ctx* ctx = st->ctx;
+    if (st->grid->D != 2 || st->nfields < 2 || st->ghosts[0] != 1 || st->ghosts[1] != 1)
+        return fail(ctx, LG_ERR_STATE, "Model C needs a 2-D state with phi and u of ghost width 1");
+    if (p->noise_amplitude != 0.0)
+        return fail(ctx, LG_ERR_INVALID, "RungeKutta4 steps deterministic models only (rk4.rs:15-19): noise must be 0");
+    if (nsteps < 0) return fail(ctx, LG_ERR_INVALID, "negative step count");
+    cudaSetDevice(ctx->device);
+    int rc = rk_workspace(st);
+    if (rc != LG_OK) return rc;
+    if (!st->ghosts_valid) {
+        rc = fill_all_ghosts(st);
+        if (rc != LG_OK) return rc;
+    }
+    lg::ModelCDev m{};
+    m.lambda = p->lambda;
+    m.d_thermal = p->d_thermal;
+    m.a_bar = std::fma(3.0, -p->eps4, 1.0);    // phasefield.rs:101
+    m.eps_prime = 3.0 * p->eps4 / m.a_bar;     // phasefield.rs:109
+    m.tol = p->anisotropy_tol;
+    m.f_a_bar = std::fma(3.0, -p->eps4, 1.0);  // finite_volume.rs:114
+    m.f_eps_prime = 3.0 * p->eps4 / m.f_a_bar;
+    m.f_a12 = 4.0 * m.f_a_bar * m.f_eps_prime;
+    m.f_tol = p->flux_tol;
+    m.inv_h2_flux = 1.0 / (st->grid->spacing[0] * st->grid->spacing[1]);
+    m.inv_h2[0] = 1.0 / (st->grid->spacing[0] * st->grid->spacing[0]);
+    m.inv_h2[1] = 1.0 / (st->grid->spacing[1] * st->grid->spacing[1]);
+    LG_CUDA(ctx, cudaMemcpyAsync(st->d_t + st->tslot, &st->t, sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    const lg::CartTopo topo = topo_of(st->grid);
+    const lg::SlabLayout L = layout_of(st, 0);
+    const int64_t ncells = st->grid->nblocks * st->grid->block[0] * st->grid->block[1];
+    const double half_dt = 0.5 * dt, sixth = dt / 6.0, third = dt / 3.0;  // rk4.rs:57, 74-75
+    char key[512];
+    snprintf(key, sizeof key, "modelc-rk4|%a|%a|%a|%a|%a|dt=%a|orient=%p", p->eps4, p->lambda, p->d_thermal,
+             p->anisotropy_tol, p->flux_tol, dt, st->orient);
+    auto step = [&]() -> int {
+        const void* y = st->arena[st->cur];
+        void* out = st->arena[st->cur ^ 1];
+        void *k1 = st->rk[0], *k2 = st->rk[1], *k3 = st->rk[2], *t0 = st->rk[3], *t1 = st->rk[4];
+        const void* stage_in[4] = {y, t0, t1, t0};
+        void* stage_out[4] = {t0, t1, t0, out};
+        void* stage_k[3] = {k1, k2, k3};
+        const double stage_c[3] = {half_dt, half_dt, dt};
+        cudaError_t e = cudaSuccess;
+        for (int i = 0; i < 4 && e == cudaSuccess; ++i) {
+            const int mode = i < 3 ? 1 : 2;
+            if (st->dtype == LG_F64)
+                e = lg::launch_modelc_rk_stage_f64(
+                    mode, static_cast<const double*>(stage_in[i]), static_cast<double*>(stage_out[i]), topo, L, m,
+                    static_cast<const double*>(y), i < 3 ? static_cast<double*>(stage_k[i]) : nullptr,
+                    static_cast<const double*>(k1), static_cast<const double*>(k2), static_cast<const double*>(k3),
+                    i < 3 ? stage_c[i] : 0.0, sixth, third, static_cast<const double*>(st->orient), ncells, st->d_t,
+                    st->tslot, dt, ctx->stream);
+            else
+                e = lg::launch_modelc_rk_stage_f32(
+                    mode, static_cast<const float*>(stage_in[i]), static_cast<float*>(stage_out[i]), topo, L, m,
+                    static_cast<const float*>(y), i < 3 ? static_cast<float*>(stage_k[i]) : nullptr,
+                    static_cast<const float*>(k1), static_cast<const float*>(k2), static_cast<const float*>(k3),
+                    i < 3 ? stage_c[i] : 0.0, sixth, third, static_cast<const float*>(st->orient), ncells, st->d_t,
+                    st->tslot, dt, ctx->stream);
+        }
+        ctx->launches += 4;
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "Model C RK4 stage launch");
+        st->cur ^= 1;
+        st->tslot ^= 1;
+        return LG_OK;
+    };
+    rc = run_steps(st, key, nsteps, flags, step);
+    if (rc != LG_OK) return rc;
+    advance_time(st, dt, nsteps);
+    return LG_OK;
 }
 
 int lg_modelc_set_orientations(lg_state* st, int theta_field) {

@@ -179,6 +179,57 @@ __global__ void __launch_bounds__(256) heat_step_kernel(const double* __restrict
     }
 }
 
+// One stage of RungeKutta4 (rk4.rs:40-79) for the heat model, one thread
+// per interior cell: k = kappa lap(in) as heat_step_kernel computes it, then
+//   MODE 1: kout = k, out = y + c k          (y_tmp = y; y_tmp += c k_i)
+//   MODE 2: out = (((y + s6 k1) + s3 k2) + s3 k3) + s6 k   (the four axpys)
+// with the output's ghost images pushed for the next stage.
+template <int D, int MODE>
+__global__ void __launch_bounds__(256) heat_rk_kernel(const double* __restrict__ in, double* __restrict__ out,
+                                                      const double* __restrict__ y, double* __restrict__ kout,
+                                                      const double* __restrict__ k1, const double* __restrict__ k2,
+                                                      const double* __restrict__ k3, CartTopo topo, SlabLayout L,
+                                                      int field, double kappa, double ih0, double ih1, double ih2,
+                                                      double c, double s6, double s3) {
+    const int64_t cells = (int64_t)topo.n[0] * (D > 1 ? topo.n[1] : 1) * (D > 2 ? topo.n[2] : 1);
+    const int64_t st1 = L.gdim[0];
+    const int64_t st2 = (int64_t)L.gdim[0] * (D > 1 ? L.gdim[1] : 1);
+    for (int b = blockIdx.y; b < topo.nblocks; b += gridDim.y) {
+        const int64_t base = slab_base(L, b, field);
+        const double* s = in + base;
+        for (int64_t cc = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; cc < cells;
+             cc += (int64_t)gridDim.x * blockDim.x) {
+            int l[3] = {0, 0, 0};
+            int64_t rem = cc;
+            l[0] = (int)(rem % topo.n[0]);
+            rem /= topo.n[0];
+            if (D > 1) { l[1] = (int)(rem % topo.n[1]); rem /= topo.n[1]; }
+            if (D > 2) l[2] = (int)rem;
+            const int64_t o = lin<D>(L, l);
+            const double center = s[o];
+            double acc = 0.0;
+            acc += ((s[o + 1] - (center + center)) + s[o - 1]) * ih0;
+            if (D > 1) acc += ((s[o + st1] - (center + center)) + s[o - st1]) * ih1;
+            if (D > 2) acc += ((s[o + st2] - (center + center)) + s[o - st2]) * ih2;
+            const double k = acc * kappa;
+            const int64_t e = base + o;
+            double v;
+            if (MODE == 1) {
+                kout[e] = k;
+                v = y[e] + c * k;
+            } else {
+                v = y[e];
+                v = v + s6 * k1[e];
+                v = v + s3 * k2[e];
+                v = v + s3 * k3[e];
+                v = v + s6 * k;
+            }
+            out[e] = v;
+            push_ghost_images<D, double>(out, topo, L, field, b, l, v);
+        }
+    }
+}
+
 // asynchronous 8-byte global -> shared copy (completes at cp_async_wait)
 __device__ __forceinline__ void cp_async8(double* smem, const double* gmem) {
     const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
@@ -416,6 +467,28 @@ cudaError_t launch_heat3d_pull(const double* in, double* out, const CartTopo& to
     cfg.numAttrs = 1;
     return cudaLaunchKernelEx(&cfg, heat3d_pull_kernel, in, out, topo, L, field, kappa, dt, inv_h2[0], inv_h2[1],
                               inv_h2[2], zc);
+}
+
+cudaError_t launch_heat_rk_stage(int mode, const double* in, double* out, const double* y, double* kout,
+                                 const double* k1, const double* k2, const double* k3, const CartTopo& topo,
+                                 const SlabLayout& L, int field, double kappa, const double* inv_h2, double c,
+                                 double s6, double s3, cudaStream_t s) {
+    const int64_t cells = (int64_t)topo.n[0] * (topo.D > 1 ? topo.n[1] : 1) * (topo.D > 2 ? topo.n[2] : 1);
+    const dim3 grid((unsigned)std::min<int64_t>((cells + 255) / 256, 1024), (unsigned)std::min(topo.nblocks, 65535));
+#define LG_HRK(DD, MM)                                                                                             \
+    heat_rk_kernel<DD, MM><<<grid, 256, 0, s>>>(in, out, y, kout, k1, k2, k3, topo, L, field, kappa, inv_h2[0],   \
+                                                 inv_h2[1], inv_h2[2], c, s6, s3)
+    if (mode == 1) {
+        if (topo.D == 1) LG_HRK(1, 1);
+        else if (topo.D == 2) LG_HRK(2, 1);
+        else LG_HRK(3, 1);
+    } else {
+        if (topo.D == 1) LG_HRK(1, 2);
+        else if (topo.D == 2) LG_HRK(2, 2);
+        else LG_HRK(3, 2);
+    }
+#undef LG_HRK
+    return cudaGetLastError();
 }
 
 cudaError_t launch_heat_step(const double* in, double* out, const CartTopo& topo, const SlabLayout& L, int field,

@@ -57,6 +57,15 @@ cudaError_t launch_modelc_step_f32(const float* in, float* out, const CartTopo& 
                                    const ModelCDev& m, double dt, const NoiseDev& nz, double* tdev, int slot,
                                    int variant, cudaStream_t s);
 
+// One RungeKutta4 stage of the heat model (rk4.rs:40-79): mode 1 writes
+// k = kappa lap(in) to kout and y + c k to out; mode 2 writes
+// (((y + s6 k1) + s3 k2) + s3 k3) + s6 k to out.  Ghost images of out are
+// pushed.  FP64, any dimension, bit-identical to the reference's stages.
+cudaError_t launch_heat_rk_stage(int mode, const double* in, double* out, const double* y, double* kout,
+                                 const double* k1, const double* k2, const double* k3, const CartTopo& topo,
+                                 const SlabLayout& L, int field, double kappa, const double* inv_h2, double c,
+                                 double s6, double s3, cudaStream_t s);
+
 // Warp-strip variants of the same steps (lg_modelc.cu, lg_modelc_f32.cu):
 // each face flux is evaluated once and shared by its two cells; `rows` rows
 // of one block per warp (0 = chosen from the grid); `minb` = CTAs per SM
@@ -80,6 +89,22 @@ cudaError_t launch_modelc_oriented_f64(const double* in, double* out, const Cart
 cudaError_t launch_modelc_oriented_f32(const float* in, float* out, const CartTopo& topo, const SlabLayout& L,
                                        const ModelCDev& m, double dt, const NoiseDev& nz, double* tdev, int slot,
                                        const float* trig, int64_t ncells, int rows, cudaStream_t s);
+
+// One RungeKutta4 stage of Model C without noise (rk4.rs:40-79) on the
+// strip schedule: mode 1 writes the drift of `in` to k and y + c k to out;
+// mode 2 writes (((y + s6 k1) + s3 k2) + s3 k3) + s6 k4 to out.  trig
+// (cos then sin theta0, or null) selects the multi-grain form.  FP64 is
+// bit-identical to the reference's stages.
+cudaError_t launch_modelc_rk_stage_f64(int mode, const double* in, double* out, const CartTopo& topo,
+                                       const SlabLayout& L, const ModelCDev& m, const double* y, double* k,
+                                       const double* k1, const double* k2, const double* k3, double c, double s6,
+                                       double s3, const double* trig, int64_t ncells, double* tdev, int slot,
+                                       double dt, cudaStream_t s);
+cudaError_t launch_modelc_rk_stage_f32(int mode, const float* in, float* out, const CartTopo& topo,
+                                       const SlabLayout& L, const ModelCDev& m, const float* y, float* k,
+                                       const float* k1, const float* k2, const float* k3, double c, double s6,
+                                       double s3, const float* trig, int64_t ncells, double* tdev, int slot,
+                                       double dt, cudaStream_t s);
 
 // Batched instances (an ensemble of independent grids of one geometry):
 // block b of the topology belongs to instance b / bpi, with the parameter

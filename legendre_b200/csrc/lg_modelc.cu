@@ -33,6 +33,22 @@ cudaError_t launch_modelc_oriented_f64(const double* in, double* out, const Cart
     return launch_strip_oriented<double, OpsExact<double>, false, 2>(in, out, g, mc, dt, scale_amp, oa, s);
 }
 
+cudaError_t launch_modelc_rk_stage_f64(int mode, const double* in, double* out, const CartTopo& topo,
+                                       const SlabLayout& L, const ModelCDev& m, const double* y, double* k,
+                                       const double* k1, const double* k2, const double* k3, double c, double s6,
+                                       double s3, const double* trig, int64_t ncells, double* tdev, int slot,
+                                       double dt, cudaStream_t s) {
+    TileArgs g{topo, L, dt, 0, tdev, slot, 0, 0, 0, 0};
+    const MC<double> mc = to_mc<double>(m);
+    const OrientArgs oa{trig, ncells};
+    const RkArgs<double> rk{y, k, k1, k2, k3, c, s6, s3};
+    if (mode == 1)
+        return trig ? launch_strip_rk<double, OpsExact<double>, 1, true>(in, out, g, mc, dt, oa, rk, s)
+                    : launch_strip_rk<double, OpsExact<double>, 1, false>(in, out, g, mc, dt, oa, rk, s);
+    return trig ? launch_strip_rk<double, OpsExact<double>, 2, true>(in, out, g, mc, dt, oa, rk, s)
+                : launch_strip_rk<double, OpsExact<double>, 2, false>(in, out, g, mc, dt, oa, rk, s);
+}
+
 size_t modelc_record_size_f64() { return sizeof(MC<double>); }
 void modelc_record_f64(const ModelCDev& m, void* out) { *static_cast<MC<double>*>(out) = to_mc<double>(m); }
 

@@ -159,6 +159,22 @@ cudaError_t launch_modelc_oriented_f32(const float* in, float* out, const CartTo
     return launch_strip_oriented<float, OpsFast32, false, 2>(in, out, g, f, (float)dt, scale_amp, oa, s);
 }
 
+cudaError_t launch_modelc_rk_stage_f32(int mode, const float* in, float* out, const CartTopo& topo,
+                                       const SlabLayout& L, const ModelCDev& m, const float* y, float* k,
+                                       const float* k1, const float* k2, const float* k3, double c, double s6,
+                                       double s3, const float* trig, int64_t ncells, double* tdev, int slot,
+                                       double dt, cudaStream_t s) {
+    TileArgs g{topo, L, dt, 0, tdev, slot, 0, 0, 0, 0};
+    const Fast32 f = fast32_of(m);
+    const OrientArgs oa{trig, ncells};
+    const RkArgs<float> rk{y, k, k1, k2, k3, (float)c, (float)s6, (float)s3};
+    if (mode == 1)
+        return trig ? launch_strip_rk<float, OpsFast32, 1, true>(in, out, g, f, (float)dt, oa, rk, s)
+                    : launch_strip_rk<float, OpsFast32, 1, false>(in, out, g, f, (float)dt, oa, rk, s);
+    return trig ? launch_strip_rk<float, OpsFast32, 2, true>(in, out, g, f, (float)dt, oa, rk, s)
+                : launch_strip_rk<float, OpsFast32, 2, false>(in, out, g, f, (float)dt, oa, rk, s);
+}
+
 size_t modelc_record_size_f32() { return sizeof(Fast32); }
 void modelc_record_f32(const ModelCDev& m, void* out) { *static_cast<Fast32*>(out) = fast32_of(m); }
 

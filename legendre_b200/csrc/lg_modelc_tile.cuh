@@ -64,6 +64,54 @@ struct BatchArgs {
     int bpi;
 };
 
+// RungeKutta4 stages (MODE 1, 2; rk4.rs:40-79).  All arenas share the
+// state's slab layout.  MODE 1: k receives the drift of the input, the output
+// is y + c k (y_tmp = y; y_tmp += c k_i).  MODE 2: the output is
+// (((y + s6 k1) + s3 k2) + s3 k3) + s6 k4, k4 the drift of the input.
+template <class T>
+struct RkArgs {
+    const T* y;
+    T* k;
+    const T* k1;
+    const T* k2;
+    const T* k3;
+    T c, s6, s3;
+};
+
+// The new phi and u of a cell from its drift (kphi, ku): the Euler-Maruyama
+// update (MODE 0) or a RungeKutta4 stage (MODE 1, 2); e0/e1 index the cell's
+// phi/u entries in any arena of the state's layout.
+template <class T, class Ops, bool NOISE, int MODE>
+__device__ __forceinline__ void cell_update(const RkArgs<T>& rk, T dt, T scale_amp, T nval, T kphi, T ku, T p, T uc,
+                                            int64_t e0, int64_t e1, bool ok, T& phin, T& un) {
+    if constexpr (MODE == 0) {
+        phin = Ops::axpy(dt, kphi, p);
+        if (NOISE) phin = Ops::add_noise(phin, scale_amp, nval);
+        un = Ops::axpy(dt, ku, uc);
+    } else if constexpr (MODE == 1) {
+        phin = un = T(0);  // cells that store nothing read nothing either
+        if (ok) {
+            rk.k[e0] = kphi;
+            rk.k[e1] = ku;
+            phin = rk.y[e0] + rk.c * kphi;
+            un = rk.y[e1] + rk.c * ku;
+        }
+    } else {
+        phin = un = T(0);
+        if (!ok) return;
+        phin = rk.y[e0];
+        phin = phin + rk.s6 * rk.k1[e0];
+        phin = phin + rk.s3 * rk.k2[e0];
+        phin = phin + rk.s3 * rk.k3[e0];
+        phin = phin + rk.s6 * kphi;
+        un = rk.y[e1];
+        un = un + rk.s6 * rk.k1[e1];
+        un = un + rk.s3 * rk.k2[e1];
+        un = un + rk.s3 * rk.k3[e1];
+        un = un + rk.s6 * ku;
+    }
+}
+
 // Multi-grain kernels (ORIENT): cos theta0 of every interior cell, blocks in
 // order and each block's cells dimension-0-fastest, followed by sin theta0
 // in the same order (ncells values each), in the kernel's element type.
@@ -88,7 +136,7 @@ __device__ __forceinline__ bool same_bits(float a, float b) { return __float_as_
 // receive the prefetch of row j+1+PF.  `off` is the slab offset of (col, j); ph/uu/po/uo
 // are the warp's slab bases.  NX > 0 fixes the block width (and the row
 // stride) at compile time; FULL means every lane owns a column.
-template <class T, class Ops, bool NOISE, int NX, bool FULL, int PF, bool TAIL, bool ORIENT>
+template <class T, class Ops, bool NOISE, int NX, bool FULL, int PF, bool TAIL, bool ORIENT, int MODE>
 __device__ __forceinline__ void strip_row(const typename Ops::Params& m, const TileArgs& g, int j, int r0, int r1,
                                           int lane,
                                           int col, bool valid, int last_lane, int n0, int n1, int off,
@@ -97,7 +145,7 @@ __device__ __forceinline__ void strip_row(const typename Ops::Params& m, const T
                                           uint64_t block_key, T bnd, const Row3<T>& A, const Row3<T>& B,
                                           const Row3<T>& C, Row3<T>& P, T UA, T UB, T UC, T& UP, T& jb, T dt,
                                           T scale_amp, const T* __restrict__ trig_b, int64_t ncells, T& cprev,
-                                          T& sprev, T& cnext, T& snext) {
+                                          T& sprev, T& cnext, T& snext, const RkArgs<T>& rk) {
     const int sy = NX > 0 ? NX + 2 : g.L.gdim[0];
     // lanes past the block's last column (valid false) run the same code on
     // a clamped column and only skip the stores: no branch splits the face,
@@ -151,9 +199,9 @@ __device__ __forceinline__ void strip_row(const typename Ops::Params& m, const T
             jbot = Ops::oyface(m, c0, s0, q * (B.c - B.a + A.c - A.a), B.b - A.b);
         T kphi, ku;
         Ops::ocell(m, jr, jl, jt, jbot, B.b, B.c - B.a, C.b - A.b, c0, s0, UB, ul, ur, UC, UA, kphi, ku);
-        T phin = Ops::axpy(dt, kphi, B.b);
-        if (NOISE) phin = Ops::add_noise(phin, scale_amp, nval);
-        const T un = Ops::axpy(dt, ku, UB);
+        T phin, un;
+        cell_update<T, Ops, NOISE, MODE>(rk, dt, scale_amp, nval, kphi, ku, B.b, UB, (po - out) + off,
+                                         (uo - out) + off, ok, phin, un);
         if (ok) {
             po[off] = phin;
             uo[off] = un;
@@ -175,9 +223,9 @@ __device__ __forceinline__ void strip_row(const typename Ops::Params& m, const T
     if (lane == last_lane) fr = fb;
     T kphi, ku;
     Ops::cell(m, fr, fl, jt, jb, B.b, B.c - B.a, C.b - A.b, UB, ul, ur, UC, UA, kphi, ku);
-    T phin = Ops::axpy(dt, kphi, B.b);
-    if (NOISE) phin = Ops::add_noise(phin, scale_amp, nval);
-    const T un = Ops::axpy(dt, ku, UB);
+    T phin, un;
+    cell_update<T, Ops, NOISE, MODE>(rk, dt, scale_amp, nval, kphi, ku, B.b, UB, (po - out) + off, (uo - out) + off,
+                                     ok, phin, un);
     if (ok) {
         po[off] = phin;
         uo[off] = un;
@@ -192,13 +240,13 @@ __device__ __forceinline__ void strip_row(const typename Ops::Params& m, const T
 // One work unit of the strip kernel: the rows [r0, r1) of the 32-column
 // strip at c0 of block b, with the parameter record m (the kernel parameter,
 // or a batched instance's record) and the Wiener key of block key_block.
-template <class T, class Ops, bool NOISE, int NX, bool FULL, int PF, bool TAIL, bool ORIENT>
+template <class T, class Ops, bool NOISE, int NX, bool FULL, int PF, bool TAIL, bool ORIENT, int MODE>
 __device__ __forceinline__ void strip_unit(const typename Ops::Params& m, uint64_t seed, int key_block,
                                            const TileArgs& g, const T* __restrict__ ph, const T* __restrict__ uu,
                                            T* __restrict__ out, T* __restrict__ po, T* __restrict__ uo,
                                            const Nbr2& nb, int r0, int r1, int lane, int col, bool valid,
                                            int last_lane, int cr, bool edge_x, int n0, int n1, int sy, double tnow,
-                                           T dt, T scale_amp, const T* __restrict__ trig_b, int64_t ncells) {
+                                           T dt, T scale_amp, const T* __restrict__ trig_b, int64_t ncells, const RkArgs<T>& rk) {
     constexpr int NB = PF + 3;
     uint64_t block_key = 0;
     if (NOISE)
@@ -260,11 +308,11 @@ __device__ __forceinline__ void strip_unit(const typename Ops::Params& m, uint64
     }
 
 #define LG_ROW(J, Q)                                                                                            \
-    strip_row<T, Ops, NOISE, NX, FULL, PF, TAIL, ORIENT>(m, g, J, r0, r1, lane, col, valid, last_lane, n0, n1, off, ph, uu, out, po,  \
+    strip_row<T, Ops, NOISE, NX, FULL, PF, TAIL, ORIENT, MODE>(m, g, J, r0, r1, lane, col, valid, last_lane, n0, n1, off, ph, uu, out, po,  \
                                        uo, nb, edge_x, block_key, bnd, w[(Q) % NB], w[((Q) + 1) % NB],          \
                                        w[((Q) + 2) % NB], w[((Q) + 2 + PF) % NB], uw[(Q) % NB],                \
                                        uw[((Q) + 1) % NB], uw[((Q) + 2) % NB], uw[((Q) + 2 + PF) % NB], jb, dt, \
-                                       scale_amp, trig_b, ncells, cpv, spv, cnx, snx);                                                              \
+                                       scale_amp, trig_b, ncells, cpv, spv, cnx, snx, rk);                                                              \
     off += sy
     for (int j = r0; j < r1; j += NB) {
 #pragma unroll
@@ -276,10 +324,10 @@ __device__ __forceinline__ void strip_unit(const typename Ops::Params& m, uint64
 // Rows per work unit are at most 32, so one batch of boundary faces (lanes
 // across rows) serves the whole unit.
 template <class T, class Ops, bool NOISE, int MINB, int NX, int PF, bool BATCH = false, bool TAIL = false,
-          bool ORIENT = false>
+          bool ORIENT = false, int MODE = 0>
 __global__ void __launch_bounds__(256, MINB)
     modelc_strip_kernel(const T* __restrict__ in, T* __restrict__ out, TileArgs g, typename Ops::Params m0, T dt,
-                        T scale_amp, BatchArgs bt, OrientArgs oa) {
+                        T scale_amp, BatchArgs bt, OrientArgs oa, RkArgs<T> rk) {
     constexpr bool FULL = NX > 0 && NX % 32 == 0;
     const CartTopo& topo = g.topo;
     const int n0 = NX > 0 ? NX : topo.n[0];
@@ -293,7 +341,7 @@ __global__ void __launch_bounds__(256, MINB)
     // writes t + dt to the other slot (simulation.rs:285), so a captured
     // sequence of steps needs no host-side time.
     const double tnow = g.tdev[g.slot];
-    if (blockIdx.x == 0 && threadIdx.x == 0) g.tdev[g.slot ^ 1] = tnow + g.dt64;
+    if (MODE != 1 && blockIdx.x == 0 && threadIdx.x == 0) g.tdev[g.slot ^ 1] = tnow + g.dt64;
 
     for (int64_t unit = (int64_t)blockIdx.x * wpc + (threadIdx.x >> 5); unit < g.units;
          unit += (int64_t)gridDim.x * wpc) {
@@ -325,15 +373,16 @@ __global__ void __launch_bounds__(256, MINB)
         if constexpr (BATCH) {
             const int inst = b / bt.bpi;
             const typename Ops::Params mi = static_cast<const typename Ops::Params*>(bt.params)[inst];
-            strip_unit<T, Ops, NOISE, NX, FULL, PF, TAIL, ORIENT>(
+            strip_unit<T, Ops, NOISE, NX, FULL, PF, TAIL, ORIENT, MODE>(
                 mi, bt.seeds[inst], b - inst * bt.bpi, g, ph, uu, out, po, uo, nb, r0, r1, lane, col, valid, last_lane,
-                cr, edge_x, n0, n1, sy, tnow, dt, scale_amp, nullptr, 0);
+                cr, edge_x, n0, n1, sy, tnow, dt, scale_amp, nullptr, 0, rk);
         } else {
             // multi-grain: this block's cos theta0 (sin theta0 follows ncells later)
             const T* trig_b = ORIENT ? static_cast<const T*>(oa.trig) + (int64_t)b * n0 * n1 : nullptr;
-            strip_unit<T, Ops, NOISE, NX, FULL, PF, TAIL, ORIENT>(m0, g.seed, b, g, ph, uu, out, po, uo, nb, r0, r1,
-                                                                  lane, col, valid, last_lane, cr, edge_x, n0, n1, sy,
-                                                                  tnow, dt, scale_amp, trig_b, oa.ncells);
+            strip_unit<T, Ops, NOISE, NX, FULL, PF, TAIL, ORIENT, MODE>(m0, g.seed, b, g, ph, uu, out, po, uo, nb,
+                                                                        r0, r1, lane, col, valid, last_lane, cr,
+                                                                        edge_x, n0, n1, sy, tnow, dt, scale_amp,
+                                                                        trig_b, oa.ncells, rk);
         }
     }
 }
@@ -380,13 +429,13 @@ cudaError_t launch_strip_batch(const T* in, T* out, TileArgs g, BatchArgs bt, T 
     const dim3 grid = strip_ctas(g), block(256);
     const typename Ops::Params m{};
     if (tail) {
-        modelc_strip_kernel<T, Ops, NOISE, MINB, 0, 1, true, true><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp, bt, OrientArgs{});
+        modelc_strip_kernel<T, Ops, NOISE, MINB, 0, 1, true, true><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp, bt, OrientArgs{}, RkArgs<T>{});
         return cudaGetLastError();
     }
     switch (g.topo.n[0]) {
-        case 32: modelc_strip_kernel<T, Ops, NOISE, MINB, 32, 1, true><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp, bt, OrientArgs{}); break;
-        case 64: modelc_strip_kernel<T, Ops, NOISE, MINB, 64, 1, true><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp, bt, OrientArgs{}); break;
-        default: modelc_strip_kernel<T, Ops, NOISE, MINB, 0, 1, true><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp, bt, OrientArgs{});
+        case 32: modelc_strip_kernel<T, Ops, NOISE, MINB, 32, 1, true><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp, bt, OrientArgs{}, RkArgs<T>{}); break;
+        case 64: modelc_strip_kernel<T, Ops, NOISE, MINB, 64, 1, true><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp, bt, OrientArgs{}, RkArgs<T>{}); break;
+        default: modelc_strip_kernel<T, Ops, NOISE, MINB, 0, 1, true><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp, bt, OrientArgs{}, RkArgs<T>{});
     }
     return cudaGetLastError();
 }
@@ -397,16 +446,16 @@ cudaError_t launch_strip_minb(const T* in, T* out, TileArgs g, const typename Op
     const bool tail = strip_plan(g, PF + 3);
     const dim3 grid = strip_ctas(g), block(256);
     if (tail) {
-        modelc_strip_kernel<T, Ops, NOISE, MINB, 0, PF, false, true><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp, BatchArgs{}, OrientArgs{});
+        modelc_strip_kernel<T, Ops, NOISE, MINB, 0, PF, false, true><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp, BatchArgs{}, OrientArgs{}, RkArgs<T>{});
         return cudaGetLastError();
     }
     switch (g.topo.n[0]) {  // block widths of the shipped configurations get a compile-time row stride
-        case 32: modelc_strip_kernel<T, Ops, NOISE, MINB, 32, PF><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp, BatchArgs{}, OrientArgs{}); break;
-        case 64: modelc_strip_kernel<T, Ops, NOISE, MINB, 64, PF><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp, BatchArgs{}, OrientArgs{}); break;
-        case 126: modelc_strip_kernel<T, Ops, NOISE, MINB, 126, PF><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp, BatchArgs{}, OrientArgs{}); break;
-        case 128: modelc_strip_kernel<T, Ops, NOISE, MINB, 128, PF><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp, BatchArgs{}, OrientArgs{}); break;
-        case 256: modelc_strip_kernel<T, Ops, NOISE, MINB, 256, PF><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp, BatchArgs{}, OrientArgs{}); break;
-        default: modelc_strip_kernel<T, Ops, NOISE, MINB, 0, PF><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp, BatchArgs{}, OrientArgs{});
+        case 32: modelc_strip_kernel<T, Ops, NOISE, MINB, 32, PF><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp, BatchArgs{}, OrientArgs{}, RkArgs<T>{}); break;
+        case 64: modelc_strip_kernel<T, Ops, NOISE, MINB, 64, PF><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp, BatchArgs{}, OrientArgs{}, RkArgs<T>{}); break;
+        case 126: modelc_strip_kernel<T, Ops, NOISE, MINB, 126, PF><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp, BatchArgs{}, OrientArgs{}, RkArgs<T>{}); break;
+        case 128: modelc_strip_kernel<T, Ops, NOISE, MINB, 128, PF><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp, BatchArgs{}, OrientArgs{}, RkArgs<T>{}); break;
+        case 256: modelc_strip_kernel<T, Ops, NOISE, MINB, 256, PF><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp, BatchArgs{}, OrientArgs{}, RkArgs<T>{}); break;
+        default: modelc_strip_kernel<T, Ops, NOISE, MINB, 0, PF><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp, BatchArgs{}, OrientArgs{}, RkArgs<T>{});
     }
     return cudaGetLastError();
 }
@@ -419,14 +468,28 @@ cudaError_t launch_strip_oriented(const T* in, T* out, TileArgs g, const typenam
     const bool tail = strip_plan(g, 1 + 3);
     const dim3 grid = strip_ctas(g), block(256);
     if (tail) {
-        modelc_strip_kernel<T, Ops, NOISE, MINB, 0, 1, false, true, true><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp, BatchArgs{}, oa);
+        modelc_strip_kernel<T, Ops, NOISE, MINB, 0, 1, false, true, true><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp, BatchArgs{}, oa, RkArgs<T>{});
         return cudaGetLastError();
     }
     switch (g.topo.n[0]) {
-        case 126: modelc_strip_kernel<T, Ops, NOISE, MINB, 126, 1, false, false, true><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp, BatchArgs{}, oa); break;
-        case 256: modelc_strip_kernel<T, Ops, NOISE, MINB, 256, 1, false, false, true><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp, BatchArgs{}, oa); break;
-        default: modelc_strip_kernel<T, Ops, NOISE, MINB, 0, 1, false, false, true><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp, BatchArgs{}, oa);
+        case 126: modelc_strip_kernel<T, Ops, NOISE, MINB, 126, 1, false, false, true><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp, BatchArgs{}, oa, RkArgs<T>{}); break;
+        case 256: modelc_strip_kernel<T, Ops, NOISE, MINB, 256, 1, false, false, true><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp, BatchArgs{}, oa, RkArgs<T>{}); break;
+        default: modelc_strip_kernel<T, Ops, NOISE, MINB, 0, 1, false, false, true><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp, BatchArgs{}, oa, RkArgs<T>{});
     }
+    return cudaGetLastError();
+}
+
+// RungeKutta4 stages of Model C (deterministic: no noise), axis-aligned or
+// multi-grain, any block width
+template <class T, class Ops, int MODE, bool ORIENT>
+cudaError_t launch_strip_rk(const T* in, T* out, TileArgs g, const typename Ops::Params& m, T dt, OrientArgs oa,
+                            RkArgs<T> rk, cudaStream_t s) {
+    const bool tail = strip_plan(g, 1 + 3);
+    const dim3 grid = strip_ctas(g), block(256);
+    if (tail)
+        modelc_strip_kernel<T, Ops, false, 2, 0, 1, false, true, ORIENT, MODE><<<grid, block, 0, s>>>(in, out, g, m, dt, T(0), BatchArgs{}, oa, rk);
+    else
+        modelc_strip_kernel<T, Ops, false, 2, 0, 1, false, false, ORIENT, MODE><<<grid, block, 0, s>>>(in, out, g, m, dt, T(0), BatchArgs{}, oa, rk);
     return cudaGetLastError();
 }
 

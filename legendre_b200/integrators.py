@@ -60,6 +60,32 @@ class EulerMaruyama:
         _run(sim, dt, nsteps, seed=self.seed, graph=graph, variant=variant)
 
 
+@dataclass
+class RungeKutta4:
+    """Classic fourth-order Runge-Kutta (rk4.rs:13-79), deterministic models
+    only (the reference enforces NoNoise): Model C with no noise, or heat.
+    Four fused stage launches per step on the device."""
+
+    def suggested_dt(self, model, grid):
+        return model.stable_dt(grid.spacing)
+
+    def validate(self, model, grid, disc):
+        if model.stochastic_drivers() or getattr(model, "noise_amplitude", 0.0) != 0.0:
+            raise TypeError("RungeKutta4 integrates deterministic models only; use EulerMaruyama")
+        _validate_model(model, grid, disc)
+
+    def run(self, sim, dt, nsteps, graph=False, variant=0):
+        st = sim.state
+        ctx = sim.scheduler.handle
+        if isinstance(sim.model, ModelC):
+            p = sim.model.params(flux_tol=sim.disc.tol)
+            N.check(N.lib.lg_modelc_rk4_run(st.handle, C.byref(p), dt, nsteps, _flags(graph)), ctx)
+        elif isinstance(sim.model, Heat):
+            N.check(N.lib.lg_heat_rk4_run(st.handle, sim.model.u, sim.model.kappa, dt, nsteps, _flags(graph)), ctx)
+        else:
+            raise TypeError(f"no device path for model {type(sim.model).__name__}")
+
+
 def _validate_model(model, grid, disc):
     if isinstance(model, ModelC):
         if grid.dim != 2:

@@ -277,6 +277,59 @@ void modelc_initialize_grains(const Grid& grid, State& st, const double* grains,
     }
 }
 
+// RungeKutta4::step (src/integrators/rk4.rs:40-79) over the fields `fields`
+// of a state: k1 = f(y); y_tmp = y; y_tmp += (0.5 dt) k1; k2 = f(y_tmp);
+// y_tmp = y; y_tmp += (0.5 dt) k2; k3 = f(y_tmp); y_tmp = y; y_tmp += dt k3;
+// k4 = f(y_tmp); y += (dt/6) k1; y += (dt/3) k2; y += (dt/3) k3;
+// y += (dt/6) k4.  Copies and axpys run over every slab entry (state.rs:
+// 559-568); a drift writes interior entries only (tendency ghosts stay 0)
+// and fills the ghosts of its input first (StepCtx::eval_drift).  Static
+// fields (theta0) are copied into y_tmp and never stepped.
+template <class Drift>
+double rk4_run(const Grid& grid, State& st, const std::vector<int>& fields, double t, double dt, int64_t steps,
+               int nthreads, Drift drift) {
+    const int64_t nb = grid.num_blocks();
+    const size_t nf = fields.size();
+    auto zeros = [&]() {
+        std::vector<std::vector<std::vector<double>>> k(nf);
+        for (size_t i = 0; i < nf; ++i)
+            k[i].assign(nb, std::vector<double>(grid.block_len(st.ghost[fields[i]]), 0.0));
+        return k;
+    };
+    auto k1 = zeros(), k2 = zeros(), k3 = zeros(), k4 = zeros();
+    State tmp = st;
+    const double half_dt = 0.5 * dt, sixth = dt / 6.0, third = dt / 3.0;
+    auto axpy = [&](State& x, double a, std::vector<std::vector<std::vector<double>>>& k) {
+        parallel_blocks(nb, nthreads, [&](int64_t b) {
+            for (size_t i = 0; i < nf; ++i) {
+                std::vector<double>& xs = x.slab[b][fields[i]];
+                for (size_t e = 0; e < xs.size(); ++e) xs[e] += a * k[i][b][e];
+            }
+        });
+    };
+    auto copy = [&]() {
+        for (int64_t b = 0; b < nb; ++b) tmp.slab[b] = st.slab[b];
+    };
+    for (int64_t s = 0; s < steps; ++s) {
+        drift(st, k1);
+        copy();
+        axpy(tmp, half_dt, k1);
+        drift(tmp, k2);
+        copy();
+        axpy(tmp, half_dt, k2);
+        drift(tmp, k3);
+        copy();
+        axpy(tmp, dt, k3);
+        drift(tmp, k4);
+        axpy(st, sixth, k1);
+        axpy(st, third, k2);
+        axpy(st, third, k3);
+        axpy(st, sixth, k4);
+        t += dt;
+    }
+    return t;
+}
+
 // phasefield.rs:286-311: theta0 by nearest-seed Voronoi.  Per block, the
 // candidates are the grains whose box distance is at most the smallest
 // farthest-corner distance of any grain; each cell takes the orientation of
@@ -410,6 +463,42 @@ void orc_fill_ghosts_mirror(const void* grid, void* s, int f) {
 double orc_heat_run(const void* grid, void* s, int f, double kappa, double t0, double dt, int64_t steps,
                     int nthreads) {
     return heat_run(*static_cast<const Grid*>(grid), *static_cast<State*>(s), f, kappa, t0, dt, steps, nthreads);
+}
+
+double orc_heat_run_rk4(const void* grid, void* s, int f, double kappa, double t0, double dt, int64_t steps,
+                        int nthreads) {
+    const Grid& g = *static_cast<const Grid*>(grid);
+    State& st = *static_cast<State*>(s);
+    const Ext e = ext_of(g);
+    return rk4_run(g, st, {f}, t0, dt, steps, nthreads, [&](State& y, std::vector<std::vector<std::vector<double>>>& k) {
+        fill_ghosts_mirror(g, y, f);
+        parallel_blocks(g.num_blocks(), nthreads,
+                        [&](int64_t b) { heat_drift_block(e, g.spacing, kappa, y.slab[b][f].data(), k[0][b].data()); });
+    });
+}
+
+// Model C (no noise: RK4 pairs with NoNoise, rk4.rs:15-19) with
+// RungeKutta4; theta_field >= 0 for the multi-grain form.
+double orc_modelc_run_rk4(const void* grid, void* s, const orc_modelc_params* p, int theta_field, double t0,
+                          double dt, int64_t steps, int nthreads) {
+    const Grid& g = *static_cast<const Grid*>(grid);
+    State& st = *static_cast<State*>(s);
+    const ModelC m = make_model(p);
+    const Ext e = ext_of(g);
+    return rk4_run(g, st, {0, 1}, t0, dt, steps, nthreads,
+                   [&](State& y, std::vector<std::vector<std::vector<double>>>& k) {
+                       fill_ghosts_mirror(g, y, 0);
+                       fill_ghosts_mirror(g, y, 1);
+                       parallel_blocks(g.num_blocks(), nthreads, [&](int64_t b) {
+                           if (theta_field >= 0)
+                               modelc_drift_block_oriented(e, g.spacing, m, y.slab[b][0].data(), y.slab[b][1].data(),
+                                                           y.slab[b][theta_field].data(), k[0][b].data(),
+                                                           k[1][b].data());
+                           else
+                               modelc_drift_block(e, g.spacing, m, y.slab[b][0].data(), y.slab[b][1].data(),
+                                                  k[0][b].data(), k[1][b].data());
+                       });
+                   });
 }
 
 double orc_modelc_run(const void* grid, void* s, const orc_modelc_params* p, double t0, double dt, uint64_t seed,

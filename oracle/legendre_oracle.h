@@ -58,6 +58,11 @@ double orc_modelc_run_oriented(const void* grid, void* s, const orc_modelc_param
                                double dt, uint64_t seed, int64_t steps, int wiener, int nthreads);
 void orc_modelc_initialize_orientations(const void* grid, void* s, int theta_field, const double* grains,
                                         int64_t n);
+/* RungeKutta4 (rk4.rs:40-79): heat on field f, Model C without noise */
+double orc_heat_run_rk4(const void* grid, void* s, int f, double kappa, double t0, double dt, int64_t steps,
+                        int nthreads);
+double orc_modelc_run_rk4(const void* grid, void* s, const orc_modelc_params* p, int theta_field, double t0,
+                          double dt, int64_t steps, int nthreads);
 int orc_num_threads_available(void);
 
 #ifdef __cplusplus

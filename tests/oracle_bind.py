@@ -53,6 +53,8 @@ def _load():
         "orc_modelc_initialize_grains": (None, [p, p, pd, i64, d]),
         "orc_modelc_run_oriented": (d, [p, p, C.POINTER(Params), C.c_int, d, d, u64, i64, C.c_int, C.c_int]),
         "orc_modelc_initialize_orientations": (None, [p, p, C.c_int, pd, i64]),
+        "orc_heat_run_rk4": (d, [p, p, C.c_int, d, d, d, i64, C.c_int]),
+        "orc_modelc_run_rk4": (d, [p, p, C.POINTER(Params), C.c_int, d, d, i64, C.c_int]),
         "orc_num_threads_available": (C.c_int, []),
     }
     for name, (res, args) in sigs.items():
@@ -162,6 +164,12 @@ class State:
     def modelc_run_oriented(self, params: Params, theta_field, t0, dt, seed, steps, wiener, threads=1):
         return lib.orc_modelc_run_oriented(self.grid.h, self.h, C.byref(params), theta_field, t0, dt, seed, steps,
                                            int(wiener), threads)
+
+    def heat_run_rk4(self, f, kappa, t0, dt, steps, threads=1):
+        return lib.orc_heat_run_rk4(self.grid.h, self.h, f, kappa, t0, dt, steps, threads)
+
+    def modelc_run_rk4(self, params: Params, t0, dt, steps, theta_field=-1, threads=1):
+        return lib.orc_modelc_run_rk4(self.grid.h, self.h, C.byref(params), theta_field, t0, dt, steps, threads)
 
     def initialize_orientations(self, theta_field, grains):
         """grains: (x, y, radius, orientation) tuples."""
