@@ -182,8 +182,8 @@ def make_sim(cfg, dtype, sched, seed_offset=0):
     model.d_thermal = cfg["d_thermal"]
     if cfg.get("orient"):
         model.with_orientations()
-    sim = L.Simulation(grid, L.FiniteVolume(), model, L.EulerMaruyama(cfg["seed"] + seed_offset), sched,
-                       L.CudaAllocator(dtype))
+    integrator = L.RungeKutta4() if cfg.get("integrator") == "rk4" else L.EulerMaruyama(cfg["seed"] + seed_offset)
+    sim = L.Simulation(grid, L.FiniteVolume(), model, integrator, sched, L.CudaAllocator(dtype))
     grains = L.seed_positions(n, h, cfg["grains"], cfg["seed"], radius=cfg["radius"], orient=cfg.get("orient", False))
     return sim, grid, model, grains
 
@@ -605,6 +605,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cells", type=int, default=None, help="override the grid's cells per dimension (small cases)")
     ap.add_argument("--instances", type=int, default=None, help="override the ensemble's instance count")
+    ap.add_argument("--integrator", default="em", choices=["em", "rk4"],
+                    help="rk4: RungeKutta4 (deterministic: the noise amplitude is set to 0)")
     ap.add_argument("--observe-every", type=int, default=0,
                     help="also time the run with an AsyncObserver snapshotting phi and u every N steps")
     args = ap.parse_args()
@@ -613,6 +615,10 @@ def main():
     cfg = dict(CONFIGS[args.config])
     if args.noise is not None:
         cfg["noise"] = args.noise
+    if args.integrator == "rk4":
+        cfg["integrator"] = "rk4"
+        cfg["noise"] = 0.0
+        cfg["workload"] += "_rk4"
     if args.cells is not None:
         cfg["cells"] = args.cells
         cfg["workload"] += f"_cells{args.cells}"
@@ -648,7 +654,7 @@ def main():
     # the project's autotuner picks the step variant for this shape unless
     # one is forced; warm-up (also captures the step graph)
     tuned = None
-    if args.variant == 0:
+    if args.variant == 0 and cfg.get("integrator") != "rk4":  # the tuner times the Euler-Maruyama step
         tuned, _ = sim.autotune(dt, trial_steps=10)
     sim.run(dt, args.warmup, graph=True, variant=args.variant)
     torch.cuda.synchronize()
@@ -743,8 +749,14 @@ def main():
 
     if rank == 0:
         peak, peak_kind = peaks()
-        # the multi-grain step also reads cos and sin theta0 of every cell
-        bpc = BYTES_PER_CELL[args.dtype] + (2 * (8 if args.dtype == "f64" else 4) if cfg.get("orient") else 0)
+        # the multi-grain step also reads cos and sin theta0 of every cell;
+        # an RK4 step is four stages: three read their input and y and write
+        # k and the next input (phi and u of each: 8 values), the last reads
+        # its input, y and k1..k3 and writes y (12 values): 36 values per cell
+        esz_ = 8 if args.dtype == "f64" else 4
+        bpc = BYTES_PER_CELL[args.dtype] + (2 * esz_ if cfg.get("orient") else 0)
+        if cfg.get("integrator") == "rk4":
+            bpc = 36 * esz_ + (4 * 2 * esz_ if cfg.get("orient") else 0)
         algo = bpc * cells
         achieved = algo / (ms_per_step / 1e3) / 1e9
         err = None
