@@ -29,8 +29,15 @@
 //   axpy(dt, k, x)          x + dt k
 //   noise(key)              N(key), the Gaussian of one cell
 //   add_noise(x, s, n)      x + s n
+//   oxface/oyface/ocell     the same in a cell's crystal frame (ORIENT)
 // The operand lists keep the reference's evaluation order available to an
 // exact policy.
+//
+// Template flags beside the arithmetic: ORIENT steps the multi-grain form
+// (every face's anisotropy in its cell's crystal frame, cos/sin theta0 from a
+// per-state table); MODE 0 is the Euler-Maruyama step, MODE 1 and 2 the
+// RungeKutta4 stages (see RkArgs); BATCH serves ensembles; TAIL blocks lower
+// than the row group.
 #pragma once
 
 #include <algorithm>
