@@ -210,6 +210,24 @@ class DeviceState:
         N.check(N.lib.lg_state_set_time(self.handle, float(t), int(step_index)))
 
 
+def observed_stretches(k: int, nsteps: int, everys) -> List[int]:
+    """Lengths of the runs between observations: starting after step k,
+    ``nsteps`` steps cut after every step that an observer with one of the
+    cadences ``everys`` fires on (step 1 and multiples of its cadence)."""
+    from .observe import fires
+
+    out, done = [], 0
+    while done < nsteps:
+        stop = nsteps - done
+        for s in range(1, stop + 1):
+            if any(fires(k + done + s, e) for e in everys):
+                stop = s
+                break
+        out.append(stop)
+        done += stop
+    return out
+
+
 class Simulation:
     """Sole owner of grid, discretization, model, integrator, scheduler and state.
 
@@ -259,19 +277,9 @@ class Simulation:
         if not self.observers:
             self.integrator.run(self, float(dt), nsteps, graph=graph, variant=variant)
             return
-        from .observe import fires
-
         # run in stretches that end on the steps some observer fires on
-        done = 0
-        while done < nsteps:
-            k = self.step_index()
-            stop = nsteps - done
-            for s in range(1, stop + 1):
-                if any(fires(k + s, getattr(o, "every", 1)) for o in self.observers):
-                    stop = s
-                    break
+        for stop in observed_stretches(self.step_index(), nsteps, [getattr(o, "every", 1) for o in self.observers]):
             self.integrator.run(self, float(dt), stop, graph=graph, variant=variant)
-            done += stop
             step = self.step_index()
             for o in self.observers:
                 o.observe(step, self.time(), 0, self.grid, self.state)

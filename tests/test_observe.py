@@ -116,3 +116,15 @@ def test_row_groups_hold_whole_blocks(tmp_path, monkeypatch):
     md = pq.ParquetFile(tmp_path / "snap_0000007.parquet").metadata
     assert [md.row_group(i).num_rows for i in range(md.num_row_groups)] == [12, 12, 12, 12]
     assert np.array_equal(pq.read_table(tmp_path / "snap_0000007.parquet")["phi"].to_numpy(), xy[0] * 3.0)
+
+
+def test_runs_are_cut_at_the_observed_steps():
+    from legendre_b200.core import observed_stretches
+
+    # from step 0: step 1 fires, then every 5
+    assert observed_stretches(0, 23, [5]) == [1, 4, 5, 5, 5, 3]
+    # two cadences: the union of their steps
+    assert observed_stretches(0, 12, [4, 6]) == [1, 3, 2, 2, 4]
+    # resuming mid-run: no step 1, the next multiple first
+    assert observed_stretches(7, 10, [5]) == [3, 5, 2]
+    assert sum(observed_stretches(3, 100, [7, 11])) == 100
