@@ -168,7 +168,8 @@ def max_over_ranks(pg, value: float) -> float:
         return value
     import torch
 
-    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    # NCCL reduces device tensors; gloo (the host-side tests) host ones
+    t = torch.tensor([value], dtype=torch.float64, device="cuda" if pg.get_backend() == "nccl" else "cpu")
     pg.all_reduce(t, op=pg.ReduceOp.MAX)
     return float(t.item())
 
