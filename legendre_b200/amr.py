@@ -105,6 +105,7 @@ class AmrSimulation:
         if base.dim != 2:
             raise ValueError("the AMR path is 2-D")
         self.grid = grid
+        self.observers = []
         self.model = model
         self.scheduler = scheduler
         if isinstance(model, ModelC):
@@ -212,13 +213,27 @@ class AmrSimulation:
     def step(self, dt: float) -> None:
         self.run(dt, 1)
 
+    def add_observer(self, observer) -> None:
+        """Observers are called after the coarse steps they fire on with
+        (step, t, epoch, grid, sim): the sim itself is the state they read, so
+        a grid-aware observer follows regrids through the epoch."""
+        self.observers.append(observer)
+
     def run(self, dt: float, nsteps: int, graph: bool = False, persistent: bool = False) -> None:
         """`nsteps` coarse steps.  `graph` replays pairs of coarse steps from a
         CUDA graph; `persistent` runs each pair as one cooperative launch
         (every level's fused fill + step and every restriction, separated by
         grid barriers) and takes precedence."""
         flags = (N.LG_RUN_GRAPH if graph else 0) | (N.LG_RUN_PERSISTENT if persistent else 0)
-        N.check(N.lib.lg_amr_sim_step(self.handle, float(dt), int(nsteps), flags), self.scheduler.handle)
+        if not self.observers:
+            N.check(N.lib.lg_amr_sim_step(self.handle, float(dt), int(nsteps), flags), self.scheduler.handle)
+            return
+        from .core import observed_stretches
+
+        for stop in observed_stretches(self.step_index(), int(nsteps), [getattr(o, "every", 1) for o in self.observers]):
+            N.check(N.lib.lg_amr_sim_step(self.handle, float(dt), stop, flags), self.scheduler.handle)
+            for o in self.observers:
+                o.observe(self.step_index(), self.time(), self.epoch, self.grid, self)
 
     # ------------------------------------------------------ transfers (c)
     def restrict(self, f) -> None:

@@ -22,6 +22,9 @@ writer (src/io/parquet.rs):
   interior cells dimension-0-fastest, SNAPPY, row groups of whole blocks
   flushed once 2^22 rows are gathered (``parquet.rs:150-215``).  It is an
   observer (synchronous) and a sink (behind an :class:`AsyncObserver`).
+  Observing an ``AmrSimulation`` it writes every level's blocks, with their
+  level and patch per cell, and a new static file at each regrid epoch
+  (the reference's grid-aware path).
 """
 from __future__ import annotations
 
@@ -71,6 +74,34 @@ def cell_centers(grid) -> np.ndarray:
     return out
 
 
+def is_amr(sim) -> bool:
+    """True for an AmrSimulation (blocks of several levels, regrid epochs)."""
+    return hasattr(sim, "patches") and hasattr(sim, "centers")
+
+
+def amr_columns(sim, names: Sequence[Tuple[str, object]]) -> Dict[str, np.ndarray]:
+    """Columns of an AMR hierarchy in the writer's row order: blocks in
+    order (level 0's, then each finer level's patches), each block's interior
+    cells dimension-0-fastest."""
+    out = {}
+    for name, f in names:
+        out[name] = np.concatenate([slab[1:-1, 1:-1].reshape(-1) for slab in sim.get(f)])
+    return out
+
+
+def amr_statics(sim):
+    """x, y, level and patch of every cell of an AMR hierarchy, row order as
+    amr_columns; x, y are the reference's cell centres (amr/grid.rs:389-395)."""
+    xs, ys, lv, pt = [], [], [], []
+    for b, (level, lo, hi) in enumerate(sim.patches()):
+        x, y = sim.centers(b)
+        xs.append(x.reshape(-1))
+        ys.append(y.reshape(-1))
+        lv.append(np.full(x.size, float(level)))
+        pt.append(np.full(x.size, float(b)))
+    return np.concatenate(xs), np.concatenate(ys), np.concatenate(lv), np.concatenate(pt)
+
+
 def state_columns(state, names: Sequence[Tuple[str, object]]) -> Dict[str, np.ndarray]:
     """Columns of a device state read synchronously (download, then the
     interior of each block in row order)."""
@@ -82,8 +113,9 @@ class ParquetObserver:
     field) -- every ``every`` steps plus step 1, into ``directory``."""
 
     def __init__(self, grid, fields: Sequence[Tuple[str, object]], every: int, directory):
-        if not 1 <= len(grid.cells) <= 3:
-            raise ValueError("the Parquet observer covers 1-, 2- and 3-D Cartesian grids")
+        cells = grid.cells if hasattr(grid, "cells") else grid.base.cells
+        if not 1 <= len(cells) <= 3:
+            raise ValueError("the Parquet observer covers 1-, 2- and 3-D grids")
         if not fields:
             raise ValueError("no fields to observe")
         self.grid = grid
@@ -105,50 +137,66 @@ class ParquetObserver:
         return self.dynamic + self.statics
 
     # ------------------------------------------------------------- writing
-    def _group_rows(self) -> int:
-        # whole blocks per row group, flushed once ROWS_PER_GROUP rows are in
-        bcells = int(np.prod(self.grid.block_cells))
-        return -(-ROWS_PER_GROUP // bcells) * bcells
+    @staticmethod
+    def _groups(block_rows: Sequence[int]) -> List[Tuple[int, int]]:
+        """Row groups as (start, rows): whole blocks, a group flushed once it
+        holds ROWS_PER_GROUP rows or more (parquet.rs:150-215)."""
+        out, start, n = [], 0, 0
+        for r in block_rows:
+            n += int(r)
+            if n >= ROWS_PER_GROUP:
+                out.append((start, n))
+                start, n = start + n, 0
+        if n:
+            out.append((start, n))
+        return out
 
-    def _write(self, path: str, cols: List[Tuple[str, object, np.ndarray]]):
+    def _block_rows(self, amr=None) -> List[int]:
+        if amr is not None:
+            return [(hi[0] - lo[0]) * (hi[1] - lo[1]) for _, lo, hi in amr.patches()]
+        bcells = int(np.prod(self.grid.block_cells))
+        return [bcells] * (int(np.prod(self.grid.cells)) // bcells)
+
+    def _write(self, path: str, cols: List[Tuple[str, object, np.ndarray]], block_rows: Sequence[int]):
         import pyarrow as pa
         import pyarrow.parquet as pq
 
         pa_type = {np.dtype(np.float64): pa.float64(), np.dtype(np.int64): pa.int64()}
         schema = pa.schema([pa.field(n, pa_type[np.dtype(dt)], nullable=False) for n, dt, _ in cols])
-        rows = max(len(v) for _, _, v in cols if not np.isscalar(v))
-        group = self._group_rows()
         with pq.ParquetWriter(path, schema, compression="snappy") as w:
-            for lo in range(0, rows, group):
-                n = min(group, rows - lo)
+            for lo, n in self._groups(block_rows):
                 arrays = []
                 for _, dt, v in cols:
                     a = np.full(n, v, dtype=dt) if np.isscalar(v) else v[lo:lo + n]
                     arrays.append(pa.array(a, type=pa_type[np.dtype(dt)]))
                 w.write_table(pa.Table.from_arrays(arrays, schema=schema), row_group_size=n)
 
-    def _write_static(self, columns: Dict[str, np.ndarray]):
-        D = len(self.grid.cells)
-        xyz = cell_centers(self.grid)
-        bcells = int(np.prod(self.grid.block_cells))
-        nb = int(np.prod(self.grid.cells)) // bcells
-        cols = [(("x", "y", "z")[d], np.float64, xyz[d]) for d in range(D)]
-        cols.append(("level", np.float64, np.zeros(nb * bcells)))
-        cols.append(("patch", np.float64, np.repeat(np.arange(nb, dtype=np.float64), bcells)))
+    def _write_static(self, columns: Dict[str, np.ndarray], amr=None):
+        if amr is not None:  # the hierarchy's blocks: per-cell level and patch (parquet.rs:186-196)
+            x, y, lv, pt = amr_statics(amr)
+            cols = [("x", np.float64, x), ("y", np.float64, y), ("level", np.float64, lv), ("patch", np.float64, pt)]
+        else:
+            D = len(self.grid.cells)
+            xyz = cell_centers(self.grid)
+            bcells = int(np.prod(self.grid.block_cells))
+            nb = int(np.prod(self.grid.cells)) // bcells
+            cols = [(("x", "y", "z")[d], np.float64, xyz[d]) for d in range(D)]
+            cols.append(("level", np.float64, np.zeros(nb * bcells)))
+            cols.append(("patch", np.float64, np.repeat(np.arange(nb, dtype=np.float64), bcells)))
         cols += [(name, np.float64, columns[name]) for name, _ in self.statics]
-        self._write(os.path.join(self.dir, f"static_{self.epoch:07d}.parquet"), cols)
+        self._write(os.path.join(self.dir, f"static_{self.epoch:07d}.parquet"), cols, self._block_rows(amr))
 
-    def write_snapshot(self, snap: Snapshot) -> None:
+    def write_snapshot(self, snap: Snapshot, amr=None) -> None:
         if snap.epoch != self.epoch:
             self.epoch = snap.epoch
             self.static_written = False
         if not self.static_written:
-            self._write_static(snap.columns)
+            self._write_static(snap.columns, amr)
             self.static_written = True
         cols = [("step", np.int64, np.int64(snap.step)), ("t", np.float64, np.float64(snap.t)),
                 ("epoch", np.int64, np.int64(snap.epoch))]
         cols += [(name, np.float64, snap.columns[name]) for name, _ in self.dynamic]
-        self._write(os.path.join(self.dir, f"snap_{snap.step:07d}.parquet"), cols)
+        self._write(os.path.join(self.dir, f"snap_{snap.step:07d}.parquet"), cols, self._block_rows(amr))
 
     # ------------------------------------------------------ as an observer
     def observe(self, step: int, t: float, epoch: int, grid, state) -> None:
@@ -159,6 +207,10 @@ class ParquetObserver:
             return
         if epoch != self.epoch:
             self.grid = grid
+        if is_amr(state):  # an AmrSimulation observes itself: blocks of every level
+            cols = amr_columns(state, self.field_names())
+            self.write_snapshot(Snapshot(step, t, epoch, grid, cols), amr=state)
+            return
         cols = state_columns(state, self.field_names())
         self.write_snapshot(Snapshot(step, t, epoch, grid, cols))
 

@@ -149,3 +149,50 @@ def test_parquet_behind_the_ring_equals_the_synchronous_writer(sched, tmp_path):
     assert sorted(p.name for p in (tmp_path / "async").iterdir()) == files
     for name in files:
         assert pq.read_table(tmp_path / "async" / name).equals(pq.read_table(tmp_path / "sync" / name)), name
+
+
+def test_parquet_follows_an_amr_run_through_its_regrids(sched, tmp_path):
+    # the reference's grid-aware path: every level's blocks with their level
+    # and patch per cell, the static file of the snapshot's epoch, snapshot
+    # rows equal to the hierarchy's interiors at their step
+    def make():
+        base = L.CartesianGrid([32, 32], [8, 8], [0.0, 0.0], [H, H])
+        grid = L.AmrGrid.from_patches(base, [2], [])
+        model = L.ModelC(0.06, 3.19, 0.0)
+        adapt = L.BergerOliger(L.GradientTagger("phi", 0.05), L.RegridPolicy(4, 1, L.ClusterParams(0.7, 4)))
+        sim = L.AmrSimulation(grid, L.FiniteVolume(), model, L.Subcycling(0), sched, L.CudaAllocator("f64"), adapt)
+        c = 16 * H
+        phi, u = sim.get("phi"), sim.get("u")
+        for b in range(sim.num_blocks):
+            x, y = sim.centers(b)
+            phi[b][1:-1, 1:-1] = -np.tanh((np.hypot(x - c, y - c) - 2.5) / np.sqrt(2.0))
+            u[b][1:-1, 1:-1] = -0.7
+        sim.set("phi", phi)
+        sim.set("u", u)
+        return sim
+
+    names = [("phi", "phi"), ("u", "u")]
+    twin = make()
+    dt = twin.stable_dt()
+    want = {}
+    for k in range(1, 11):
+        twin.run(dt, 1)
+        if k == 1 or k % 3 == 0:
+            x = np.concatenate([twin.centers(b)[0].reshape(-1) for b in range(twin.num_blocks)])
+            want[k] = (twin.epoch, {n: np.concatenate([s[1:-1, 1:-1].reshape(-1) for s in twin.get(f)])
+                                    for n, f in names}, x, twin.patches())
+    sim = make()
+    sim.add_observer(L.ParquetObserver(sim.grid, names, 3, tmp_path))
+    sim.run(dt, 10)
+    # the hierarchy was refined before the first snapshot (the writer's
+    # epoch changes are covered on the host, test_observe.py)
+    assert any(l > 0 for l, _, _ in want[1][3])
+    for k, (epoch, cols, x, patches) in want.items():
+        snap = pq.read_table(tmp_path / f"snap_{k:07d}.parquet")
+        assert np.array_equal(snap["epoch"].to_numpy(), np.full(len(x), epoch, dtype=np.int64))
+        for n, _ in names:
+            assert np.array_equal(snap[n].to_numpy(), cols[n]), (k, n)
+        st = pq.read_table(tmp_path / f"static_{epoch:07d}.parquet")
+        assert np.array_equal(st["x"].to_numpy(), x)
+        lv = np.concatenate([np.full((hi[0] - lo[0]) * (hi[1] - lo[1]), float(l)) for l, lo, hi in patches])
+        assert np.array_equal(st["level"].to_numpy(), lv)
