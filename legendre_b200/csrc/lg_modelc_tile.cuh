@@ -85,6 +85,64 @@ struct RkArgs {
     T c, s6, s3;
 };
 
+// Ghost images of a strip's x-edge cells (the block's columns 0 and n0 - 1)
+// for the rows of one unit: lane k holds row r0 + k's phi and u of the left
+// (l0, l1) and right (r0, r1) edge cells, gathered by shuffles as the rows
+// are stepped and written once at the unit's end (rows 0 and n1 - 1, whose
+// images include y ghosts and corners, are pushed in full as they go).
+template <class T>
+struct EdgeHold {
+    T l0, l1, r0, r1;
+};
+
+// store the cell, and take care of its ghost images (see EdgeHold)
+template <class T>
+__device__ __forceinline__ void store_cell(T* __restrict__ out, T* __restrict__ po, T* __restrict__ uo, int off,
+                                           T phin, T un, bool ok, bool live, bool edge_x, int j, int r0, int n0,
+                                           int n1, int col, int lane, int last_lane, const SlabLayout& L,
+                                           const Nbr2& nb, EdgeHold<T>& eh) {
+    if (ok) {
+        po[off] = phin;
+        uo[off] = un;
+    }
+    if (j == 0 || j == n1 - 1) {  // warp-uniform
+        if (ok) {
+            push_ghosts_2d_g1(out, L, 0, nb, n0, n1, col, j, phin);
+            push_ghosts_2d_g1(out, L, 1, nb, n0, n1, col, j, un);
+        }
+    } else if (edge_x) {  // warp-uniform: warps on a block's x edge collect their edge cells
+        const T l0 = __shfl_sync(0xffffffffu, phin, 0), l1 = __shfl_sync(0xffffffffu, un, 0);
+        const T rr0 = __shfl_sync(0xffffffffu, phin, last_lane), rr1 = __shfl_sync(0xffffffffu, un, last_lane);
+        if (live && lane == ((j - r0) & 31)) {
+            eh.l0 = l0;
+            eh.l1 = l1;
+            eh.r0 = rr0;
+            eh.r1 = rr1;
+        }
+    }
+}
+
+// the collected x-edge images of a unit's rows (r0 .. r1-1, not 0 or n1-1):
+// the left edge's into the left neighbour's ghost column n0 (or this block's
+// mirror ghost column -1), the right edge's likewise (push_ghosts_2d_g1)
+template <class T>
+__device__ __forceinline__ void flush_edges(T* __restrict__ out, const SlabLayout& L, const Nbr2& nb, int n0, int n1,
+                                            int r0, int r1, int lane, bool left, bool right, const EdgeHold<T>& eh) {
+    const int r = r0 + lane;
+    if (r >= r1 || r == 0 || r == n1 - 1) return;
+    const int64_t row = (int64_t)(r + 1) * L.gdim[0];
+    if (left) {
+        const int tb = nb.l >= 0 ? nb.l : nb.b, ci = nb.l >= 0 ? n0 : -1;
+        out[slab_base(L, tb, 0) + (ci + 1) + row] = eh.l0;
+        out[slab_base(L, tb, 1) + (ci + 1) + row] = eh.l1;
+    }
+    if (right) {
+        const int tb = nb.r >= 0 ? nb.r : nb.b, ci = nb.r >= 0 ? -1 : n0;
+        out[slab_base(L, tb, 0) + (ci + 1) + row] = eh.r0;
+        out[slab_base(L, tb, 1) + (ci + 1) + row] = eh.r1;
+    }
+}
+
 // The new phi and u of a cell from its drift (kphi, ku): the Euler-Maruyama
 // update (MODE 0) or a RungeKutta4 stage (MODE 1, 2); e0/e1 index the cell's
 // phi/u entries in any arena of the state's layout.
@@ -152,7 +210,7 @@ __device__ __forceinline__ void strip_row(const typename Ops::Params& m, const T
                                           uint64_t block_key, T bnd, const Row3<T>& A, const Row3<T>& B,
                                           const Row3<T>& C, Row3<T>& P, T UA, T UB, T UC, T& UP, T& jb, T dt,
                                           T scale_amp, const T* __restrict__ trig_b, int64_t ncells, T& cprev,
-                                          T& sprev, T& cnext, T& snext, const RkArgs<T>& rk) {
+                                          T& sprev, T& cnext, T& snext, const RkArgs<T>& rk, EdgeHold<T>& eh) {
     const int sy = NX > 0 ? NX + 2 : g.L.gdim[0];
     // lanes past the block's last column (valid false) run the same code on
     // a clamped column and only skip the stores: no branch splits the face,
@@ -209,14 +267,7 @@ __device__ __forceinline__ void strip_row(const typename Ops::Params& m, const T
         T phin, un;
         cell_update<T, Ops, NOISE, MODE>(rk, dt, scale_amp, nval, kphi, ku, B.b, UB, (po - out) + off,
                                          (uo - out) + off, ok, phin, un);
-        if (ok) {
-            po[off] = phin;
-            uo[off] = un;
-            if (edge_x || j == 0 || j == n1 - 1) {
-                push_ghosts_2d_g1(out, g.L, 0, nb, n0, n1, col, j, phin);
-                push_ghosts_2d_g1(out, g.L, 1, nb, n0, n1, col, j, un);
-            }
-        }
+        store_cell(out, po, uo, off, phin, un, ok, live, edge_x, j, r0, n0, n1, col, lane, last_lane, g.L, nb, eh);
         jb = jt;
         cprev = c0;
         sprev = s0;
@@ -233,14 +284,7 @@ __device__ __forceinline__ void strip_row(const typename Ops::Params& m, const T
     T phin, un;
     cell_update<T, Ops, NOISE, MODE>(rk, dt, scale_amp, nval, kphi, ku, B.b, UB, (po - out) + off, (uo - out) + off,
                                      ok, phin, un);
-    if (ok) {
-        po[off] = phin;
-        uo[off] = un;
-        if (edge_x || j == 0 || j == n1 - 1) {  // warp-uniform: only warps on a block edge push ghosts
-            push_ghosts_2d_g1(out, g.L, 0, nb, n0, n1, col, j, phin);
-            push_ghosts_2d_g1(out, g.L, 1, nb, n0, n1, col, j, un);
-        }
-    }
+    store_cell(out, po, uo, off, phin, un, ok, live, edge_x, j, r0, n0, n1, col, lane, last_lane, g.L, nb, eh);
     jb = jt;
 }
 
@@ -314,18 +358,20 @@ __device__ __forceinline__ void strip_unit(const typename Ops::Params& m, uint64
         jb = Ops::oyface(m, cpv, spv, T(0.25) * (w[1].c - w[1].a + w[0].c - w[0].a), w[1].b - w[0].b);
     }
 
+    EdgeHold<T> eh{T(0), T(0), T(0), T(0)};
 #define LG_ROW(J, Q)                                                                                            \
     strip_row<T, Ops, NOISE, NX, FULL, PF, TAIL, ORIENT, MODE>(m, g, J, r0, r1, lane, col, valid, last_lane, n0, n1, off, ph, uu, out, po,  \
                                        uo, nb, edge_x, block_key, bnd, w[(Q) % NB], w[((Q) + 1) % NB],          \
                                        w[((Q) + 2) % NB], w[((Q) + 2 + PF) % NB], uw[(Q) % NB],                \
                                        uw[((Q) + 1) % NB], uw[((Q) + 2) % NB], uw[((Q) + 2 + PF) % NB], jb, dt, \
-                                       scale_amp, trig_b, ncells, cpv, spv, cnx, snx, rk);                                                              \
+                                       scale_amp, trig_b, ncells, cpv, spv, cnx, snx, rk, eh);                                                              \
     off += sy
     for (int j = r0; j < r1; j += NB) {
 #pragma unroll
         for (int q = 0; q < NB; ++q) { LG_ROW(j + q, q); }
     }
 #undef LG_ROW
+    if (edge_x) flush_edges(out, g.L, nb, n0, n1, r0, r1, lane, col - lane == 0, cr == n0 - 1, eh);
 }
 
 // Rows per work unit are at most 32, so one batch of boundary faces (lanes
