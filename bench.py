@@ -70,11 +70,11 @@ CONFIGS = {
 BYTES_PER_CELL = {"f64": 32, "f32": 16}  # read phi, u; write phi, u
 
 # DRAM bytes (read + write) per cell-update of the dominant kernel, from one
-# ncu capture each (profiles/): the strip kernel on 4096^2 (FP64 513 MB and
+# ncu capture each (profiles/): the strip kernel on 4096^2 (FP64 502 MB and
 # FP32 226 MB per 16.8M-cell launch) and the 3-D heat kernel on 256^3 (319 MB
 # per 16.8M cells; the 512^3 run has the same per-block work, so its traffic
 # scales with the cell count).  Other workloads report null.
-TRAFFIC_PER_CELL = {("c2", "f64"): 513.4e6 / 4096 ** 2, ("c2", "f32"): 226.3e6 / 4096 ** 2,
+TRAFFIC_PER_CELL = {("c2", "f64"): 502.4e6 / 4096 ** 2, ("c2", "f32"): 226.3e6 / 4096 ** 2,
                     ("c1big", "f64"): 318.7e6 / 256 ** 3}
 
 
