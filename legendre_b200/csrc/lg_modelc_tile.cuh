@@ -16,9 +16,9 @@
 // is the y face above it in the previous row, carried in a register.
 //
 // The row loop keeps a window of four phi rows (j-1, j, j+1 and the
-// prefetch of j+2).  FP32 unrolls it four times so the window rotates with
-// no register moves; FP64, whose row code is twice as large, keeps one copy
-// of the row and shifts the window by moves.
+// prefetch of j+2).  It keeps one copy of the row code and shifts the window
+// by register moves; only the FP32 oriented form unrolls it four times, so
+// that the window rotates with no moves.
 //
 // Ops (the arithmetic policy) provides, for element type T:
 //   xface(m, dn, d1, c, e)  flux A (A dn - A' dt) through an x face, with the
@@ -368,13 +368,14 @@ __device__ __forceinline__ void strip_unit(const typename Ops::Params& m, uint64
                                        uw[((Q) + 1) % NB], uw[((Q) + 2) % NB], uw[((Q) + 2 + PF) % NB], jb, dt, \
                                        scale_amp, trig_b, ncells, cpv, spv, cnx, snx, rk, eh);                                                              \
     off += sy
-    if constexpr (sizeof(T) == 8) {
-        // one copy of the (large) FP64 row code: the window shifts down by
-        // one row through registers instead of rotating through NB unrolled
-        // copies, which overflowed the instruction cache and spilled (FP64
-        // 4096^2: 51.8 against 45.1 Gcell/s; 10080^2 with 1000 oriented
-        // grains: 33.7 against 25.3).  The smaller FP32 row code is faster
-        // unrolled (oriented 10080^2: 74.7 against 71.8).
+    if constexpr (sizeof(T) == 8 || !ORIENT) {
+        // one copy of the row code: the window shifts down by one row
+        // through registers instead of rotating through NB unrolled copies,
+        // which overflowed the instruction cache and spilled (FP64 4096^2:
+        // 51.8 against 45.1 Gcell/s; 10080^2 with 1000 oriented grains: 33.7
+        // against 25.3; FP32 4096^2: 100.1 against 94.2, and 3 CTAs per SM
+        // without spills).  The FP32 oriented form is faster unrolled
+        // (10080^2: 74.7 against 71.8).
 #pragma unroll 1
         for (int j = r0; j < r1; ++j) {
             LG_ROW(j, 0);
