@@ -1,0 +1,48 @@
+"""bench.py's reference arm on the host: rank 0 times the oracle (the C++
+restatement of the reference's CPU path) and prints one JSON line with the
+GPU arm's metric, unit and direction, the CPU sample it timed and a zero-copy
+e2e block.  Small grids stand in for the configurations' full sizes."""
+import json
+import sys
+from pathlib import Path
+
+import pytest
+
+ROOT = Path(__file__).resolve().parent.parent
+
+
+class _Args:
+    steps, warmup, gpus = 2, 3, 1
+
+
+def _line(capsys, cfg):
+    sys.path.insert(0, str(ROOT))
+    import bench
+
+    bench.run_reference(_Args(), cfg)
+    out = capsys.readouterr().out.strip().splitlines()
+    assert len(out) == 1
+    return json.loads(out[0])
+
+
+@pytest.mark.parametrize("name, over", [
+    ("c2", dict(cells=128, block=32)),
+    ("c3o", dict(cells=126, block=63, grains=6)),
+])
+def test_reference_arm_line(capsys, monkeypatch, name, over):
+    sys.path.insert(0, str(ROOT))
+    import bench
+
+    monkeypatch.setenv("RANK", "0")
+    cfg = dict(bench.CONFIGS[name], **over)
+    d = _line(capsys, cfg)
+    assert d["impl"] == "reference"
+    assert (d["metric"], d["unit"], d["higher_is_better"]) == ("Gcell-updates/s", "Gcell-updates/s", True)
+    assert d["value"] > 0 and d["steps"] == 2 and d["warmup"] == 3 and d["n_gpus"] == 1
+    assert d["config"]["workload"] == cfg["workload"] and d["config"]["cells"] == cfg["cells"]
+    cb = d["cpu_baseline"]
+    assert cb["kind"] == "port" and cb["cores"] >= 1 and cb["value"] == d["value"]
+    assert cb["sample"].startswith("2 of 2 steps")
+    e2e = d["e2e"]
+    assert e2e["value"] == d["value"] and e2e["unit"] == d["unit"]
+    assert e2e["h2d_bytes_per_step"] == 0 and e2e["d2h_bytes_per_step"] == 0
