@@ -304,7 +304,10 @@ int lg_ensemble_set_adjoint_kernel(lg_ensemble* e, int kernel);
 /* Device bytes value_and_grad may spend on a resident tail: the last
  * segments whose every state fits are kept from the forward pass instead of
  * being recomputed from their checkpoints (the gradients are the same bits).
- * 0, the default, is pure checkpointing; 0 also frees the kept states. */
+ * 0, the default, is pure checkpointing; 0 also frees the kept states.  The
+ * budget is taken as given: it must fit in the free device memory beside the
+ * checkpoints and recomputed states, or value_and_grad returns LG_ERR_NOMEM
+ * (a caller sizes it from cudaMemGetInfo less a margin). */
 int lg_ensemble_set_resident_budget(lg_ensemble* e, uint64_t bytes);
 
 /* ---- Observation: snapshots off the stepping stream --------------------
