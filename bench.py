@@ -227,8 +227,11 @@ def tip_position(phi, row, x0, h):
 def fp32_error(cfg, sched, steps):
     """The FP32 path against the FP64 path (bit-identical to the CPU
     oracle) from the same initial state and noise keys: phi L2 (RMS) and
-    L-inf after `steps` steps, solid fractions (phi > 0), and the +x tip
-    velocity of the grain nearest the domain centre over the second half."""
+    L-inf after `steps` steps, solid fractions (phi > 0), the +x tip
+    velocity of the grain nearest the domain centre over the second half,
+    and the total enthalpy h^2 sum(u - phi/2) at the start and the end (FP64
+    device sums; the noise moves it, the deterministic step only by
+    rounding)."""
     import numpy as np
 
     n, b, h = cfg["cells"], cfg["block"], cfg["h"]
@@ -236,6 +239,7 @@ def fp32_error(cfg, sched, steps):
     for dtype in ("f64", "f32"):
         sim, grid, model, grains = make_sim(cfg, dtype, sched)
         initialize(sim, grid, model, grains, cfg, dtype, sched)
+        h0 = model.enthalpy(grid, sim.state)
         c = min(grains, key=lambda g: (g.center[0] - n * h / 2) ** 2 + (g.center[1] - n * h / 2) ** 2)
         row = int(c.center[1] / h)
         sim.run(cfg["dt"], steps // 2, graph=True)
@@ -244,13 +248,15 @@ def fp32_error(cfg, sched, steps):
         p2 = to_global(sim.state.interior("phi").astype(np.float64), n, b)
         v = (tip_position(p2, row, c.center[0], h) - tip_position(p1, row, c.center[0], h)) / (
             (steps - steps // 2) * cfg["dt"])
-        out[dtype] = (p2, v, float(np.mean(p2 > 0.0)))
+        out[dtype] = (p2, v, float(np.mean(p2 > 0.0)), (h0, model.enthalpy(grid, sim.state)))
         del sim
     d = out["f32"][0] - out["f64"][0]
     return {"steps": steps, "phi_l2": float(np.sqrt(np.mean(d * d))), "phi_linf": float(np.max(np.abs(d))),
             "solid_fraction_f64": out["f64"][2], "solid_fraction_f32": out["f32"][2],
             "tip_velocity_f64": out["f64"][1], "tip_velocity_f32": out["f32"][1],
             "tip_velocity_rel_err": abs(out["f32"][1] - out["f64"][1]) / abs(out["f64"][1]),
+            "enthalpy_f64": list(out["f64"][3]), "enthalpy_f32": list(out["f32"][3]),
+            "enthalpy_rel_diff": abs(out["f32"][3][1] - out["f64"][3][1]) / abs(out["f64"][3][1]),
             "reference": "the FP64 path, bit-identical to the CPU oracle, from the same state and noise keys"}
 
 

@@ -349,6 +349,15 @@ int lg_snapshot_ring_stats(lg_snapshot_ring* r, int64_t* captured, int64_t* drop
  * device and no context. */
 int lg_cell_centers(int D, const int64_t* cells, const int64_t* block_cells, const double* origin,
                     const double* spacing, double* out);
+/* FP64 sum of one field over every block's interior cells of the current
+ * state (values widened from the state's precision), in a fixed order: per
+ * block, 256 strided partial sums joined by a fixed shuffle tree and the
+ * warps in order; then the blocks in index order.  The same state gives the
+ * same bits.  Model C's enthalpy is h^D (sum u - sum phi / 2); with no noise
+ * and periodic or zero-flux boundaries a step changes it only by rounding
+ * (du/dt = D lap u + dphi/dt / 2, phasefield.rs:353-422).  The reference has
+ * no such reduction.  Waits for the context's stream. */
+int lg_state_field_sum(lg_state* st, int field, double* sum);
 
 /* Standard normals of n keys on the device (`rng::standard_normal`,
  * src/util/rng.rs:43-49); host arrays in and out. */

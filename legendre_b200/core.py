@@ -189,6 +189,13 @@ class DeviceState:
         sl = (slice(None),) + tuple(slice(g, g + n) for n in reversed(self.grid.block_cells))
         return np.ascontiguousarray(a[sl])
 
+    def field_sum(self, f) -> float:
+        """FP64 sum of field ``f`` over every block's interior cells, on the
+        device in a fixed order (the same state gives the same bits)."""
+        out = C.c_double()
+        N.check(N.lib.lg_state_field_sum(self.handle, self._index(f), C.byref(out)), self.scheduler.handle)
+        return out.value
+
     def fill_ghosts(self, f) -> None:
         """``fill_ghosts_mirror`` for one field (cartesian.rs:392-401)."""
         N.check(N.lib.lg_fill_ghosts(self.handle, self._index(f)), self.scheduler.handle)

@@ -1,6 +1,7 @@
 // Observation: the device side of the reference's AsyncObserver
-// (src/core/observer.rs:65-165) and the coordinate columns of its Parquet
-// snapshots (src/io/parquet.rs:150-215).
+// (src/core/observer.rs:65-165), the coordinate columns of its Parquet
+// snapshots (src/io/parquet.rs:150-215), and an FP64 sum of a field over the
+// interior cells (the conserved totals of a run: Model C's enthalpy).
 //
 // A snapshot ring holds `nslots` slots, each a device buffer and a pinned
 // host buffer of the chosen fields' interior cells in the Parquet row order
@@ -55,6 +56,45 @@ __global__ void __launch_bounds__(256) snapshot_pack_kernel(const T* __restrict_
             const int64_t y = r % a.n1, z = r / a.n1;
             dst[i] = (double)slab[(x + g) + (y + g1) * gx + (z + g2) * gx * gy];
         }
+    }
+}
+
+struct SumArgs {
+    int field, ghost, D, n0, n1;
+    int64_t nfields, slab_stride, nblocks, bcells;
+};
+
+// partial[b] = the FP64 sum of field `field`'s interior cells of block b.
+// The order is fixed: thread t adds cells t, t + 256, ... in turn, the
+// warps' sums meet by a fixed shuffle tree and the eight warp sums in warp
+// order, so a state gives the same bits on every call.
+constexpr int kSumThreads = 256;
+
+template <class T>
+__global__ void __launch_bounds__(kSumThreads) field_sum_kernel(const T* __restrict__ arena,
+                                                                double* __restrict__ partial, SumArgs a) {
+    __shared__ double warp_sum[kSumThreads / 32];
+    const int g = a.ghost;
+    const int64_t gx = a.n0 + 2 * g;
+    const int64_t gy = a.D > 1 ? a.n1 + 2 * g : 1;
+    const int g1 = a.D > 1 ? g : 0, g2 = a.D > 2 ? g : 0;
+    for (int64_t b = blockIdx.x; b < a.nblocks; b += gridDim.x) {
+        const T* slab = arena + (b * a.nfields + a.field) * a.slab_stride;
+        double s = 0.0;
+        for (int64_t i = threadIdx.x; i < a.bcells; i += kSumThreads) {
+            const int64_t x = i % a.n0, r = i / a.n0;
+            const int64_t y = r % a.n1, z = r / a.n1;
+            s += (double)slab[(x + g) + (y + g1) * gx + (z + g2) * gx * gy];
+        }
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+        if ((threadIdx.x & 31) == 0) warp_sum[threadIdx.x >> 5] = s;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double t = 0.0;
+            for (int w = 0; w < kSumThreads / 32; ++w) t += warp_sum[w];
+            partial[b] = t;
+        }
+        __syncthreads();  // warp_sum is rewritten for the next block
     }
 }
 
@@ -302,6 +342,51 @@ int lg_cell_centers(int D, const int64_t* cells, const int64_t* block_cells, con
                     }
                 }
     }
+    return LG_OK;
+}
+
+int lg_state_field_sum(lg_state* st, int field, double* sum) {
+    if (!st || !sum) return LG_ERR_INVALID;
+    lg::StateView v;
+    int rc = lg::abi_state_view(st, &v);
+    if (rc != LG_OK) return rc;
+    if (field < 0 || field >= v.nfields) return lg::abi_fail(v.ctx, LG_ERR_INVALID, "field index out of range");
+    cudaSetDevice(lg::abi_device(v.ctx));
+    cudaStream_t s = lg::abi_stream(v.ctx);
+    SumArgs a{};
+    a.field = field;
+    a.ghost = v.ghosts[field];
+    a.D = v.D;
+    a.n0 = (int)v.block[0];
+    a.n1 = (int)v.block[1];
+    a.nfields = v.nfields;
+    a.slab_stride = v.slab_stride;
+    a.nblocks = v.nblocks;
+    a.bcells = v.block[0] * v.block[1] * v.block[2];
+    double* d = nullptr;
+    cudaError_t e = cudaMallocAsync(&d, (size_t)v.nblocks * sizeof(double), s);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return lg::abi_fail(v.ctx, e == cudaErrorMemoryAllocation ? LG_ERR_NOMEM : LG_ERR_CUDA,
+                            std::string("field sum: ") + cudaGetErrorString(e));
+    }
+    const unsigned grid = (unsigned)std::min<int64_t>(v.nblocks, 148 * 8);
+    if (v.dtype == LG_F64)
+        field_sum_kernel<double><<<grid, kSumThreads, 0, s>>>(static_cast<const double*>(v.arena), d, a);
+    else
+        field_sum_kernel<float><<<grid, kSumThreads, 0, s>>>(static_cast<const float*>(v.arena), d, a);
+    e = cudaGetLastError();
+    lg::abi_count_launch(v.ctx, 1);
+    std::vector<double> part((size_t)v.nblocks);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(part.data(), d, part.size() * sizeof(double), cudaMemcpyDeviceToHost, s);
+    const cudaError_t f = cudaFreeAsync(d, s);
+    if (e == cudaSuccess) e = f;
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return lg::abi_fail(v.ctx, LG_ERR_CUDA, std::string("field sum: ") + cudaGetErrorString(e));
+    double total = 0.0;
+    for (double p : part) total += p;  // blocks in index order
+    *sum = total;
     return LG_OK;
 }
 

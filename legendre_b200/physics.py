@@ -76,6 +76,17 @@ class ModelC:
         return N.ModelCParams(self.eps4, self.lambda_, self.d_thermal, self.noise_amplitude, self.anisotropy_tol,
                               flux_tol)
 
+    def enthalpy(self, grid, state) -> float:
+        """Total enthalpy h^D * sum(u - phi / 2) over the interior cells, from
+        FP64 device sums.  du/dt = D lap u + (dphi/dt) / 2 (phasefield.rs:
+        353-422), so without noise and with periodic or zero-flux boundaries a
+        step changes it only by rounding: the conservation check of a run in
+        either precision.  (The reference has no such diagnostic.)"""
+        vol = 1.0
+        for h in grid.spacing:
+            vol *= h
+        return vol * (state.field_sum("u") - 0.5 * state.field_sum("phi"))
+
     # ------------------------------------------------------ initial state
     def with_orientations(self) -> "ModelC":
         """Per-grain crystal orientations (phasefield.rs:118-125): a static
