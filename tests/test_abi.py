@@ -80,3 +80,24 @@ def test_seed_positions_follow_the_example():
     assert g[3].center[0] == margin + unit_open(mix_key(42, [3, 0])) * span
     one = seed_positions(630, 0.4, 1, 42)
     assert one[0].center == (0.4, 0.4) and one[0].radius == 4.0
+
+
+def test_every_entry_point_rejects_null_handles_without_a_device():
+    # each entry point checks its handle and output pointers before any CUDA
+    # call: with null pointers and zero counts it returns LG_ERR_INVALID (the
+    # two counters -1, lg_last_error its fixed text)
+    import ctypes as C
+    import legendre_b200._native as N
+    special = {"lg_abi_version": 1, "lg_ctx_kernel_launches": -1, "lg_grid_num_blocks": -1,
+               "lg_last_error": b"null context"}
+    for name, (_res, args) in N._SIGS.items():
+        vals = []
+        for a in args:
+            if a in (C.c_int, C.c_int64, C.c_uint64, C.c_uint32):
+                vals.append(0)
+            elif a is C.c_double:
+                vals.append(0.0)
+            else:  # a pointer or handle
+                vals.append(None)
+        got = getattr(N.lib, name)(*vals)
+        assert got == special.get(name, N.LG_ERR_INVALID), name
