@@ -78,10 +78,12 @@ class CudaAllocator:
 
     dtype: str = "f64"
 
-    @property
-    def code(self) -> int:
+    def __post_init__(self):
         if self.dtype not in ("f64", "f32"):
             raise ValueError("dtype must be 'f64' or 'f32'")
+
+    @property
+    def code(self) -> int:
         return N.LG_F64 if self.dtype == "f64" else N.LG_F32
 
     @property
