@@ -25,6 +25,9 @@ def test_oracle_reproduces_frozen_states():
     assert mg.heat_case() == FIX["heat3d_16_2x2x2"]
     assert mg.modelc_case(0.0, 100) == FIX["modelc_64_quiet"]
     assert mg.modelc_case(0.05, 100) == FIX["modelc_64_noisy"]
+    assert mg.oriented_case(100) == FIX["modelc_64_oriented_noisy"]
+    assert mg.heat_rk4_case() == FIX["heat3d_16_rk4"]
+    assert mg.modelc_rk4_oriented_case(60) == FIX["modelc_64_rk4_oriented"]
 
 
 @pytest.mark.gpu
