@@ -99,12 +99,17 @@ def build_library(force: bool = False, verbose: bool = False) -> Path:
 def build_oracle(force: bool = False) -> Path:
     srcs = [ORACLE_DIR / "legendre_oracle.cpp", ORACLE_DIR / "legendre_oracle_amr.cpp"]
     deps = srcs + [ORACLE_DIR / "legendre_oracle.h", ORACLE_DIR / "oracle_core.hpp"]
-    if not force and not _stale(ORACLE_LIB, deps):
+    # -ffp-contract=off: no a*b+c is fused except the reference's mul_add
+    # sites (std::fma).  Without -ffast-math GCC reassociates no
+    # floating-point operation at any level, so -O3 gives the bits of -O2
+    # (the golden fixtures check it).  No -march=native: the library travels
+    # to hosts with other CPUs.
+    flags = ["-O3", "-std=c++17", "-ffp-contract=off", "-fopenmp", "-fPIC", "-shared"]
+    if not force and not _stale(ORACLE_LIB, deps, repr(flags)):
         return ORACLE_LIB
     cxx = shutil.which("g++") or "g++"
-    _run([cxx, "-O2", "-std=c++17", "-ffp-contract=off", "-fopenmp", "-fPIC", "-shared", *map(str, srcs),
-          "-o", str(ORACLE_LIB)])
-    _stamp(ORACLE_LIB, deps)
+    _run([cxx, *flags, *map(str, srcs), "-o", str(ORACLE_LIB)])
+    _stamp(ORACLE_LIB, deps, repr(flags))
     return ORACLE_LIB
 
 
