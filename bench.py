@@ -78,12 +78,38 @@ TRAFFIC_PER_CELL = {("c2", "f64"): 502.4e6 / 4096 ** 2, ("c2", "f32"): 226.3e6 /
                     ("c1big", "f64"): 318.7e6 / 256 ** 3}
 
 
+# ncu pipe use of the dominant kernel, reported beside its HBM fraction (one
+# capture each, named after its summary in profiles/): issue slots and the
+# FP64 pipe, fractions of peak sustained while active.  The multi-grain
+# figures come from the same block shape on 5040^2.
+NCU_PIPES = {("c2", "f64"): {"issue_active": 0.682, "fp64_pipe": 0.388, "capture": "modelc_strip_f64_4096sq"},
+             ("c3o", "f64"): {"issue_active": 0.568, "fp64_pipe": 0.332,
+                              "capture": "modelc_oriented_f64_5040sq_126blocks"}}
+
+NOMINAL_HBM_GBS = 8000.0  # a B200's nominal HBM3e bandwidth, the second denominator
+
+
+def captured(args) -> bool:
+    """True when the run is the configuration the ncu figures were taken on:
+    no size, noise, integrator or kernel-variant override."""
+    return args.cells is None and args.noise is None and args.integrator == "em" and args.variant in (0, 32002)
+
+
 def traffic(args, cells_per_step):
     """Measured DRAM bytes per launch of the dominant kernel, or None."""
-    if args.cells is not None or args.variant not in (0, 32002):
+    if not captured(args):
         return None
     per = TRAFFIC_PER_CELL.get((args.config, args.dtype))
     return None if per is None else per * cells_per_step
+
+
+def hbm_roofline(achieved, peak, peak_kind, **more):
+    """The roofline object: achieved GB/s against the measured copy bandwidth
+    (or the fallback) and against the nominal 8 TB/s."""
+    r = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+         "peak_kind": peak_kind, "nominal_peak": NOMINAL_HBM_GBS, "frac_nominal": achieved / NOMINAL_HBM_GBS}
+    r.update(more)
+    return r
 
 
 def peaks():
@@ -405,9 +431,9 @@ def run_other(args, cfg):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": dict({"workload": cfg["workload"], "parallelism": f"replicas{world}", "graph": True}, **extra),
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": traffic(args, cells) if cfg["kind"] == "heat" else None,
-                         "peak_kind": peak_kind, "algorithmic_bytes_per_cell": bytes_per_cell},
+            "roofline": hbm_roofline(achieved, peak, peak_kind,
+                                     traffic=traffic(args, cells) if cfg["kind"] == "heat" else None,
+                                     algorithmic_bytes_per_cell=bytes_per_cell),
             "cpu_baseline": None, "e2e": None,
             "gpu_launches": sched.kernel_launches - launches0,
             "clocks": {"sm_mhz": clk["sm_mhz"], "sm_max_mhz": clk["sm_max_mhz"], "reasons": clk["reasons"],
@@ -572,9 +598,7 @@ def run_ensemble(args, cfg):
             "config": {"workload": cfg["workload"], "instances": ninst, "cells": n, "block": b,
                        "noise": cfg["noise"], "parallelism": f"replicas{world}", "graph": True,
                        "l2": "state larger than L2; no flush"},
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
-                         "algorithmic_bytes_per_cell": bpc},
+            "roofline": hbm_roofline(achieved, peak, peak_kind, traffic=None, algorithmic_bytes_per_cell=bpc),
             "adjoint": {"steps": T, "checkpoint_every": cfg["ckpt"], "forward_ms": ms_fwd,
                         "value_and_grad_ms": ms_vg, "cost_ratio": ms_vg / ms_fwd,
                         "what": "value_and_grad = forward with checkpoints + loss + per segment: recompute and "
@@ -783,9 +807,9 @@ def main():
                        "noise": cfg["noise"], "parallelism": f"replicas{world}",
                        "l2": "state 2 fields x 2 buffers larger than L2; no flush",
                        "graph": True, "variant": args.variant, "autotuned_variant": tuned},
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": traffic(args, cells), "peak_kind": peak_kind,
-                         "algorithmic_bytes_per_cell": bpc},
+            "roofline": hbm_roofline(achieved, peak, peak_kind, traffic=traffic(args, cells),
+                                     algorithmic_bytes_per_cell=bpc,
+                                     ncu_pipes=NCU_PIPES.get((args.config, args.dtype)) if captured(args) else None),
             "cpu_baseline": cpu,
             "e2e": e2e,
             "fp32_error": err,

@@ -46,3 +46,22 @@ def test_reference_arm_line(capsys, monkeypatch, name, over):
     e2e = d["e2e"]
     assert e2e["value"] == d["value"] and e2e["unit"] == d["unit"]
     assert e2e["h2d_bytes_per_step"] == 0 and e2e["d2h_bytes_per_step"] == 0
+
+
+def test_roofline_object_carries_both_denominators_and_the_captured_figures():
+    import types
+
+    sys.path.insert(0, str(ROOT))
+    import bench
+
+    a = types.SimpleNamespace(cells=None, noise=None, integrator="em", variant=0, config="c2", dtype="f64")
+    r = bench.hbm_roofline(1600.0, 6400.0, "measured", traffic=bench.traffic(a, 4096 ** 2),
+                           algorithmic_bytes_per_cell=32)
+    assert r["bound"] == "hbm" and r["unit"] == "GB/s"
+    assert r["frac"] == 0.25 and r["frac_nominal"] == 1600.0 / 8000.0 and r["peak_kind"] == "measured"
+    assert r["traffic"] == bench.TRAFFIC_PER_CELL[("c2", "f64")] * 4096 ** 2
+    assert bench.NCU_PIPES[("c2", "f64")]["fp64_pipe"] > 0
+    # the ncu figures belong to the captured configuration only
+    for over in (dict(cells=512), dict(noise=0.0), dict(integrator="rk4"), dict(variant=3)):
+        b = types.SimpleNamespace(**dict(vars(a), **over))
+        assert not bench.captured(b) and bench.traffic(b, 4096 ** 2) is None
