@@ -65,3 +65,32 @@ def test_roofline_object_carries_both_denominators_and_the_captured_figures():
     for over in (dict(cells=512), dict(noise=0.0), dict(integrator="rk4"), dict(variant=3)):
         b = types.SimpleNamespace(**dict(vars(a), **over))
         assert not bench.captured(b) and bench.traffic(b, 4096 ** 2) is None
+
+
+def test_tip_extents_find_each_grains_four_tips():
+    import numpy as np
+
+    sys.path.insert(0, str(ROOT))
+    import bench
+
+    n, h = 96, 0.4
+    x = (np.arange(n) + 0.5) * h
+    X, Y = np.meshgrid(x, x)  # rows = y
+    grains = [((10.2, 11.0), 3.1), ((26.0, 24.4), 4.4)]
+
+    def field(scale):
+        phi = np.full((n, n), -1.0)
+        for (cx, cy), r in grains:
+            phi = np.maximum(phi, np.tanh((scale * r - np.hypot(X - cx, Y - cy)) / (2 * h)))
+        return phi
+
+    for scale in (1.0, 1.25):
+        ext = bench.tip_extents(field(scale), [c for c, _ in grains], h)
+        for g, (_, r) in enumerate(grains):
+            assert np.all(np.abs(ext[g] - scale * r) < 0.02 * h)
+    # +x agrees with the single-tip helper
+    phi = field(1.0)
+    (cx, cy), _ = grains[1]
+    assert abs(bench.tip_extents(phi, [(cx, cy)], h)[0, 0] + cx - bench.tip_position(phi, int(cy / h), cx, h)) < 1e-12
+    # a centre outside the solid has no tips
+    assert np.all(np.isnan(bench.tip_extents(phi, [(1.0, 1.0)], h)))
