@@ -262,6 +262,14 @@ int lg_amr_tag_level(lg_amr_sim* sim, int field, int level, double threshold, in
  * resolves the scratch's address and must come before any stream capture. */
 int lg_amr_tag_level_static(lg_amr_sim* sim, int field, int level, double threshold, int64_t* cells_out,
                             int64_t cap, int64_t* count);
+/* Berger-Rigoutsos clustering of flagged cells, `cluster` (amr/cluster.rs:
+ * 144-290): flags are nflags (x, y) pairs of one level, in any order (the
+ * boxes do not depend on it; flags must not repeat); *nboxes receives the number of boxes,
+ * boxes the first min(cap, *nboxes) as (lo_x, lo_y, hi_x, hi_y), half-open.
+ * efficiency in (0, 1], min_width >= 1 (LG_ERR_INVALID otherwise).  Host
+ * only: it needs no device and no context; the regrid uses the same code. */
+int lg_amr_cluster(const int64_t* flags, int64_t nflags, double efficiency, int64_t min_width, int64_t* boxes,
+                   int64_t cap, int64_t* nboxes);
 
 /* ----------------------------------------------------------- ensembles --
  * Batched Model C: `ninst` independent instances of one 2-D grid geometry

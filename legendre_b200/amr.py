@@ -56,6 +56,20 @@ class ClusterParams:
     min_width: int = 4
 
 
+def cluster(flags, params: Optional[ClusterParams] = None) -> List[CellBox]:
+    """Berger-Rigoutsos boxes covering the flagged cells of one level
+    (``cluster``, amr/cluster.rs:144-290), computed by the library's host code
+    (the same code as its regrids); ``flags`` is a sequence of (x, y)."""
+    params = params or ClusterParams()
+    arr = np.ascontiguousarray(np.asarray(flags, dtype=np.int64).reshape(-1, 2))
+    cap = max(1, len(arr))  # every box holds at least one flag
+    out = np.zeros((cap, 4), dtype=np.int64)
+    n = C.c_int64()
+    N.check(N.lib.lg_amr_cluster(arr.ctypes.data_as(C.POINTER(C.c_int64)), len(arr), float(params.efficiency),
+                                 int(params.min_width), out.ctypes.data_as(C.POINTER(C.c_int64)), cap, C.byref(n)))
+    return [CellBox((int(b[0]), int(b[1])), (int(b[2]), int(b[3]))) for b in out[:n.value]]
+
+
 @dataclass
 class GradientTagger:
     """Flag where max_d |u(i+e_d) - u(i-e_d)|/2 > threshold (adapt.rs:48-104)."""

@@ -4,6 +4,7 @@
 #include <cstdlib>
 #include <unordered_map>
 
+#include "../../include/legendre_b200.h"
 #include "lg_amr_host.h"
 
 namespace lg {
@@ -616,3 +617,26 @@ bool migrate_field(const Layout& og, const std::vector<const double*>& old, cons
 
 }  // namespace amr
 }  // namespace lg
+
+extern "C" int lg_amr_cluster(const int64_t* flags, int64_t nflags, double efficiency, int64_t min_width,
+                              int64_t* boxes, int64_t cap, int64_t* nboxes) {
+    if (!nboxes || nflags < 0 || (nflags > 0 && !flags) || cap < 0 || (cap > 0 && !boxes) ||
+        !(efficiency > 0.0 && efficiency <= 1.0) || min_width < 1)
+        return LG_ERR_INVALID;  // the reference's debug_asserts (cluster.rs:145-149)
+    try {
+        std::vector<std::array<int64_t, 2>> f((size_t)nflags);
+        for (int64_t i = 0; i < nflags; ++i) f[(size_t)i] = {flags[2 * i], flags[2 * i + 1]};
+        const std::vector<lg::amr::Box> out = lg::amr::cluster(f, efficiency, min_width);
+        *nboxes = (int64_t)out.size();
+        for (int64_t k = 0; k < std::min<int64_t>(cap, (int64_t)out.size()); ++k) {
+            const lg::amr::Box& b = out[(size_t)k];
+            boxes[4 * k + 0] = b.lo[0];
+            boxes[4 * k + 1] = b.lo[1];
+            boxes[4 * k + 2] = b.hi[0];
+            boxes[4 * k + 3] = b.hi[1];
+        }
+    } catch (const std::bad_alloc&) {
+        return LG_ERR_NOMEM;
+    }
+    return LG_OK;
+}
