@@ -270,6 +270,13 @@ int lg_amr_tag_level_static(lg_amr_sim* sim, int field, int level, double thresh
  * only: it needs no device and no context; the regrid uses the same code. */
 int lg_amr_cluster(const int64_t* flags, int64_t nflags, double efficiency, int64_t min_width, int64_t* boxes,
                    int64_t cap, int64_t* nboxes);
+/* `AmrGrid::from_patches` validation (amr/grid.rs:90-196) of a 2-D
+ * hierarchy: base cells and block as for lg_amr_sim_create, patches as
+ * (level, lo_x, lo_y, hi_x, hi_y) rows.  LG_OK, or LG_ERR_INVALID with the
+ * reason (the GridError) in err (NUL-terminated, at most errlen bytes).
+ * The same check lg_amr_sim_create and every regrid run; host only. */
+int lg_amr_check_hierarchy(const int64_t* cells, const int64_t* block, const uint32_t* ratios, int nratios,
+                           const int64_t* patches, int64_t npatches, char* err, int64_t errlen);
 
 /* ----------------------------------------------------------- ensembles --
  * Batched Model C: `ninst` independent instances of one 2-D grid geometry

@@ -105,6 +105,8 @@ _SIGS = {
     "lg_state_get_time": (C.c_int, [_p, _pd, _pi64]),
     "lg_state_field_sum": (C.c_int, [_p, C.c_int, _pd]),
     "lg_amr_cluster": (C.c_int, [_pi64, _i64, _d, _i64, _pi64, _i64, _pi64]),
+    "lg_amr_check_hierarchy": (C.c_int, [_pi64, _pi64, C.POINTER(C.c_uint32), C.c_int, _pi64, _i64, C.c_char_p,
+                                         _i64]),
     "lg_state_set_time": (C.c_int, [_p, _d, _i64]),
     "lg_fill_ghosts": (C.c_int, [_p, C.c_int]),
     "lg_heat_fe_run": (C.c_int, [_p, C.c_int, _d, _d, _i64, C.c_uint32]),

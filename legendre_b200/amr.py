@@ -16,6 +16,7 @@ from typing import List, Optional, Sequence, Tuple
 import numpy as np
 
 from . import _native as N
+from .geometry import GridError
 from .physics import Heat, ModelC
 
 Box = Tuple[Tuple[int, int], Tuple[int, int]]
@@ -41,7 +42,23 @@ class AmrGrid:
 
     @classmethod
     def from_patches(cls, base, ratios, levels=()):
-        return cls(base, list(ratios), [list(l) for l in levels])
+        """The hierarchy, validated as the reference's ``from_patches`` does
+        (ratios >= 2, patches inside their level's domain, aligned to the
+        ratio, disjoint and properly nested): ``GridError`` otherwise."""
+        g = cls(base, list(ratios), [list(l) for l in levels])
+        if base.dim == 2:  # the device AMR path is 2-D; AmrSimulation refuses other bases
+            g.validate()
+        return g
+
+    def validate(self) -> None:
+        pa = np.ascontiguousarray(self.patch_array())
+        r = (C.c_uint32 * max(1, len(self.ratios)))(*[int(x) for x in self.ratios])
+        err = C.create_string_buffer(256)
+        rc = N.lib.lg_amr_check_hierarchy((C.c_int64 * 2)(*self.base.cells), (C.c_int64 * 2)(*self.base.block_cells),
+                                          r, len(self.ratios), pa.ctypes.data_as(C.POINTER(C.c_int64)), len(pa),
+                                          err, len(err))
+        if rc != N.LG_OK:
+            raise GridError(err.value.decode() or f"invalid hierarchy ({rc})")
 
     def patch_array(self) -> np.ndarray:
         rows = [[lv + 1, b.lo[0], b.lo[1], b.hi[0], b.hi[1]] for lv, boxes in enumerate(self.levels) for b in boxes]

@@ -640,3 +640,48 @@ extern "C" int lg_amr_cluster(const int64_t* flags, int64_t nflags, double effic
     }
     return LG_OK;
 }
+
+extern "C" int lg_amr_check_hierarchy(const int64_t* cells, const int64_t* block, const uint32_t* ratios, int nratios,
+                                      const int64_t* patches, int64_t npatches, char* err, int64_t errlen) {
+    auto put = [&](const std::string& m) {
+        if (!err || errlen < 1) return;
+        const size_t n = std::min<size_t>(m.size(), (size_t)(errlen - 1));
+        std::copy(m.begin(), m.begin() + (std::ptrdiff_t)n, err);
+        err[n] = '\0';
+    };
+    if (!cells || !block || nratios < 0 || (nratios > 0 && !ratios) || npatches < 0 || (npatches > 0 && !patches)) {
+        put("null argument");
+        return LG_ERR_INVALID;
+    }
+    try {
+        lg::amr::Base base{};
+        for (int d = 0; d < 2; ++d) {
+            base.cells[d] = cells[d];
+            base.block[d] = block[d];
+            base.spacing[d] = 1.0;
+        }
+        const std::vector<uint32_t> r(ratios, ratios + nratios);
+        std::vector<std::vector<lg::amr::Box>> levels;
+        for (int64_t i = 0; i < npatches; ++i) {
+            const int64_t lv = patches[5 * i];
+            if (lv < 1 || lv > nratios) {
+                put("patch level out of range");
+                return LG_ERR_INVALID;
+            }
+            if ((int64_t)levels.size() < lv) levels.resize((size_t)lv);
+            lg::amr::Box b;
+            b.lo[0] = patches[5 * i + 1];
+            b.lo[1] = patches[5 * i + 2];
+            b.hi[0] = patches[5 * i + 3];
+            b.hi[1] = patches[5 * i + 4];
+            levels[(size_t)(lv - 1)].push_back(b);
+        }
+        lg::amr::Layout g;
+        const std::string m = lg::amr::build_layout(base, r, levels, &g);
+        put(m);
+        return m.empty() ? LG_OK : LG_ERR_INVALID;
+    } catch (const std::bad_alloc&) {
+        put("out of memory");
+        return LG_ERR_NOMEM;
+    }
+}
