@@ -38,7 +38,7 @@ import numpy as np
 
 from . import _native as N
 
-ROWS_PER_GROUP = 1 << 22  # parquet.rs:57
+ROWS_PER_GROUP = 1 << 22  # parquet.rs:60
 
 
 def fires(step: int, every: int) -> bool:
