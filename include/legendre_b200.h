@@ -82,7 +82,7 @@ int lg_grid_face_neighbor(const lg_grid* grid, int64_t block, int dim, int dir, 
 /* ------------------------------------------------------------------ state
  * The `CudaAllocator`: one device arena per state, block-major slabs, zero
  * initialised (replaces StateBuilder::build / BlockStorage::allocate,
- * src/core/state.rs:207-264, and SystemAllocator, storage.rs:560-572).
+ * src/core/state.rs:207-264, and SystemAllocator, storage.rs:177-189).
  * Field f has ghost width ghosts[f] <= every block extent
  * (cartesian.rs:456-462).  The arena is double-buffered: steps read one
  * copy and write the other, which stands in for the reference's stage

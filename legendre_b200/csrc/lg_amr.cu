@@ -868,7 +868,7 @@ double stable_dt_at(const lg_amr_sim* s, int level) {
     const auto& h = s->layout.level_spacing[level];
     const double hm = std::min(h[0], h[1]);
     if (s->model == LG_MODEL_C) return 0.2 * (hm * hm) / s->mp.d_thermal;  // phasefield.rs:446-449
-    return 0.25 * (hm * hm) / s->kappa;                                     // tests/amr.rs:341-343
+    return 0.25 * (hm * hm) / s->kappa;                                     // tests/amr.rs:339-341
 }
 
 // Subcycle::advance (subcycling.rs:195-267): ghosts (coarse source

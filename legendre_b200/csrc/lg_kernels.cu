@@ -322,7 +322,7 @@ __global__ void __launch_bounds__(256) modelc_step_ref_kernel(const T* __restric
     const int n0 = topo.n[0], n1 = topo.n[1];
     const int64_t sy = L.gdim[0];
     // Simulation::t lives on the device in two slots: this step reads
-    // tdev[slot] (its bits are the Wiener salt, euler_maruyama.rs:128) and
+    // tdev[slot] (its bits are the Wiener salt, euler_maruyama.rs:73) and
     // writes t + dt to the other slot (simulation.rs:285), so a captured
     // sequence of steps needs no host-side time.
     const double t = tdev[slot];

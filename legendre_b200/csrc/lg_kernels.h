@@ -17,7 +17,7 @@ struct ModelCDev {
     double a_bar, eps_prime, tol;                 // ModelC (phasefield.rs:100-116)
     double f_a_bar, f_eps_prime, f_a12, f_tol;    // KarmaRappelFlux (finite_volume.rs:113-122)
     double inv_h2_flux;                           // 1/(hx*hy)   (finite_volume.rs:254)
-    double inv_h2[2];                             // 1/(h_d*h_d) (finite_difference.rs:371)
+    double inv_h2[2];                             // 1/(h_d*h_d) (finite_difference.rs:54)
 };
 
 struct NoiseDev {

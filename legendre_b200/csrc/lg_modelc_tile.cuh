@@ -411,7 +411,7 @@ __global__ void __launch_bounds__(256, MINB)
     const int wpc = blockDim.x >> 5;
 
     // Simulation::t lives on the device in two slots: this step reads
-    // tdev[slot] (its bits are the Wiener salt, euler_maruyama.rs:128) and
+    // tdev[slot] (its bits are the Wiener salt, euler_maruyama.rs:73) and
     // writes t + dt to the other slot (simulation.rs:285), so a captured
     // sequence of steps needs no host-side time.
     const double tnow = g.tdev[g.slot];

@@ -3,7 +3,7 @@
 ``ForwardEuler`` and ``EulerMaruyama`` mirror src/integrators/euler.rs and
 euler_maruyama.rs; their ``run`` dispatches the fused device step for the
 model at hand.  ``FiniteVolume`` / ``FiniteDifference`` are the reference's
-discretisation policies (finite_volume.rs:41-50, finite_difference.rs:338-356).
+discretisation policies (finite_volume.rs:41-50, finite_difference.rs:23-43).
 """
 from __future__ import annotations
 
@@ -46,7 +46,7 @@ class ForwardEuler:
 
 @dataclass
 class EulerMaruyama:
-    """Euler-Maruyama (euler_maruyama.rs:66-131); ``seed`` keys the noise."""
+    """Euler-Maruyama (euler_maruyama.rs:21-75); ``seed`` keys the noise."""
 
     seed: int = 0
 
