@@ -624,9 +624,11 @@ bool hierarchy_acceptable(const AmrGrid& g, const std::vector<std::vector<CellBo
 }
 
 // BergerOliger::regrid (adapt.rs:152-237); returns true with the new grid
-// and migrated state when the hierarchy changes.
+// and migrated state when the hierarchy changes.  `forced`, when given,
+// holds each source level's flags in place of the gradient tagger (a test's
+// own TagCells, tests/amr.rs:800-823).
 bool regrid(const AmrGrid& g, AmrState& s, const Policy& pol, const std::vector<int>& prepare_fields,
-            int64_t step, AmrGrid* ng, AmrState* ns) {
+            int64_t step, AmrGrid* ng, AmrState* ns, const std::vector<std::vector<Cell>>* forced = nullptr) {
     if (step % pol.every != 0) return false;
     for (int f : prepare_fields) {
         restrict_all(g, s, f);
@@ -637,7 +639,11 @@ bool regrid(const AmrGrid& g, AmrState& s, const Policy& pol, const std::vector<
     for (int target = capacity; target >= 1; --target) {
         const int src = target - 1;
         std::vector<Cell> flags;
-        if (src < g.num_levels()) tag_level(g, s, pol.field, pol.threshold, src, flags);
+        if (forced) {
+            if (src < (int)forced->size()) flags = (*forced)[src];
+        } else if (src < g.num_levels()) {
+            tag_level(g, s, pol.field, pol.threshold, src, flags);
+        }
         if (pol.buffer > 0) {
             std::vector<Cell> seeds;
             seeds.swap(flags);
@@ -704,7 +710,7 @@ struct AmrSim {
     int nthreads = 1;
 
     int nfields() const { return model == MODEL_C ? 2 : 1; }
-    // phasefield.rs:446-449 (0.2 h^2 / D) ; tests/amr.rs:341-343 (0.25 h^2 / kappa)
+    // phasefield.rs:446-449 (0.2 h^2 / D) ; tests/amr.rs:339-341 (0.25 h^2 / kappa)
     double stable_dt_at(int level) const {
         const auto& h = grid.level_spacing[level];
         double hm = std::min(h[0], h[1]);
@@ -927,6 +933,26 @@ int64_t orc_amr_sim_tag(const void* s, int f, double threshold, int level, int64
         out[2 * i + 1] = flags[i][1];
     }
     return (int64_t)flags.size();
+}
+// a regrid now, with the level-0 flags given (n (x, y) pairs) instead of the
+// tagger, buffer and clustering as given, no field preparation; 1 when the
+// hierarchy changed (its epoch advances), 0 when it was kept
+int orc_amr_sim_regrid_flags(void* s, const int64_t* flags, int64_t n, int64_t buffer, double efficiency,
+                             int64_t min_width) {
+    AmrSim* sim = static_cast<AmrSim*>(s);
+    Policy pol = sim->policy;
+    pol.every = 1;
+    pol.buffer = buffer;
+    pol.cluster = ClusterParams{efficiency, min_width};
+    std::vector<std::vector<Cell>> forced(1);
+    for (int64_t i = 0; i < n; ++i) forced[0].push_back({flags[2 * i], flags[2 * i + 1], 0});
+    AmrGrid ng;
+    AmrState ns;
+    if (!regrid(sim->grid, sim->state, pol, {}, 0, &ng, &ns, &forced)) return 0;
+    sim->grid = std::move(ng);
+    sim->state = std::move(ns);
+    sim->epoch += 1;
+    return 1;
 }
 void orc_amr_sim_cell_center(const void* s, int64_t b, const int64_t* idx, double* out) {
     static_cast<const AmrSim*>(s)->grid.cell_center(b, idx, out);

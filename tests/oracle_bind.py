@@ -218,6 +218,7 @@ def _amr_sigs():
         "orc_amr_sim_restrict": (None, [p, C.c_int]),
         "orc_amr_sim_fill_ghosts": (None, [p, C.c_int]),
         "orc_amr_sim_tag": (i64, [p, C.c_int, d, C.c_int, pi64, i64]),
+        "orc_amr_sim_regrid_flags": (C.c_int, [p, pi64, i64, i64, d, i64]),
         "orc_amr_sim_cell_center": (None, [p, i64, pi64, pd]),
     }
     for name, (res, args) in sigs.items():
@@ -322,6 +323,13 @@ class AmrSim:
         out = np.zeros(2 * cap, dtype=np.int64)
         n = lib.orc_amr_sim_tag(self.h, f, threshold, level, out.ctypes.data_as(C.POINTER(C.c_int64)), cap)
         return [tuple(out[2 * i:2 * i + 2]) for i in range(n)]
+
+    def regrid_flags(self, flags, buffer, efficiency, min_width):
+        """Regrid now with these level-0 flags in place of the tagger; True
+        when the hierarchy changed."""
+        arr = np.ascontiguousarray(np.array(flags, dtype=np.int64).reshape(-1, 2))
+        return bool(lib.orc_amr_sim_regrid_flags(self.h, arr.ctypes.data_as(C.POINTER(C.c_int64)), len(arr),
+                                                 buffer, efficiency, min_width))
 
     def centers(self, b):
         """(xc, yc) arrays of the interior cell centres of block b, shape (ny, nx)."""
