@@ -42,7 +42,8 @@ def test_null_arguments_are_rejected_without_a_device():
 
 
 def test_grid_validation_mirrors_the_reference():
-    # CartesianGrid::new errors (cartesian.rs:48-82) on the host mirror
+    # CartesianGrid::new errors (cartesian.rs:48-82; tests/framework.rs:30-46)
+    # on the host mirror
     import pytest
     from legendre_b200 import CartesianGrid, GridError
     with pytest.raises(GridError):

@@ -1,7 +1,9 @@
 """Snapshots through the device ring (AsyncObserver) on a GPU.
 
 * Every snapshot equals the state of a twin run at its step, bit for bit
-  (FP64, FP32 widened to FP64, 2-D Model C and 3-D heat), with step and time.
+  (FP64, FP32 widened to FP64, 2-D Model C and 3-D heat), with step and time;
+  the sinks see every snapshot and their finish() at shutdown
+  (tests/model_c.rs:144-178).
 * When the sink falls behind, snapshots are dropped and counted; the run
   itself is unchanged bit for bit, and the snapshots that did go through are
   the right ones.

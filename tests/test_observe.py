@@ -128,3 +128,16 @@ def test_runs_are_cut_at_the_observed_steps():
     # resuming mid-run: no step 1, the next multiple first
     assert observed_stretches(7, 10, [5]) == [3, 5, 2]
     assert sum(observed_stretches(3, 100, [7, 11])) == 100
+
+
+def test_async_observer_cadence_of_the_reference():
+    # tests/model_c.rs:144-178: every 20 over 100 steps observes steps 1, 20,
+    # 40, 60, 80 and 100 (delivery and the drain at shutdown run on the
+    # device in tests/test_gpu_observe.py)
+    from itertools import accumulate
+
+    from legendre_b200.core import observed_stretches
+
+    ends = list(accumulate(observed_stretches(0, 100, [20])))
+    assert [s for s in ends if s == 1 or s % 20 == 0] == [1, 20, 40, 60, 80, 100]
+    assert ends[-1] == 100
