@@ -141,3 +141,28 @@ def test_async_observer_cadence_of_the_reference():
     ends = list(accumulate(observed_stretches(0, 100, [20])))
     assert [s for s in ends if s == 1 or s % 20 == 0] == [1, 20, 40, 60, 80, 100]
     assert ends[-1] == 100
+
+
+def test_runs_end_exactly_at_the_observed_steps_property():
+    # every step an observer fires on ends a run, and no other step does
+    # (except the last step of the call)
+    from hypothesis import given, settings
+    from hypothesis import strategies as st
+
+    from legendre_b200.core import observed_stretches
+    from legendre_b200.observe import fires
+
+    @settings(max_examples=200, deadline=None)
+    @given(st.integers(0, 60), st.integers(1, 80), st.lists(st.integers(1, 13), min_size=1, max_size=3))
+    def check(k, n, everys):
+        runs = observed_stretches(k, n, everys)
+        assert all(r > 0 for r in runs) and sum(runs) == n
+        ends, e = [], k
+        for r in runs:
+            e += r
+            ends.append(e)
+        fired = [s for s in range(k + 1, k + n + 1) if any(fires(s, c) for c in everys)]
+        assert [s for s in ends if s in fired] == fired
+        assert all(s in fired for s in ends[:-1])
+
+    check()
