@@ -2,6 +2,8 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdlib>
+#include <system_error>
+#include <thread>
 #include <unordered_map>
 
 #include "../../include/legendre_b200.h"
@@ -603,16 +605,40 @@ bool migrate_field(const Layout& og, const std::vector<const double*>& old, cons
             if (!old[b]) return false;
             std::copy(old[b], old[b] + (size_t)(bx.extent(0) + 2) * (size_t)(bx.extent(1) + 2), out[b]);
         }
-    Sampler smp(og, old);
-    for (int level = 1; level < ng.num_levels(); ++level)
-        for (uint32_t b = ng.level_start[level]; b < ng.level_start[level + 1]; ++b) {
+    // The refined blocks: each is sampled on its own (sample is a pure
+    // function of the old hierarchy), so blocks b0 + t, b0 + t + nt, ... go
+    // to thread t with its own memo, and the result is the same for any
+    // thread count.
+    const uint32_t b0 = ng.num_levels() > 1 ? ng.level_start[1] : (uint32_t)ng.num_blocks();
+    const uint32_t b1 = (uint32_t)ng.num_blocks();
+    uint64_t cells = 0;
+    for (uint32_t b = b0; b < b1; ++b) cells += ng.patches[b].bx.cells();
+    auto work = [&](unsigned t, unsigned nt, char* missing) {
+        Sampler smp(og, old);
+        for (uint32_t b = b0 + t; b < b1; b += nt) {
+            const int level = ng.patches[b].level;
             const Box& bx = ng.patches[b].bx;
             for (int64_t j = 0; j < bx.extent(1); ++j)
                 for (int64_t i = 0; i < bx.extent(0); ++i)
                     out[b][(size_t)((i + 1) + (j + 1) * (bx.extent(0) + 2))] =
                         smp.at(level, bx.lo[0] + i, bx.lo[1] + j, false);
         }
-    return !smp.missing;
+        *missing = smp.missing ? 1 : 0;
+    };
+    unsigned nt = std::min(std::max(1u, std::thread::hardware_concurrency()), 16u);
+    nt = (unsigned)std::min<uint64_t>(nt, std::max<uint64_t>(1, cells / 8192));  // >= 8192 cells a thread
+    std::vector<char> missing(nt, 0);
+    std::vector<std::thread> pool;
+    unsigned started = 1;
+    try {
+        for (; started < nt; ++started) pool.emplace_back(work, started, nt, &missing[started]);
+    } catch (const std::system_error&) {
+        // no more threads: this one takes the remaining shares
+    }
+    work(0, nt, &missing[0]);
+    for (unsigned t = started; t < nt; ++t) work(t, nt, &missing[t]);
+    for (std::thread& th : pool) th.join();
+    return std::find(missing.begin(), missing.end(), 1) == missing.end();
 }
 
 }  // namespace amr
