@@ -70,12 +70,13 @@ CONFIGS = {
 BYTES_PER_CELL = {"f64": 32, "f32": 16}  # read phi, u; write phi, u
 
 # DRAM bytes (read + write) per cell-update of the dominant kernel, from one
-# ncu capture each (profiles/): the strip kernel on 4096^2 (FP64 502 MB and
-# FP32 226 MB per 16.8M-cell launch) and the 3-D heat kernel on 256^3 (319 MB
-# per 16.8M cells; the 512^3 run has the same per-block work, so its traffic
-# scales with the cell count).  Other workloads report null.
-TRAFFIC_PER_CELL = {("c2", "f64"): 502.4e6 / 4096 ** 2, ("c2", "f32"): 226.3e6 / 4096 ** 2,
-                    ("c1big", "f64"): 318.7e6 / 256 ** 3}
+# ncu capture each of the kernel as it now is (profiles/): the FP64 strip
+# kernel on 4096^2 (502 MB per 16.8M-cell launch) and the 3-D heat kernel on
+# 256^3 (319 MB per 16.8M cells; the 512^3 run has the same per-block work,
+# so its traffic scales with the cell count).  Other workloads, the FP32
+# strip kernel among them (its capture predates its rolled row loop),
+# report null.
+TRAFFIC_PER_CELL = {("c2", "f64"): 502.4e6 / 4096 ** 2, ("c1big", "f64"): 318.7e6 / 256 ** 3}
 
 
 # ncu pipe use of the dominant kernel, reported beside its HBM fraction (one
