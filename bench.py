@@ -1,12 +1,13 @@
 #!/usr/bin/env python
 """Throughput of the fused Model C step on B200 (Gcell-updates/s).
 
-Workload (default): Karma-Rappel Model C on 4096^2 cells as 16x16 blocks of
-256^2, ghost 1, h = 0.4, dt = 0.008, D = 2, lambda = D/0.6267, eps4 = 0.05,
-u0 = -0.55, 16 seeded grains of radius 8, zero-flux boundaries, Gaussian
-noise b = 0.01, Euler-Maruyama, FP64.  A step is one time step over the whole
-grid (16.8M cell-updates).  The state (2 fields x 2 buffers, 0.54 GB) is
-larger than L2, so no flush is needed between steps.
+Workload (default, --config c3): Karma-Rappel Model C on 10080^2 =
+101,606,400 cells as 80x80 blocks of 126^2, ghost 1, h = 0.4, dt = 0.008,
+D = 2, lambda = D/0.6267, eps4 = 0.05, u0 = -0.5, 64 seeded grains of radius
+8, zero-flux boundaries, Gaussian noise b = 0.01, Euler-Maruyama, FP64.  A
+step is one time step over the whole grid (101.6M cell-updates).  The state
+(2 fields x 2 buffers, 4.2 GB) is far larger than L2, so no flush is needed
+between steps.  --config c2 is the 4096^2 grid of 16x16 blocks of 256^2.
 
 Arms:
   default          this library on N GPUs (N independent replicas, one per
@@ -90,7 +91,7 @@ NCU_PIPES = {("c2", "f64"): {"issue_active": 0.682, "fp64_pipe": 0.388, "capture
 NOMINAL_HBM_GBS = 8000.0  # a B200's nominal HBM3e bandwidth, the second denominator
 
 
-def captured(args) -> bool:
+def ncu_capture_config(args) -> bool:
     """True when the run is the configuration the ncu figures were taken on:
     no size, noise, integrator or kernel-variant override."""
     return args.cells is None and args.noise is None and args.integrator == "em" and args.variant in (0, 32002)
@@ -98,7 +99,7 @@ def captured(args) -> bool:
 
 def traffic(args, cells_per_step):
     """Measured DRAM bytes per launch of the dominant kernel, or None."""
-    if not captured(args):
+    if not ncu_capture_config(args):
         return None
     per = TRAFFIC_PER_CELL.get((args.config, args.dtype))
     return None if per is None else per * cells_per_step
@@ -326,13 +327,15 @@ def fp32_error(cfg, sched, steps):
             "reference": "the FP64 path, bit-identical to the CPU oracle, from the same state and noise keys"}
 
 
-def cpu_oracle_rate(cfg, steps_budget_s: float, max_steps: int):
+def cpu_oracle_rate(cfg, steps_budget_s: float, max_steps: int, warmup: int = 1):
     """Oracle (C++ restatement of the reference's CPU path), all host threads,
-    on the full grid; returns (Gcell/s, steps run, threads)."""
+    on the full grid; returns (Gcell/s, steps run, threads, ms per step).
+    Loads only the oracle's library: the seed placement comes from the
+    package's pure-Python module, which maps no device code."""
     sys.path.insert(0, str(ROOT / "tests"))
     import oracle_bind as orc
 
-    from legendre_b200 import seed_positions
+    from legendre_b200.seeding import seed_positions
 
     n, b, h = cfg["cells"], cfg["block"], cfg["h"]
     og = orc.Grid([n, n], [b, b], [0.0, 0.0], [h, h])
@@ -351,27 +354,29 @@ def cpu_oracle_rate(cfg, steps_budget_s: float, max_steps: int):
         return st.modelc_run(p, t, cfg["dt"], cfg["seed"], k, True, threads)
 
     t0 = time.perf_counter()
-    t = run(0.0, 1)
-    one = time.perf_counter() - t0
+    t = run(0.0, max(1, warmup))
+    one = (time.perf_counter() - t0) / max(1, warmup)
     steps = max(1, min(max_steps, int(steps_budget_s / max(one, 1e-6))))
     t0 = time.perf_counter()
     run(t, steps)
     el = time.perf_counter() - t0
-    return n * n * steps / el / 1e9, steps, threads
+    return n * n * steps / el / 1e9, steps, threads, 1e3 * el / steps
 
 
 def run_reference(args, cfg):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    rate, steps, threads = cpu_oracle_rate(cfg, steps_budget_s=60.0, max_steps=args.steps)
+    rate, steps, threads, ms_step = cpu_oracle_rate(cfg, steps_budget_s=60.0, max_steps=args.steps,
+                                                    warmup=args.warmup)
     line = {
         "metric": "Gcell-updates/s", "value": rate, "unit": "Gcell-updates/s", "impl": "reference",
-        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+        "n_gpus": args.gpus, "steps": steps, "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
         "dtype": "f64", "data": "synthetic",
         "config": {"workload": cfg["workload"], "cells": cfg["cells"], "block": cfg["block"], "noise": cfg["noise"]},
         "cpu_baseline": {"value": rate, "unit": "Gcell-updates/s", "cores": threads, "kind": "port",
-                         "sample": f"{steps} of {args.steps} steps on the full {cfg['cells']}^2 grid (plus 1 warm-up)"},
+                         "sample": f"{steps} of {args.steps} steps on the full {cfg['cells']}^2 grid "
+                                   f"(after {args.warmup} warm-up steps)"},
         "e2e": {"value": rate, "unit": "Gcell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "note": "the reference (Rust) cannot be built here; this arm times the C++ restatement of its "
                 "SerialScheduler path with OpenMP over blocks (RayonScheduler's parallelism)",
@@ -626,7 +631,7 @@ def run_ensemble(args, cfg):
         if not args.no_cpu_baseline and world == 1:
             c2 = dict(CONFIGS["c2"], cells=n, block=b, grains=1, noise=cfg["noise"], u0=delta[0], eps4=eps4[0],
                       dt=dt)
-            rate, steps_run, threads = cpu_oracle_rate(c2, steps_budget_s=15.0, max_steps=2000)
+            rate, steps_run, threads, _ = cpu_oracle_rate(c2, steps_budget_s=15.0, max_steps=2000)
             cpu = {"value": rate, "unit": "Gcell-updates/s", "cores": threads, "kind": "port",
                    "sample": f"{steps_run} steps of one {n}^2 instance (the instances are independent; the rate "
                              "per cell-update is the same), OpenMP over blocks"}
@@ -663,13 +668,63 @@ def run_ensemble(args, cfg):
         pg.destroy_process_group()
 
 
-def main():
+def model_c_line(args, cfg, world, ms, clk, launches, tuned, e2e, observed, err, cpu, peak, peak_kind):
+    """The JSON line of a uniform-grid Model C run from its measured parts
+    (device time of the K timed steps `ms`, sampled clocks, launch count,
+    autotuner choice, end-to-end and observer blocks, FP32 error, CPU
+    baseline and the HBM peak); pure, so it is tested on the host."""
+    cells = cfg["cells"] ** 2
+    ms_per_step = ms / args.steps
+    value = world * cells * args.steps / (ms / 1e3) / 1e9
+    # the multi-grain step also reads cos and sin theta0 of every cell; an
+    # RK4 step is four stages: three read their input and y and write k and
+    # the next input (phi and u of each: 8 values), the last reads its input,
+    # y and k1..k3 and writes y (12 values): 36 values per cell
+    esz = 8 if args.dtype == "f64" else 4
+    bpc = BYTES_PER_CELL[args.dtype] + (2 * esz if cfg.get("orient") else 0)
+    if cfg.get("integrator") == "rk4":
+        bpc = 36 * esz + (4 * 2 * esz if cfg.get("orient") else 0)
+    achieved = bpc * cells / (ms_per_step / 1e3) / 1e9
+    captured_cfg = ncu_capture_config(args)
+    return {
+        "metric": "Gcell-updates/s", "value": value, "unit": "Gcell-updates/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": args.dtype, "data": "synthetic",
+        "config": {"workload": cfg["workload"], "cells": cfg["cells"], "block": cfg["block"],
+                   "noise": cfg["noise"], "parallelism": f"replicas{world}",
+                   "l2": "state 2 fields x 2 buffers larger than L2; no flush",
+                   "graph": True, "variant": args.variant, "autotuned_variant": tuned},
+        "roofline": hbm_roofline(achieved, peak, peak_kind, traffic=traffic(args, cells),
+                                 algorithmic_bytes_per_cell=bpc,
+                                 ncu_pipes=NCU_PIPES.get((args.config, args.dtype)) if captured_cfg else None),
+        "cpu_baseline": cpu,
+        "e2e": e2e,
+        "fp32_error": err,
+        "observer": observed,
+        "gpu_launches": launches,
+        "clocks": {"sm_mhz": clk["sm_mhz"], "sm_max_mhz": clk["sm_max_mhz"], "reasons": clk["reasons"],
+                   "samples": clk["samples"]},
+    }
+
+
+def observer_block(args, world, cells, ms, ms_obs, snaps_taken, snaps_dropped):
+    """The `observer` object of a Model C line: the same K steps timed with an
+    AsyncObserver attached, against `ms` without it."""
+    return {"every": args.observe_every, "slots": 3,
+            "value": world * cells * args.steps / (ms_obs / 1e3) / 1e9, "unit": "Gcell-updates/s",
+            "slowdown": ms_obs / ms - 1.0, "captured": snaps_taken, "dropped": snaps_dropped,
+            "snapshot_bytes": 2 * cells * 8,
+            "what": "device-timed K steps with the observer attached (gather kernel on the stepping "
+                    "stream, copy on the ring's stream, a host thread reducing each snapshot)"}
+
+
+def parse_args(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=2000)
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="own", choices=["own", "reference"])
-    ap.add_argument("--config", default="c2", choices=sorted(CONFIGS))
+    ap.add_argument("--config", default="c3", choices=sorted(CONFIGS))
     ap.add_argument("--dtype", default="f64", choices=["f64", "f32"])
     ap.add_argument("--variant", type=int, default=0)
     ap.add_argument("--noise", type=float, default=None, help="override the noise amplitude b")
@@ -680,8 +735,9 @@ def main():
                     help="rk4: RungeKutta4 (deterministic: the noise amplitude is set to 0)")
     ap.add_argument("--observe-every", type=int, default=0,
                     help="also time the run with an AsyncObserver snapshotting phi and u every N steps")
-    args = ap.parse_args()
-    args.dtype_given = any(a == "--dtype" or a.startswith("--dtype=") for a in sys.argv[1:])
+    argv = sys.argv[1:] if argv is None else list(argv)
+    args = ap.parse_args(argv)
+    args.dtype_given = any(a == "--dtype" or a.startswith("--dtype=") for a in argv)
     args.warmup = max(args.warmup, 3)
     cfg = dict(CONFIGS[args.config])
     if args.noise is not None:
@@ -696,16 +752,28 @@ def main():
     if args.instances is not None:
         cfg["instances"] = args.instances
         cfg["workload"] += f"_inst{args.instances}"
+    return args, cfg
+
+
+def main():
+    args, cfg = parse_args()
     if args.impl == "reference":
         run_reference(args, cfg)
         return
-
     if cfg.get("kind") in ("heat", "amr"):
         run_other(args, cfg)
         return
     if cfg.get("kind") == "ensemble":
         run_ensemble(args, cfg)
         return
+    run_model_c(args, cfg)
+
+
+def run_model_c(args, cfg):
+    """Uniform-grid Model C (c2, c3, c3o): device-timed K steps, the same K
+    steps end to end through the C ABI from pinned host buffers, and the
+    optional observer, FP32-error and CPU-baseline legs."""
+    import ctypes as C
 
     import torch
 
@@ -746,17 +814,12 @@ def main():
     clk = clocks.stop()
     launches = sched.kernel_launches - launches0
     ms = max_over_ranks(pg, e0.elapsed_time(e1))
-    ms_per_step = ms / args.steps
-    value = world * cells * args.steps / (ms / 1e3) / 1e9
 
-    # end to end through the public API: pinned host state in, K steps, state out
-    e2e = None
+    # end to end through the C ABI: pinned host state in, K steps, state out
     sdtype = torch.float64 if args.dtype == "f64" else torch.float32
     n_el = grid.num_blocks() * grid.block_len(1)
     host_in = [torch.from_numpy(sim.state.download(f).reshape(-1)).pin_memory() for f in ("phi", "u")]
     host_out = [torch.empty(n_el, dtype=sdtype).pin_memory() for _ in range(2)]
-    import ctypes as C
-
     barrier(pg)
     torch.cuda.synchronize()
     e2 = torch.cuda.Event(enable_timing=True)
@@ -777,7 +840,7 @@ def main():
     e2e = {"value": world * cells * args.steps / (ms_e2e / 1e3) / 1e9, "unit": "Gcell-updates/s",
            "h2d_bytes_per_step": 2 * n_el * esz / args.steps, "d2h_bytes_per_step": 2 * n_el * esz / args.steps,
            "what": f"lg_state_upload_field x2 from pinned host + {args.steps} steps + lg_state_download_field x2, "
-                   "bytes amortised per step"}
+                   "device-timed on the library's stream, bytes amortised per step"}
 
     # observed: the same K steps with an AsyncObserver taking snapshots of
     # phi and u every N steps into a 3-slot ring; its sink reduces each one on
@@ -808,56 +871,23 @@ def main():
         e5.record(stream)
         torch.cuda.synchronize()
         ms_obs = max_over_ranks(pg, e4.elapsed_time(e5))
-        captured, dropped = obs.stats()
+        snaps_taken, snaps_dropped = obs.stats()
         obs.close()
         sim.observers.clear()
-        observed = {"every": args.observe_every, "slots": 3,
-                    "value": world * cells * args.steps / (ms_obs / 1e3) / 1e9, "unit": "Gcell-updates/s",
-                    "slowdown": ms_obs / ms - 1.0, "captured": captured, "dropped": dropped,
-                    "snapshot_bytes": 2 * cells * 8,
-                    "what": "device-timed K steps with the observer attached (gather kernel on the stepping "
-                            "stream, copy on the ring's stream, a host thread reducing each snapshot)"}
+        observed = observer_block(args, world, cells, ms, ms_obs, snaps_taken, snaps_dropped)
 
     if rank == 0:
         peak, peak_kind = peaks()
-        # the multi-grain step also reads cos and sin theta0 of every cell;
-        # an RK4 step is four stages: three read their input and y and write
-        # k and the next input (phi and u of each: 8 values), the last reads
-        # its input, y and k1..k3 and writes y (12 values): 36 values per cell
-        esz_ = 8 if args.dtype == "f64" else 4
-        bpc = BYTES_PER_CELL[args.dtype] + (2 * esz_ if cfg.get("orient") else 0)
-        if cfg.get("integrator") == "rk4":
-            bpc = 36 * esz_ + (4 * 2 * esz_ if cfg.get("orient") else 0)
-        algo = bpc * cells
-        achieved = algo / (ms_per_step / 1e3) / 1e9
         err = None
         if args.dtype == "f32" and world == 1:
             err = fp32_error(cfg, sched, min(args.steps, cfg["full_steps"]))
         cpu = None
         if not args.no_cpu_baseline and world == 1:
-            rate, steps_run, threads = cpu_oracle_rate(cfg, steps_budget_s=15.0, max_steps=1000)
+            rate, steps_run, threads, _ = cpu_oracle_rate(cfg, steps_budget_s=15.0, max_steps=1000)
             cpu = {"value": rate, "unit": "Gcell-updates/s", "cores": threads, "kind": "port",
                    "sample": f"{steps_run} steps of the same {cfg['cells']}^2 grid after 1 warm-up step, "
                              "OpenMP over blocks"}
-        line = {
-            "metric": "Gcell-updates/s", "value": value, "unit": "Gcell-updates/s", "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": args.dtype, "data": "synthetic",
-            "config": {"workload": cfg["workload"], "cells": cfg["cells"], "block": cfg["block"],
-                       "noise": cfg["noise"], "parallelism": f"replicas{world}",
-                       "l2": "state 2 fields x 2 buffers larger than L2; no flush",
-                       "graph": True, "variant": args.variant, "autotuned_variant": tuned},
-            "roofline": hbm_roofline(achieved, peak, peak_kind, traffic=traffic(args, cells),
-                                     algorithmic_bytes_per_cell=bpc,
-                                     ncu_pipes=NCU_PIPES.get((args.config, args.dtype)) if captured(args) else None),
-            "cpu_baseline": cpu,
-            "e2e": e2e,
-            "fp32_error": err,
-            "observer": observed,
-            "gpu_launches": launches,
-            "clocks": {"sm_mhz": clk["sm_mhz"], "sm_max_mhz": clk["sm_max_mhz"], "reasons": clk["reasons"],
-                       "samples": clk["samples"]},
-        }
+        line = model_c_line(args, cfg, world, ms, clk, launches, tuned, e2e, observed, err, cpu, peak, peak_kind)
         print(json.dumps(line), flush=True)
     sched.close()
     if pg is not None:

@@ -258,8 +258,11 @@ int lg_amr_tag_level(lg_amr_sim* sim, int field, int level, double threshold, in
  * a static device scratch of 2^18 cells (4 MiB) and sorted in place in
  * cells_out.  Fails with LG_ERR_INVALID when the level has more than 2^18
  * cells, or when cap < *count (nothing copied, *count set).  Calls that
- * overlap on the GPU race on the scratch; the first call on a device
- * resolves the scratch's address and must come before any stream capture. */
+ * overlap on the GPU race on the scratch.  Every call synchronises the
+ * context's stream (the flag count is read back), so it must not be called
+ * while that stream is being captured.  The first call on a device resolves
+ * the scratch's address and caches it: not valid across a cudaDeviceReset.
+ * Only the error paths allocate (a host message string). */
 int lg_amr_tag_level_static(lg_amr_sim* sim, int field, int level, double threshold, int64_t* cells_out,
                             int64_t cap, int64_t* count);
 /* Berger-Rigoutsos clustering of flagged cells, `cluster` (amr/cluster.rs:

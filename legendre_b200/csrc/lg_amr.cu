@@ -1561,19 +1561,22 @@ int lg_amr_tag_level(lg_amr_sim* s, int field, int level, double threshold, int6
     return LG_OK;
 }
 
-// A tagging entry point that allocates nothing (no cudaMalloc, cudaFree or
-// allocating library call on the device, no host heap): the flags are
-// compacted into the file-scope static scratch above, whose address is
-// resolved once per device, and sorted in place in the caller's buffer.  It
+// A tagging entry point that allocates nothing on its success path (no
+// cudaMalloc, cudaFree or allocating library call, no host heap; only its
+// error reports build a message string): the flags are compacted into the
+// file-scope static scratch above, whose address is resolved once per
+// device, and sorted in place in the caller's buffer.  It
 // serves callers that cannot allocate: a step loop whose device memory is
 // all held by a caching allocator (a cudaMalloc there fails or forces the
 // cache to be released), and latency-bound loops in which cudaMalloc /
 // cudaFree, which synchronise the device, would stall the stream.
 // Limits: the level has at most 2^18 cells; cells_out needs room for every
 // flagged cell (cap >= *count), else nothing is copied and the call fails
-// with *count set.  Calls that overlap on the GPU race on the scratch; the
-// first call on a device (which resolves the scratch address) must come
-// before any stream capture.
+// with *count set.  Calls that overlap on the GPU race on the scratch.  Every
+// call waits for its stream (it reads the flag count back to the host), so
+// no call may be made while that stream is being captured into a graph.  The
+// scratch address cached per device is that of the device's current primary
+// context: the library must not be used on a device after a cudaDeviceReset.
 namespace {
 std::mutex g_scratch_mutex;
 int64_t* g_scratch_ptr[64] = {};

@@ -7,7 +7,6 @@ from __future__ import annotations
 
 import ctypes as C
 import math
-from dataclasses import dataclass
 from typing import Optional, Sequence
 
 import numpy as np
@@ -15,19 +14,11 @@ import numpy as np
 from . import _native as N
 from .core import TIME, wiener
 from .rng import fma
+from .seeding import Grain, seed_positions  # noqa: F401  (re-exported)
 
 #: Karma-Rappel thin-interface constants (src/physics/phasefield.rs:41-44).
 A1 = 0.8836
 A2 = 0.6267
-
-
-@dataclass
-class Grain:
-    """One nucleation site (phasefield.rs:78-88)."""
-
-    center: Sequence[float]
-    radius: float
-    orientation: float = 0.0
 
 
 class ModelC:
@@ -122,31 +113,6 @@ class ModelC:
         if self.orientations:  # theta0 by nearest-seed Voronoi (phasefield.rs:286-311)
             N.check(N.lib.lg_modelc_initialize_orientations(state.handle, state._index("theta0"), ptr, len(grains)),
                     state.scheduler.handle)
-
-
-def seed_positions(cells: int, h: float, nseeds: int, seed: int, radius: Optional[float] = None,
-                   orient: bool = False):
-    """Seed placement of the model_c example (examples/model_c.rs:175-206):
-    one corner seed, or ``nseeds`` uniform positions with a margin of two
-    radii; with ``orient`` grain i has the orientation
-    unit_open(mix_key(seed, [i, 2])) * pi/2 (the 4-fold fundamental domain)."""
-    import math
-
-    from .rng import mix_key, unit_open
-
-    radius = 10.0 * h if radius is None else float(radius)
-    orientation = (lambda i: unit_open(mix_key(seed, [i, 2])) * (math.pi / 2)) if orient else (lambda i: 0.0)
-    if nseeds <= 1:
-        return [Grain((h, h), radius, orientation(0))]
-    extent = cells * h
-    margin = 2.0 * radius
-    span = fma(2.0, -margin, extent)
-    out = []
-    for i in range(nseeds):
-        x = margin + unit_open(mix_key(seed, [i, 0])) * span
-        y = margin + unit_open(mix_key(seed, [i, 1])) * span
-        out.append(Grain((x, y), radius, orientation(i)))
-    return out
 
 
 class Heat:
