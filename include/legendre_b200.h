@@ -381,6 +381,22 @@ int lg_state_field_sum(lg_state* st, int field, double* sum);
  * src/util/rng.rs:43-49); host arrays in and out. */
 int lg_standard_normal(lg_ctx* ctx, const uint64_t* keys, int64_t n, double* out);
 
+/* Compute-side roofline denominators, measured on the context's device (no
+ * counterpart in the reference, which publishes no device figures):
+ * retired operations per second, over all SMs, of independent chains of
+ * FP64 FMAs, FP32 FMAs, 32-bit integer multiply-adds and plain 32-bit ALU
+ * operations (xor, add) at full occupancy; best of three ~ms-long launches
+ * timed with CUDA events.  Waits for the context's stream. */
+typedef struct lg_compute_peaks {
+    double dfma_per_s;
+    double ffma_per_s;
+    double imad_per_s;
+    double alu_per_s;
+    int32_t sms;
+    double clock_mhz;  /* the device's reported maximum SM clock */
+} lg_compute_peaks;
+int lg_measure_compute_peaks(lg_ctx* ctx, lg_compute_peaks* out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -63,6 +63,17 @@ class AmrPolicy(C.Structure):
     ]
 
 
+class ComputePeaks(C.Structure):
+    _fields_ = [
+        ("dfma_per_s", C.c_double),
+        ("ffma_per_s", C.c_double),
+        ("imad_per_s", C.c_double),
+        ("alu_per_s", C.c_double),
+        ("sms", C.c_int32),
+        ("clock_mhz", C.c_double),
+    ]
+
+
 LG_MODEL_HEAT = 0
 LG_MODEL_C = 1
 LG_AMR_SUBCYCLING = 0
@@ -152,6 +163,7 @@ _SIGS = {
     "lg_snapshot_ring_stats": (C.c_int, [_p, _pi64, _pi64, _pi64]),
     "lg_cell_centers": (C.c_int, [C.c_int, _pi64, _pi64, _pd, _pd, _pd]),
     "lg_amr_tag_level_static": (C.c_int, [_p, C.c_int, C.c_int, _d, _pi64, _i64, _pi64]),
+    "lg_measure_compute_peaks": (C.c_int, [_p, C.POINTER(ComputePeaks)]),
 }
 
 for _name, (_res, _args) in _SIGS.items():

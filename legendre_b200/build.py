@@ -40,6 +40,7 @@ SOURCES = [
     ("lg_adjoint.cu", []),      # not bit-matched to anything: contraction allowed
     ("lg_ensemble.cu", ["-fmad=false"]),
     ("lg_observe.cu", ["-fmad=false"]),
+    ("lg_peaks.cu", []),        # microbenchmarks of explicit fma / integer chains
 ]
 
 

@@ -57,6 +57,15 @@ class CudaScheduler:
     def max_concurrency(self) -> int:
         return 1
 
+    def compute_peaks(self) -> dict:
+        """Measured FP64/FP32 FMA, integer multiply-add and ALU operation
+        rates of this device (operations per second over all SMs), the
+        compute-side roofline denominators of the step kernels."""
+        out = N.ComputePeaks()
+        N.check(N.lib.lg_measure_compute_peaks(self.handle, C.byref(out)), self.handle)
+        return {"dfma_per_s": out.dfma_per_s, "ffma_per_s": out.ffma_per_s, "imad_per_s": out.imad_per_s,
+                "alu_per_s": out.alu_per_s, "sms": out.sms, "clock_mhz": out.clock_mhz}
+
     def close(self) -> None:
         if self.handle:
             for destroy in reversed(self._owned):
