@@ -243,6 +243,13 @@ int lg_amr_sim_suggested_dt(const lg_amr_sim* sim, double* dt);
  * if one gives up the call returns LG_ERR_TIMEOUT and the state is invalid.
  * It takes precedence over LG_RUN_GRAPH. */
 int lg_amr_sim_step(lg_amr_sim* sim, double dt, int64_t nsteps, uint32_t flags);
+/* Polls (each of at least 128 ns) a grid barrier of the LG_RUN_PERSISTENT
+ * launch waits for the other CTAs before it gives up and the step returns
+ * LG_ERR_TIMEOUT (default 4,000,000: over a second).  No counterpart in the
+ * reference, whose Rayon scheduler has no device waits; a watchdog knob,
+ * and the way to make a barrier give up at once (0) to exercise the
+ * timeout path without any fault. */
+int lg_amr_sim_set_barrier_spin_limit(lg_amr_sim* sim, int64_t polls);
 /* (c) transfers on the current state: `restrict` (intergrid.rs:97-105) of
  * one field, finest level first; `fill_ghosts_mirror` of every level
  * (intergrid.rs:155-168); `GradientTagger::tag_level` (adapt.rs:78-103),

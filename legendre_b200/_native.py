@@ -141,6 +141,7 @@ _SIGS = {
     "lg_amr_sim_time": (C.c_int, [_p, _pd, _pi64]),
     "lg_amr_sim_suggested_dt": (C.c_int, [_p, _pd]),
     "lg_amr_sim_step": (C.c_int, [_p, _d, _i64, C.c_uint32]),
+    "lg_amr_sim_set_barrier_spin_limit": (C.c_int, [_p, _i64]),
     "lg_amr_restrict": (C.c_int, [_p, C.c_int]),
     "lg_amr_fill_ghosts": (C.c_int, [_p]),
     "lg_amr_tag_level": (C.c_int, [_p, C.c_int, C.c_int, _d, _pi64, _i64, _pi64]),

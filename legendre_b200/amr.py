@@ -266,6 +266,12 @@ class AmrSimulation:
             for o in self.observers:
                 o.observe(self.step_index(), self.time(), self.epoch, self.grid, self)
 
+    def set_barrier_spin_limit(self, polls: int) -> None:
+        """Polls a grid barrier of the persistent launch waits before it gives
+        up (the step then raises LegendreError with LG_ERR_TIMEOUT and the
+        state is invalid); 0 makes a waiting barrier give up at once."""
+        N.check(N.lib.lg_amr_sim_set_barrier_spin_limit(self.handle, int(polls)), self.scheduler.handle)
+
     # ------------------------------------------------------ transfers (c)
     def restrict(self, f) -> None:
         N.check(N.lib.lg_amr_restrict(self.handle, self._index(f)), self.scheduler.handle)

@@ -741,7 +741,7 @@ cudaError_t launch_adjoint(const T* x, const T* lam_in, T* lam_out, const void* 
         configured = true;
     }
     const int64_t items = (int64_t)g.ninst * g.tiles_x * g.tiles_y;
-    const unsigned grid = (unsigned)std::min<int64_t>(items, (int64_t)148 * 32);
+    const unsigned grid = (unsigned)std::min<int64_t>(items, (int64_t)lg::device_sm_count() * 32);
     kernel<<<grid, 256, smem, s>>>(x, lam_in, lam_out, static_cast<const AdjParams<T>*>(prm), g, (T)dt, acc);
     return cudaGetLastError();
 }
@@ -771,7 +771,7 @@ int adjoint_strips(const Geo& g) { return (g.N0 + SW - 1) / SW; }
 int adjoint_strip_rows(const Geo& g) {
     const int strips = adjoint_strips(g);
     int rows = std::max(1, g.N1);
-    while (rows > 16 && g.ninst * strips * ((g.N1 + rows - 1) / rows) < (int64_t)148 * 32) rows = (rows + 1) / 2;
+    while (rows > 16 && g.ninst * strips * ((g.N1 + rows - 1) / rows) < (int64_t)lg::device_sm_count() * 32) rows = (rows + 1) / 2;
     return rows;
 }
 
@@ -795,7 +795,7 @@ cudaError_t launch_loss_seed(int dtype, const void* x, const double* target, voi
     g.tiles_x = (g.N0 + TW - 1) / TW;
     g.tiles_y = (g.N1 + 8 - 1) / 8;
     const int64_t items = (int64_t)g.ninst * g.tiles_x * g.tiles_y;
-    const unsigned grid = (unsigned)std::min<int64_t>(items, (int64_t)148 * 32);
+    const unsigned grid = (unsigned)std::min<int64_t>(items, (int64_t)lg::device_sm_count() * 32);
     if (dtype == 0)
         loss_seed_kernel<double><<<grid, 256, 0, s>>>((const double*)x, target, (double*)lam, g, loss);
     else

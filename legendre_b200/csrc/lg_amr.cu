@@ -487,7 +487,7 @@ __global__ void __launch_bounds__(256) amr_persistent(PersistArgs a) {
 
 unsigned grid_for(int64_t n, int threads) {
     int64_t g = (n + threads - 1) / threads;
-    return (unsigned)std::max<int64_t>(1, std::min<int64_t>(g, 148 * 32));
+    return (unsigned)std::max<int64_t>(1, std::min<int64_t>(g, (int64_t)lg::device_sm_count() * 32));
 }
 
 template <class T>
@@ -553,6 +553,7 @@ struct lg_amr_sim {
     std::map<std::string, std::pair<void*, int>> phase_tabs;  // device table, phase count
     unsigned* d_bar = nullptr;
     int* d_err = nullptr;
+    long long barrier_spin_limit = 4000000;  // polls of >= 128 ns: well over a second
     int coop_grid[2] = {0, 0};  // per model kind (noise-free / noisy) once measured
     std::vector<double> host_old, host_new;  // regrid staging
     std::vector<TileShape> tile_shapes;      // per level
@@ -609,8 +610,8 @@ std::pair<int64_t, int64_t> level_range(const lg_amr_sim* s, int level) {
 // each face flux is shared down a warp's rows.  A sparse fine level is
 // latency-bound (its launch is one short wave): tiles of at most 8 rows with
 // one row per warp, the tallest that still gives two tiles per SM.
-constexpr int kSMs = 148;
 std::vector<TileShape> choose_tile_shapes(const lg::amr::Layout& g) {
+    const int kSMs = lg::device_sm_count();
     std::vector<TileShape> shapes(g.max_levels(), TileShape{lg::amr::kTile, 4});
     for (int l = 0; l < g.num_levels(); ++l) {
         int64_t cells = 0;
@@ -846,7 +847,7 @@ int launch_level(lg_amr_sim* s, int level, bool interp, double alpha, double dt,
     a.chain = chain;
     a.seed = s->seed;
     a.scale_amp = std::sqrt(dt) * s->mp.noise_amplitude;
-    const unsigned g = (unsigned)std::min<int64_t>(t1 - t0, kSMs * 16);
+    const unsigned g = (unsigned)std::min<int64_t>(t1 - t0, (int64_t)lg::device_sm_count() * 16);
     const int threads = tile_threads(s->tile_shapes[level]);
     cudaStream_t st = lg::abi_stream(s->ctx);
     if (s->model == LG_MODEL_C) {
@@ -1068,7 +1069,7 @@ int run_persistent(lg_amr_sim* s, double dt, int nsteps) {
     }
     a.bar = s->d_bar;
     a.err = s->d_err;
-    a.spin_limit = 4000000;  // polls of >= 128 ns: well over a second
+    a.spin_limit = s->barrier_spin_limit;
     int rc;
     if (s->model == LG_MODEL_C)
         rc = s->mp.noise_amplitude != 0.0 ? launch_persistent_kernel<LG_MODEL_C, true>(s, a)
@@ -1428,6 +1429,12 @@ int lg_amr_sim_suggested_dt(const lg_amr_sim* s, double* dt) {
     // Subcycling::suggested_dt: level 0; a global-dt scheme: the finest
     // level the ratios allow (integrators/mod.rs:218-223, subcycling.rs:54-61)
     *dt = stable_dt_at(s, s->integrator == LG_AMR_SUBCYCLING ? 0 : (int)s->layout.level_spacing.size() - 1);
+    return LG_OK;
+}
+
+int lg_amr_sim_set_barrier_spin_limit(lg_amr_sim* s, int64_t polls) {
+    if (!s || polls < 0) return fail(s, LG_ERR_INVALID, "the spin limit is a non-negative poll count");
+    s->barrier_spin_limit = (long long)polls;
     return LG_OK;
 }
 

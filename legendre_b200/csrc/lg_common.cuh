@@ -84,4 +84,17 @@ __device__ __forceinline__ float standard_normal_f32(uint64_t key) {
 // Wiener stream tag of driver index j: (1 << 32) | j (driver.rs:134-140).
 constexpr uint64_t kWienerStream0 = (1ull << 32) | 0ull;
 
+// Streaming multiprocessors of the current device, queried once per device
+// ordinal; the grid-sizing heuristics scale with it.
+inline int device_sm_count() {
+    static int cache[64] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0) dev = 0;
+    int v = dev < 64 ? cache[dev] : 0;
+    if (v > 0) return v;
+    if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || v <= 0) v = 1;
+    if (dev < 64) cache[dev] = v;
+    return v;
+}
+
 }  // namespace lg

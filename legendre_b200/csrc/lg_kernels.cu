@@ -444,7 +444,7 @@ cudaError_t launch_heat3d_pull(const double* in, double* out, const CartTopo& to
     const int64_t plane = (int64_t)(topo.n[0] + 2) * (topo.n[1] + 2) * sizeof(double);
     int zc = std::min(n2, 16);
     while (zc > 1 && (zc + 2) * plane > 96 * 1024) --zc;
-    while (zc > 4 && (int64_t)topo.nblocks * ((n2 + zc - 1) / zc) < 148 * 8) zc = (zc + 1) / 2;
+    while (zc > 4 && (int64_t)topo.nblocks * ((n2 + zc - 1) / zc) < (int64_t)lg::device_sm_count() * 8) zc = (zc + 1) / 2;
     const int64_t items = (int64_t)topo.nblocks * ((n2 + zc - 1) / zc);
     const unsigned grid = (unsigned)std::min<int64_t>(items, (int64_t)1 << 30);
     const size_t smem = (size_t)(zc + 2) * plane;

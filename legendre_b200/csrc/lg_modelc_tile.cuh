@@ -468,7 +468,7 @@ __global__ void __launch_bounds__(256, MINB)
 inline int strip_rows(const CartTopo& topo, int strips, int rows, int nb) {
     const int n1 = topo.n[1];
     if (rows <= 0) {
-        const int64_t want_units = (int64_t)148 * 48 * 2;
+        const int64_t want_units = (int64_t)device_sm_count() * 48 * 2;
         const int64_t per_chunk = (int64_t)topo.nblocks * strips;
         const int chunks =
             (int)std::max<int64_t>(1, std::min<int64_t>(n1, (want_units + per_chunk - 1) / per_chunk));

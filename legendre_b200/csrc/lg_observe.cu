@@ -24,6 +24,7 @@
 #include <vector>
 
 #include "../../include/legendre_b200.h"
+#include "lg_common.cuh"
 #include "lg_state_view.h"
 
 namespace {
@@ -370,7 +371,7 @@ int lg_state_field_sum(lg_state* st, int field, double* sum) {
         return lg::abi_fail(v.ctx, e == cudaErrorMemoryAllocation ? LG_ERR_NOMEM : LG_ERR_CUDA,
                             std::string("field sum: ") + cudaGetErrorString(e));
     }
-    const unsigned grid = (unsigned)std::min<int64_t>(v.nblocks, 148 * 8);
+    const unsigned grid = (unsigned)std::min<int64_t>(v.nblocks, (int64_t)lg::device_sm_count() * 8);
     if (v.dtype == LG_F64)
         field_sum_kernel<double><<<grid, kSumThreads, 0, s>>>(static_cast<const double*>(v.arena), d, a);
     else

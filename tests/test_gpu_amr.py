@@ -153,3 +153,26 @@ def test_adaptive_model_c_three_levels_with_noise(sched, orc, mode):
     ref.step(dt, 12)
     assert dev.num_levels == ref.num_levels == 3
     same_state(dev, ref, 2, exact=False)
+
+
+def test_persistent_barrier_timeout_returns_an_error_and_the_context_stays_usable(sched, orc):
+    """The one bounded device wait: a grid barrier of the persistent launch
+    told to give up at its first poll returns LG_ERR_TIMEOUT (no fault, no
+    hang), and a fresh simulation on the same context then steps to the
+    oracle's bits."""
+    dev, ref0 = make_pair(sched, orc, [48, 48], [24, 24], 0.4, [2], [], model="modelc", integrator="subcycling",
+                          seed=7, policy=MC_POLICY)
+    set_both(dev, ref0, 0, _seed)
+    set_both(dev, ref0, 1, lambda x, y: np.full_like(x, -0.7))
+    dt = dev.stable_dt()
+    dev.set_barrier_spin_limit(0)
+    with pytest.raises(L.LegendreError) as err:
+        dev.run(dt, 4, persistent=True)
+    assert err.value.status == L._native.LG_ERR_TIMEOUT
+    dev2, ref = make_pair(sched, orc, [48, 48], [24, 24], 0.4, [2], [], model="modelc", integrator="subcycling",
+                          seed=7, policy=MC_POLICY)
+    set_both(dev2, ref, 0, _seed)
+    set_both(dev2, ref, 1, lambda x, y: np.full_like(x, -0.7))
+    dev2.run(dt, 12, persistent=True)
+    ref.step(dt, 12)
+    same_state(dev2, ref, 2)
