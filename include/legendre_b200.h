@@ -320,6 +320,18 @@ int lg_ensemble_run(lg_ensemble* e, double dt, int64_t nsteps, uint32_t flags);
  * x_T.  Parameter gradients accumulate in FP64 (FP32 ensembles included). */
 int lg_ensemble_value_and_grad(lg_ensemble* e, double dt, int64_t nsteps, int64_t ckpt_every, const double* target,
                                double* loss, double* grad_params, double* grad_phi0, double* grad_u0);
+/* The backward API of one Simulation (north of `Simulation::step`,
+ * simulation.rs:255-290; the reference has no adjoint): the same
+ * differentiation for a 2-D zero-flux Model C state of phi and u (ghost 1)
+ * stepped by Euler-Maruyama with `p` and Wiener `seed` from the state's
+ * current time.  target, grad_phi0 and grad_u0 are row-major over the whole
+ * grid (x fastest, cells[0] * cells[1] values); loss[0] and grad_params[0..3]
+ * = dL/d(lambda, D, eps4, Delta), Delta shifting the initial u by -Delta on
+ * every cell.  The state is left at x_T with its time advanced, as after
+ * lg_modelc_em_run of nsteps.  LG_ERR_STATE for other states. */
+int lg_modelc_value_and_grad(lg_state* state, const lg_modelc_params* p, double dt, uint64_t seed, int64_t nsteps,
+                             int64_t ckpt_every, const double* target, double* loss, double* grad_params,
+                             double* grad_phi0, double* grad_u0);
 /* The form of the step adjoint value_and_grad runs: LG_ADJOINT_STRIP (warp
  * strips walking up the rows; the default) or LG_ADJOINT_TILE (shared-memory
  * tiles with a two-cell halo).  Both give the same gradients up to rounding. */

@@ -155,6 +155,8 @@ _SIGS = {
     "lg_ensemble_run": (C.c_int, [_p, _d, _i64, C.c_uint32]),
     "lg_ensemble_value_and_grad": (C.c_int, [_p, _d, _i64, _i64, _pd, _pd, _pd, _pd, _pd]),
     "lg_ensemble_set_adjoint_kernel": (C.c_int, [_p, C.c_int]),
+    "lg_modelc_value_and_grad": (C.c_int, [_p, C.POINTER(ModelCParams), _d, _u64, _i64, _i64, _pd, _pd, _pd, _pd,
+                                           _pd]),
     "lg_ensemble_set_resident_budget": (C.c_int, [_p, C.c_uint64]),
     "lg_snapshot_ring_create": (C.c_int, [_p, C.POINTER(C.c_int), C.c_int, C.c_int, C.POINTER(_p)]),
     "lg_snapshot_ring_destroy": (C.c_int, [_p]),

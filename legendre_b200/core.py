@@ -302,6 +302,38 @@ class Simulation:
             for o in self.observers:
                 o.observe(step, self.time(), 0, self.grid, self.state)
 
+    def value_and_grad(self, dt: float, nsteps: int, ckpt_every: int, target, cell_grads: bool = True) -> dict:
+        """The backward API of this Simulation: from its current state, runs
+        ``nsteps`` Euler-Maruyama steps of Model C (the trajectory ``run``
+        gives), evaluates L = sum over the cells of (phi_T - target)^2 and
+        returns L with dL/d(lambda, D, eps4, Delta) and, with ``cell_grads``,
+        dL/dphi_0 and dL/du_0 per cell -- the hand-written adjoint of the fused
+        step with a checkpoint every ``ckpt_every`` steps (the noise replays
+        from its keys).  Delta shifts the initial u by -Delta on every cell.
+        ``target`` and the cell gradients are (cells_y, cells_x) arrays.  The
+        state is left at the final step, as after ``run``.  2-D zero-flux
+        Model C grids, axis-aligned, only."""
+        import numpy as np
+
+        from .integrators import EulerMaruyama
+        from .physics import ModelC
+
+        if not isinstance(self.model, ModelC) or not isinstance(self.integrator, EulerMaruyama):
+            raise TypeError("value_and_grad differentiates Model C stepped by EulerMaruyama")
+        shape = (self.grid.cells[1], self.grid.cells[0])
+        tgt = np.ascontiguousarray(np.broadcast_to(target, shape), dtype=np.float64)
+        loss, gp = np.empty(1), np.empty(4)
+        dphi = np.empty(shape) if cell_grads else None
+        du = np.empty(shape) if cell_grads else None
+        ptr = lambda a: a.ctypes.data_as(C.POINTER(C.c_double)) if a is not None else None
+        p = self.model.params(flux_tol=self.disc.tol)
+        N.check(N.lib.lg_modelc_value_and_grad(self.state.handle, C.byref(p), float(dt),
+                                               int(self.integrator.seed) & ((1 << 64) - 1), int(nsteps),
+                                               int(ckpt_every), ptr(tgt), ptr(loss), ptr(gp), ptr(dphi), ptr(du)),
+                self.scheduler.handle)
+        return {"loss": float(loss[0]), "lambda": float(gp[0]), "d_thermal": float(gp[1]), "eps4": float(gp[2]),
+                "delta": float(gp[3]), "phi0": dphi, "u0": du}
+
     def autotune(self, dt: float, trial_steps: int = 20):
         """Pick the fastest Model C step variant for this grid and precision by
         timing every candidate from a copy of the state (the state, its time

@@ -228,7 +228,10 @@ int abi_state_view(const lg_state* st, StateView* v) {
     for (int d = 0; d < 3; ++d) {
         v->block[d] = g->block[d];
         v->nb[d] = g->nb[d];
+        v->spacing[d] = g->spacing[d];
+        v->periodic[d] = g->periodic[d];
     }
+    v->arena_rw = st->arena[st->cur];
     return LG_OK;
 }
 cudaStream_t abi_stream(lg_ctx* ctx) { return ctx->stream; }

@@ -23,13 +23,7 @@
 #include "../../include/legendre_b200.h"
 #include "lg_adjoint.h"
 #include "lg_kernels.h"
-
-namespace lg {
-int abi_fail(lg_ctx* ctx, int code, const std::string& msg);
-cudaStream_t abi_stream(lg_ctx* ctx);
-int abi_device(lg_ctx* ctx);
-void abi_count_launch(lg_ctx* ctx, int64_t n);
-}  // namespace lg
+#include "lg_state_view.h"
 
 struct lg_ensemble {
     lg_ctx* ctx = nullptr;
@@ -578,6 +572,56 @@ int lg_ensemble_set_adjoint_kernel(lg_ensemble* e, int kernel) {
         return efail(e, LG_ERR_INVALID, "unknown adjoint kernel");
     e->adj_kernel = kernel == LG_ADJOINT_STRIP ? lg::adj::kAdjointStrip : lg::adj::kAdjointTile;
     return LG_OK;
+}
+
+// The backward API of one Simulation: its state (a 2-D zero-flux Model C
+// state of phi and u, ghost 1) is exactly the block-major arena of a
+// one-instance ensemble -- same slabs, same order, same stride -- so the
+// state moves into such an ensemble by one device copy, goes through
+// value_and_grad, and x_T moves back the same way.  The instance's noise
+// keys are the Simulation's (its seed, its time, the block ids), so the
+// forward pass inside is the trajectory lg_modelc_em_run produces.
+int lg_modelc_value_and_grad(lg_state* state, const lg_modelc_params* p, double dt, uint64_t seed, int64_t nsteps,
+                             int64_t ckpt_every, const double* target, double* loss, double* grad_params,
+                             double* grad_phi0, double* grad_u0) {
+    lg::StateView v{};
+    if (!state || !p || lg::abi_state_view(state, &v) != LG_OK) return LG_ERR_INVALID;
+    if (v.D != 2 || v.nfields != 2 || v.ghosts[0] != 1 || v.ghosts[1] != 1)
+        return lg::abi_fail(v.ctx, LG_ERR_STATE, "value_and_grad needs a 2-D Model C state of phi and u (ghost 1)");
+    if (v.periodic[0] || v.periodic[1])
+        return lg::abi_fail(v.ctx, LG_ERR_STATE, "value_and_grad supports zero-flux (mirror) boundaries only");
+    double t = 0.0;
+    int64_t step = 0;
+    lg_state_get_time(state, &t, &step);
+    const int64_t cells[2] = {v.block[0] * v.nb[0], v.block[1] * v.nb[1]};
+    const int64_t block[2] = {v.block[0], v.block[1]};
+    const double spacing[2] = {v.spacing[0], v.spacing[1]};
+    const double eps4 = p->eps4;
+    lg_ensemble* e = nullptr;
+    int rc = lg_ensemble_create(v.ctx, cells, block, spacing, 1, p, &eps4, &seed, v.dtype, &e);
+    if (rc != LG_OK) return rc;
+    cudaStream_t st = lg::abi_stream(v.ctx);
+    const size_t bytes = (size_t)state_bytes(e);
+    if (e->slab_stride != v.slab_stride || bytes != (size_t)v.nblocks * 2 * v.slab_stride * v.esize) {
+        lg_ensemble_destroy(e);
+        return lg::abi_fail(v.ctx, LG_ERR_STATE, "state layout differs from the ensemble's");
+    }
+    cudaError_t ce = cudaMemcpyAsync(e->state[e->cur], v.arena, bytes, cudaMemcpyDeviceToDevice, st);
+    if (ce == cudaSuccess) rc = fill_ghosts(e, e->state[e->cur]);
+    else rc = lg::abi_fail(v.ctx, LG_ERR_CUDA, std::string("state copy: ") + cudaGetErrorString(ce));
+    if (rc == LG_OK) {
+        e->t = t;
+        e->step_index = step;
+        rc = lg_ensemble_value_and_grad(e, dt, nsteps, ckpt_every, target, loss, grad_params, grad_phi0, grad_u0);
+    }
+    if (rc == LG_OK) {
+        ce = cudaMemcpyAsync(v.arena_rw, e->state[e->cur], bytes, cudaMemcpyDeviceToDevice, st);
+        if (ce == cudaSuccess) ce = cudaStreamSynchronize(st);
+        if (ce != cudaSuccess) rc = lg::abi_fail(v.ctx, LG_ERR_CUDA, std::string("state copy: ") + cudaGetErrorString(ce));
+        else lg_state_set_time(state, e->t, e->step_index);
+    }
+    lg_ensemble_destroy(e);
+    return rc;
 }
 
 }  // extern "C"

@@ -19,6 +19,9 @@ struct StateView {
     int64_t slab_stride;  // elements between consecutive slabs (block b, field f at (b * nfields + f) * slab_stride)
     int64_t nblocks;
     int64_t block[3], nb[3];  // cells per block and blocks per dimension (1 past D)
+    double spacing[3];
+    int periodic[3];
+    void* arena_rw;       // the same arena, writable (for entry points that replace the state)
 };
 
 int abi_state_view(const lg_state* st, StateView* v);

@@ -63,3 +63,72 @@ def test_no_flags_no_boxes():
 def test_invalid_parameters_are_refused(eff, mw):
     with pytest.raises(LegendreError):
         cluster([(0, 0)], ClusterParams(eff, mw))
+
+
+# ---- the reference's own assertions (amr/cluster.rs:306-431), checked on the
+# product's clustering directly, not through the oracle
+def _cover_disjoint(flags, boxes):
+    """cluster.rs:306-319: every flag in exactly one box; boxes pairwise
+    disjoint (half-open)."""
+    for f in flags:
+        n = sum(1 for b in boxes if b[0][0] <= f[0] < b[1][0] and b[0][1] <= f[1] < b[1][1])
+        assert n == 1, f"flag {f} covered by {n} boxes: {boxes}"
+    for i, a in enumerate(boxes):
+        for b in boxes[i + 1:]:
+            overlap = all(max(a[0][d], b[0][d]) < min(a[1][d], b[1][d]) for d in range(2))
+            assert not overlap, f"boxes overlap: {a} {b}"
+
+
+def _cells(b):
+    return (b[1][0] - b[0][0]) * (b[1][1] - b[0][1])
+
+
+def _flags_in(flags, b):
+    return sum(1 for f in flags if b[0][0] <= f[0] < b[1][0] and b[0][1] <= f[1] < b[1][1])
+
+
+def test_reference_dense_rectangle_is_one_full_box():
+    # cluster.rs:320-331
+    flags = art(["xxxx", "xxxx", "xxxx"])
+    boxes = boxes_of(flags, 0.8, 4)
+    assert boxes == [((0, 0), (4, 3))]
+    _cover_disjoint(flags, boxes)
+
+
+def test_reference_islands_split_at_holes():
+    # cluster.rs:333-346: two islands, each boxed tightly
+    flags = art(["xx....xxx", "xx....xxx", "......xxx"])
+    boxes = boxes_of(flags, 0.8, 4)
+    assert len(boxes) == 2, boxes
+    _cover_disjoint(flags, boxes)
+    assert sum(_cells(b) for b in boxes) == len(flags)
+
+
+def test_reference_l_shape_splits_at_inflection():
+    # cluster.rs:348-374: two boxes cover the L exactly
+    flags = art(["xx......"] * 4 + ["xxxxxxxx"] * 2)
+    boxes = boxes_of(flags, 0.95, 2)
+    _cover_disjoint(flags, boxes)
+    assert sum(_cells(b) for b in boxes) == len(flags), boxes
+    assert len(boxes) == 2, boxes
+
+
+def test_reference_v_shape_is_covered_efficiently():
+    # cluster.rs:376-395
+    flags = art(["x.....x", "x.....x", ".x...x.", ".x...x.", "..x.x..", "..xxx.."])
+    boxes = boxes_of(flags, 0.7, 1)
+    _cover_disjoint(flags, boxes)
+    assert len(flags) / sum(_cells(b) for b in boxes) >= 0.7, boxes
+
+
+def test_reference_diagonal_stripe_bisects_past_the_anomaly():
+    # cluster.rs:397-431: bisection makes progress on a 45-degree stripe;
+    # with a width floor every box keeps at least half its cells flagged
+    flags = [(i, i) for i in range(8)]
+    boxes = boxes_of(flags, 0.8, 1)
+    _cover_disjoint(flags, boxes)
+    assert len(flags) / sum(_cells(b) for b in boxes) >= 0.8, boxes
+    boxes = boxes_of(flags, 0.8, 2)
+    _cover_disjoint(flags, boxes)
+    for b in boxes:
+        assert _flags_in(flags, b) / _cells(b) >= 0.5, (b, boxes)

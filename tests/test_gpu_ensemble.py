@@ -242,3 +242,59 @@ def test_resident_tail_gives_the_same_bits(sched, dtype):
         for k in ("loss", "lambda", "d_thermal", "eps4", "delta", "phi0", "u0", "phi_T"):
             assert np.array_equal(g[k], out[0][k]), k
         assert g["time"] == out[0]["time"]
+
+
+# ------------------------------------------------- Simulation backward API --
+def _sim(sched, eps4=EPS4[0], lam=LAM, d=D, seed=SEEDS[0], tol=0.0, phi0=None, delta=DELTA[0], dtype="f64"):
+    grid = L.CartesianGrid([N_, N_], [BLOCK, BLOCK], [0.0, 0.0], [H, H])
+    model = L.ModelC(eps4, lam, NOISE)
+    model.d_thermal = d
+    model.anisotropy_tol = tol
+    sim = L.Simulation(grid, L.FiniteVolume(tol=tol), model, L.EulerMaruyama(seed), sched, L.CudaAllocator(dtype))
+    sim.state.upload("phi", to_blocks(seeds_field(1, N_)[0] if phi0 is None else phi0, BLOCK))
+    sim.state.upload("u", to_blocks(np.full((N_, N_), -delta), BLOCK))
+    return sim
+
+
+def test_simulation_value_and_grad_equals_the_one_instance_ensemble(sched):
+    """Simulation.value_and_grad gives the one-instance ensemble's loss and
+    gradients bit for bit, and leaves the state where run() leaves it."""
+    target = _losses(sched, 0.0, eps4=[e + 0.01 for e in EPS4], delta=[d + 0.03 for d in DELTA])[0]
+    sim = _sim(sched)
+    g = sim.value_and_grad(DT, STEPS, CKPT, target)
+    ens = make(sched, N_, BLOCK, EPS4[:1], SEEDS[:1], NOISE, tol=0.0)
+    ens.set("phi", seeds_field(1, N_))
+    ens.set("u", np.full((1, N_, N_), -DELTA[0]))
+    ge = ens.value_and_grad(DT, STEPS, CKPT, target)
+    ens._destroy()
+    assert g["loss"] == ge["loss"][0]
+    for k in ("lambda", "d_thermal", "eps4", "delta"):
+        assert g[k] == ge[k][0], k
+    assert np.array_equal(g["phi0"], ge["phi0"][0]) and np.array_equal(g["u0"], ge["u0"][0])
+    fwd = _sim(sched)
+    fwd.run(DT, STEPS)
+    assert np.array_equal(sim.state.interior("phi"), fwd.state.interior("phi"))
+    assert np.array_equal(sim.state.interior("u"), fwd.state.interior("u"))
+    assert sim.time() == fwd.time() and sim.step_index() == fwd.step_index() == STEPS
+
+
+def test_simulation_value_and_grad_matches_finite_differences(sched):
+    """dL/dlambda and dL/dphi_0 of one Simulation against central differences
+    of its own forward runs (continuous form, h = 1e-4), to 1e-6."""
+    target = _losses(sched, 0.0, eps4=[e + 0.01 for e in EPS4], delta=[d + 0.03 for d in DELTA])[0]
+    g = _sim(sched).value_and_grad(DT, STEPS, CKPT, target)
+
+    def loss(**kw):
+        s = _sim(sched, **kw)
+        s.run(DT, STEPS)
+        return ((from_blocks(s.state.interior("phi"), N_, BLOCK) - target) ** 2).sum()
+
+    h = 1e-4
+    _close(g["lambda"], (loss(lam=LAM + h) - loss(lam=LAM - h)) / (2 * h))
+    _close(g["delta"], (loss(delta=DELTA[0] + h) - loss(delta=DELTA[0] - h)) / (2 * h))
+    base = seeds_field(1, N_)[0]
+    y, x = 16, 9
+    pp, pm = base.copy(), base.copy()
+    pp[y, x] += h
+    pm[y, x] -= h
+    _close(g["phi0"][y, x], (loss(phi0=pp) - loss(phi0=pm)) / (2 * h))
