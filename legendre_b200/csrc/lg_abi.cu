@@ -24,6 +24,7 @@ struct lg_ctx {
     std::string err;
     int64_t launches = 0;
     std::map<std::string, int> tuned;  // Model C variant chosen by lg_modelc_autotune, per shape
+    int* d_flag = nullptr;  // set by a kernel whose bounded device wait gave up (allocated on first use)
 };
 
 struct lg_grid {
@@ -234,6 +235,16 @@ int abi_state_view(const lg_state* st, StateView* v) {
     v->arena_rw = st->arena[st->cur];
     return LG_OK;
 }
+int* abi_device_flag(lg_ctx* ctx) {
+    if (!ctx->d_flag) {
+        if (cudaMalloc(&ctx->d_flag, sizeof(int)) != cudaSuccess) {
+            ctx->d_flag = nullptr;
+            return nullptr;
+        }
+        if (cudaMemsetAsync(ctx->d_flag, 0, sizeof(int), ctx->stream) != cudaSuccess) return nullptr;
+    }
+    return ctx->d_flag;
+}
 cudaStream_t abi_stream(lg_ctx* ctx) { return ctx->stream; }
 int abi_device(lg_ctx* ctx) { return ctx->device; }
 void abi_count_launch(lg_ctx* ctx, int64_t n) { ctx->launches += n; }
@@ -270,6 +281,7 @@ int lg_ctx_destroy(lg_ctx* ctx) {
     if (!ctx) return LG_ERR_INVALID;
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
+    if (ctx->d_flag) cudaFree(ctx->d_flag);
     if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
     return LG_OK;
@@ -279,12 +291,22 @@ const char* lg_last_error(const lg_ctx* ctx) { return ctx ? ctx->err.c_str() : "
 
 int64_t lg_ctx_kernel_launches(const lg_ctx* ctx) { return ctx ? ctx->launches : -1; }
 
+// after the stream has drained: did a kernel's bounded device wait give up?
+static int check_device_flag(lg_ctx* ctx) {
+    if (!ctx->d_flag) return LG_OK;
+    int v = 0;
+    LG_CUDA(ctx, cudaMemcpy(&v, ctx->d_flag, sizeof v, cudaMemcpyDeviceToHost));
+    if (v == 0) return LG_OK;
+    LG_CUDA(ctx, cudaMemset(ctx->d_flag, 0, sizeof(int)));
+    return fail(ctx, LG_ERR_DEVICE, "a kernel's bounded wait for its tile copies gave up; results are invalid");
+}
+
 int lg_sync(lg_ctx* ctx, int64_t timeout_ms) {
     if (!ctx) return LG_ERR_INVALID;
     auto t0 = std::chrono::steady_clock::now();
     for (;;) {
         cudaError_t e = cudaStreamQuery(ctx->stream);
-        if (e == cudaSuccess) return LG_OK;
+        if (e == cudaSuccess) return check_device_flag(ctx);
         if (e != cudaErrorNotReady) return cuda_fail(ctx, e, "stream");
         if (timeout_ms >= 0) {
             auto ms = std::chrono::duration_cast<std::chrono::milliseconds>(std::chrono::steady_clock::now() - t0);
@@ -453,7 +475,7 @@ static int field_copy(lg_state* st, int field, void* host, int64_t nelem, bool u
                                        ctx->stream));
     }
     LG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-    return LG_OK;
+    return upload ? LG_OK : check_device_flag(ctx);
 }
 
 int lg_state_upload_field(lg_state* st, int field, const void* host, int64_t nelem) {
@@ -521,12 +543,16 @@ int lg_heat_fe_run(lg_state* st, int field, double kappa, double dt, int64_t nst
     snprintf(key, sizeof key, "heat|f=%d|k=%a|dt=%a", field, kappa, dt);
     // 3-D: halos pulled from the neighbour blocks, ghosts filled once at the
     // end; otherwise the push kernel, which keeps the ghosts valid each step
+    // (even block widths: the tiles staged by tensor copies; odd: by cp.async)
     const bool pull = lg::heat3d_pull_supported(topo, L);
+    int* dflag = nullptr;
+    const bool tma = pull && lg::heat3d_tma_supported(topo, L) && (dflag = lg::abi_device_flag(ctx)) != nullptr;
     auto step = [&]() -> int {
         const double* in = static_cast<const double*>(st->arena[st->cur]);
         double* out = static_cast<double*>(st->arena[st->cur ^ 1]);
-        cudaError_t e = pull ? lg::launch_heat3d_pull(in, out, topo, L, field, kappa, dt, inv_h2, ctx->stream)
-                             : lg::launch_heat_step(in, out, topo, L, field, kappa, dt, inv_h2, ctx->stream);
+        cudaError_t e = tma    ? lg::launch_heat3d_tma(in, out, topo, L, field, kappa, dt, inv_h2, dflag, ctx->stream)
+                        : pull ? lg::launch_heat3d_pull(in, out, topo, L, field, kappa, dt, inv_h2, ctx->stream)
+                               : lg::launch_heat_step(in, out, topo, L, field, kappa, dt, inv_h2, ctx->stream);
         ctx->launches++;
         if (e != cudaSuccess) return cuda_fail(ctx, e, "heat step launch");
         st->cur ^= 1;

@@ -9,6 +9,9 @@
 #include <cmath>
 #include <cstdio>
 
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
 #include "lg_common.cuh"
 #include "lg_kernels.h"
 #include "lg_modelc_ops.cuh"
@@ -310,6 +313,167 @@ __global__ void __launch_bounds__(1024) heat3d_pull_kernel(const double* __restr
     }
 }
 
+// ------------------------------------------------- TMA-staged 3-D heat step
+// shared-memory address of a generic pointer into this CTA's shared memory
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
+    unsigned ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// wait for phase `parity` of the barrier, at most `limit` polls
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned parity, long long limit) {
+    for (long long it = 0; it < limit; ++it)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+// one tiled tensor copy global -> shared of box `map` at (c0, c1, c2, c3),
+// completing on `bar` (no cluster multicast: the map covers this GPU's
+// memory only)
+__device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* map, int c0, int c1, int c2, int c3,
+                                            uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], "
+        "[%6];" ::"r"(smem_u32(dst)),
+        "l"((uint64_t)map), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_u32(bar))
+        : "memory");
+}
+
+// Tensor maps over one field of a 3-D state arena, all on the same 4-D
+// tensor (x = slab column, y = slab row, z = slab plane, w = block), whose
+// slabs keep their ghost ring: interior cell (i, j, k) of block b is at
+// (i + 1, j + 1, k + 1, b).  Boxes: `main` the zc planes of a block's
+// interior rows (every column of each row, the two ghost columns included:
+// a row's interior starts 8 bytes in, and a box's first column must sit on a
+// 16-byte boundary); `plane` one such plane (the z halos); `row` one row
+// over zc planes (the y halos); `col` two columns over the interior rows of
+// zc planes (the x halos; the wanted column is one of the two).
+struct HeatMaps {
+    CUtensorMap main, plane, row, col;
+};
+
+// 3-D heat step with every tile staged by the tensor-memory accelerator.
+// One CTA owns a z-range of up to zc planes of one block, threads on the
+// (x, y) plane.  Thread (0, 0) issues seven tensor copies onto one mbarrier:
+// the range's interior rows, the z halo planes below and above, the y halo
+// rows and the x halo columns of every plane of the range -- the halos from
+// the face-neighbour blocks' interiors or, at a mirror boundary, the block's
+// own edge cells (the zero-flux ghost, boundary.rs:63-80) -- so no ghost
+// entry is read or written per step.  The wait for them is bounded: if it
+// gives up, the CTA sets the context's error word, waits once more (bounded)
+// for its copies to land and skips its update.  Each thread then walks its
+// column through the range, reading from shared memory; arithmetic and
+// operand order are heat_step_kernel's, so results are bit-identical.
+// Stores are plain coalesced writes (an interior row starts 8 bytes into
+// the slab row, which a tensor store cannot start on).
+__global__ void __launch_bounds__(1024) heat3d_tma_kernel(const __grid_constant__ HeatMaps maps, double* __restrict__ out,
+                                                          CartTopo topo, SlabLayout L, int field, double kappa,
+                                                          double dt, double ih0, double ih1, double ih2, int zc,
+                                                          int* err, long long spin_limit) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    const int n0 = topo.n[0], n1 = topo.n[1], n2 = topo.n[2];
+    const int W = n0 + 2;  // doubles per staged row
+    // stage regions, each 128-byte aligned: S[zc][n1][W], ZL/ZH[n1][W],
+    // YL/YH[zc][W], XL/XH[zc][n1][2], then the mbarrier
+    auto up128 = [](size_t b) { return (b + 127) & ~size_t(127); };
+    const size_t bS = up128((size_t)zc * n1 * W * 8), bZ = up128((size_t)n1 * W * 8), bY = up128((size_t)zc * W * 8),
+                 bX = up128((size_t)zc * n1 * 2 * 8);
+    double* S = reinterpret_cast<double*>(smem_raw);
+    double* ZL = reinterpret_cast<double*>(smem_raw + bS);
+    double* ZH = reinterpret_cast<double*>(smem_raw + bS + bZ);
+    double* YL = reinterpret_cast<double*>(smem_raw + bS + 2 * bZ);
+    double* YH = reinterpret_cast<double*>(smem_raw + bS + 2 * bZ + bY);
+    double* XL = reinterpret_cast<double*>(smem_raw + bS + 2 * bZ + 2 * bY);
+    double* XH = reinterpret_cast<double*>(smem_raw + bS + 2 * bZ + 2 * bY + bX);
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smem_raw + bS + 2 * bZ + 2 * bY + 2 * bX);
+    const unsigned tx_bytes =
+        (unsigned)(((size_t)zc * n1 * W + 2 * (size_t)n1 * W + 2 * (size_t)zc * W + 2 * (size_t)zc * n1 * 2) * 8);
+    const int x = threadIdx.x, y = threadIdx.y;
+    const bool leader = x == 0 && y == 0;
+    if (leader) {
+        mbar_init(bar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    // programmatic dependent launch: the next step may launch now; this one
+    // waits for the previous step's grid (and its writes) before staging
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    const int64_t sy = L.gdim[0], sz = (int64_t)L.gdim[0] * L.gdim[1];
+    const int nchunks = (n2 + zc - 1) / zc;
+    const int64_t items = (int64_t)topo.nblocks * nchunks;
+    unsigned parity = 0;
+    for (int64_t item = blockIdx.x; item < items; item += gridDim.x) {
+        const int b = (int)(item / nchunks);
+        const int z0 = (int)(item - (int64_t)b * nchunks) * zc, nz = min(zc, n2 - z0);
+        const int* nb = topo.nbr + b * 6;
+        if (leader) {
+            // source block and slab coordinate of each halo
+            const int bxl = nb[0] >= 0 ? nb[0] : b, cxl = nb[0] >= 0 ? n0 : 1;  // left: the neighbour's last column
+            const int bxh = nb[1] >= 0 ? nb[1] : b, cxh = nb[1] >= 0 ? 1 : n0;  // right: its first column
+            const int byl = nb[2] >= 0 ? nb[2] : b, ryl = nb[2] >= 0 ? n1 : 1;
+            const int byh = nb[3] >= 0 ? nb[3] : b, ryh = nb[3] >= 0 ? 1 : n1;
+            int bzl = b, pzl = z0;                 // plane z0 - 1 of this block
+            if (z0 == 0) { bzl = nb[4] >= 0 ? nb[4] : b; pzl = nb[4] >= 0 ? n2 : 1; }
+            int bzh = b, pzh = z0 + nz + 1;        // plane z0 + nz of this block
+            if (z0 + nz == n2) { bzh = nb[5] >= 0 ? nb[5] : b; pzh = nb[5] >= 0 ? 1 : n2; }
+            mbar_arrive_expect_tx(bar, tx_bytes);
+            tma_load_4d(S, &maps.main, 0, 1, z0 + 1, b, bar);
+            tma_load_4d(ZL, &maps.plane, 0, 1, pzl, bzl, bar);
+            tma_load_4d(ZH, &maps.plane, 0, 1, pzh, bzh, bar);
+            tma_load_4d(YL, &maps.row, 0, ryl, z0 + 1, byl, bar);
+            tma_load_4d(YH, &maps.row, 0, ryh, z0 + 1, byh, bar);
+            tma_load_4d(XL, &maps.col, cxl & ~1, 1, z0 + 1, bxl, bar);
+            tma_load_4d(XH, &maps.col, cxh & ~1, 1, z0 + 1, bxh, bar);
+        }
+        bool ok = mbar_wait_bounded(bar, parity, spin_limit);
+        if (!ok) {
+            if (leader) atomicExch(err, 1);
+            mbar_wait_bounded(bar, parity, spin_limit);  // let the copies land before the stage is reused
+        }
+        parity ^= 1u;
+        if (ok) {
+            // slab columns the x halos came from: left = neighbour's n0 (or
+            // own 1), right = neighbour's 1 (or own n0); index within the pair
+            const int il = (nb[0] >= 0 ? n0 : 1) & 1, ih = (nb[1] >= 0 ? 1 : n0) & 1;
+            double* o = out + slab_base(L, b, field);
+            for (int r = 0; r < nz; ++r) {
+                const double* q = S + ((size_t)r * n1 + y) * W + (x + 1);
+                const double uc = q[0];
+                const double xm = x == 0 ? XL[((size_t)r * n1 + y) * 2 + il] : q[-1];
+                const double xp = x == n0 - 1 ? XH[((size_t)r * n1 + y) * 2 + ih] : q[1];
+                const double ym = y == 0 ? YL[(size_t)r * W + x + 1] : q[-W];
+                const double yp = y == n1 - 1 ? YH[(size_t)r * W + x + 1] : q[W];
+                const double zm = r == 0 ? ZL[(size_t)y * W + x + 1] : q[-(int64_t)n1 * W];
+                const double zp = r == nz - 1 ? ZH[(size_t)y * W + x + 1] : q[(int64_t)n1 * W];
+                double acc = 0.0;
+                acc += ((xp - (uc + uc)) + xm) * ih0;
+                acc += ((yp - (uc + uc)) + ym) * ih1;
+                acc += ((zp - (uc + uc)) + zm) * ih2;
+                const double k = acc * kappa;
+                o[(int64_t)(x + 1) + (y + 1) * sy + (z0 + r + 1) * sz] = uc + dt * k;
+            }
+        }
+        // every thread is done with the stage before the next item's copies
+        // (async proxy) overwrite it
+        __syncthreads();
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+}
+
 // Reference-order Model C step, one thread per interior cell: the flux
 // kernel (finite_volume.rs:258-283), the local terms (phasefield.rs:395-404),
 // the u Laplacian and coupling (phasefield.rs:412-421), the Time driver
@@ -467,6 +631,94 @@ cudaError_t launch_heat3d_pull(const double* in, double* out, const CartTopo& to
     cfg.numAttrs = 1;
     return cudaLaunchKernelEx(&cfg, heat3d_pull_kernel, in, out, topo, L, field, kappa, dt, inv_h2[0], inv_h2[1],
                               inv_h2[2], zc);
+}
+
+// ---- TMA heat launcher: tensor maps are encoded on the host per launch
+// (cheap; a captured graph keeps the parameters it was captured with)
+namespace {
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        tried = true;
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }
+    return fn;
+}
+
+bool encode_heat_map(CUtensorMap* m, const double* base, const CartTopo& topo, const SlabLayout& L, uint32_t bx,
+                     uint32_t by, uint32_t bz) {
+    auto enc = tensor_map_encoder();
+    if (!enc) return false;
+    const cuuint64_t dims[4] = {(cuuint64_t)topo.n[0] + 2, (cuuint64_t)topo.n[1] + 2, (cuuint64_t)topo.n[2] + 2,
+                                (cuuint64_t)topo.nblocks};
+    const cuuint64_t strides[3] = {(cuuint64_t)(topo.n[0] + 2) * 8, (cuuint64_t)(topo.n[0] + 2) * (topo.n[1] + 2) * 8,
+                                   (cuuint64_t)L.nfields * L.slab_stride * 8};
+    const cuuint32_t box[4] = {bx, by, bz, 1};
+    const cuuint32_t estr[4] = {1, 1, 1, 1};
+    return enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, const_cast<double*>(base), dims, strides, box, estr,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+size_t heat_tma_smem(const CartTopo& topo, int zc) {
+    auto up128 = [](size_t b) { return (b + 127) & ~size_t(127); };
+    const size_t W = topo.n[0] + 2, n1 = topo.n[1];
+    return up128(zc * n1 * W * 8) + 2 * up128(n1 * W * 8) + 2 * up128(zc * W * 8) + 2 * up128(zc * n1 * 2 * 8) + 16;
+}
+}  // namespace
+
+bool heat3d_tma_supported(const CartTopo& topo, const SlabLayout& L) {
+    // rows of an even number of doubles keep every stride a multiple of 16
+    // bytes; a box edge is at most 256 elements; one thread per (x, y)
+    return heat3d_pull_supported(topo, L) && topo.n[0] % 2 == 0 && topo.n[0] + 2 <= 256 && topo.n[1] <= 256 &&
+           (L.slab_stride * 8) % 16 == 0 && heat_tma_smem(topo, 1) <= 200 * 1024 && tensor_map_encoder() != nullptr;
+}
+
+cudaError_t launch_heat3d_tma(const double* in, double* out, const CartTopo& topo, const SlabLayout& L, int field,
+                              double kappa, double dt, const double inv_h2[3], int* err, cudaStream_t s) {
+    // planes per CTA: at most 16 and the stage at most 200 KB, fewer when
+    // whole blocks would not fill the GPU several times over
+    const int n2 = topo.n[2];
+    int zc = std::min(n2, 16);
+    while (zc > 1 && heat_tma_smem(topo, zc) > 200 * 1024) --zc;
+    while (zc > 4 && (int64_t)topo.nblocks * ((n2 + zc - 1) / zc) < (int64_t)lg::device_sm_count() * 8) zc = (zc + 1) / 2;
+    HeatMaps maps;
+    const double* base = in + (int64_t)field * L.slab_stride;
+    const uint32_t W = (uint32_t)topo.n[0] + 2, n1 = (uint32_t)topo.n[1];
+    if (!encode_heat_map(&maps.main, base, topo, L, W, n1, (uint32_t)zc) ||
+        !encode_heat_map(&maps.plane, base, topo, L, W, n1, 1) ||
+        !encode_heat_map(&maps.row, base, topo, L, W, 1, (uint32_t)zc) ||
+        !encode_heat_map(&maps.col, base, topo, L, 2, n1, (uint32_t)zc))
+        return cudaErrorInvalidValue;
+    const int64_t items = (int64_t)topo.nblocks * ((n2 + zc - 1) / zc);
+    const unsigned grid = (unsigned)std::min<int64_t>(items, (int64_t)1 << 30);
+    const size_t smem = heat_tma_smem(topo, zc);
+    static bool configured = false;
+    if (!configured) {
+        cudaError_t e = cudaFuncSetAttribute(heat3d_tma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             200 * 1024 + 1024);
+        if (e != cudaSuccess) return e;
+        configured = true;
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(topo.n[0], topo.n[1]);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    // ~20M polls of the barrier: well over a second before a copy counts as lost
+    const long long spin_limit = 20000000;
+    return cudaLaunchKernelEx(&cfg, heat3d_tma_kernel, maps, out, topo, L, field, kappa, dt, inv_h2[0], inv_h2[1],
+                              inv_h2[2], zc, err, spin_limit);
 }
 
 cudaError_t launch_heat_rk_stage(int mode, const double* in, double* out, const double* y, double* kout,

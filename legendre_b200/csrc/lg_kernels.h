@@ -44,6 +44,13 @@ bool heat3d_pull_supported(const CartTopo& topo, const SlabLayout& L);
 cudaError_t launch_heat3d_pull(const double* in, double* out, const CartTopo& topo, const SlabLayout& L, int field,
                                double kappa, double dt, const double inv_h2[3], cudaStream_t s);
 
+// The same step with each CTA's tile and its six halo faces staged by
+// tensor copies (TMA) onto one mbarrier; needs an even block width too.  A
+// wait for the copies that gives up sets *err (the context's device word).
+bool heat3d_tma_supported(const CartTopo& topo, const SlabLayout& L);
+cudaError_t launch_heat3d_tma(const double* in, double* out, const CartTopo& topo, const SlabLayout& L, int field,
+                              double kappa, double dt, const double inv_h2[3], int* err, cudaStream_t s);
+
 // (a) fused Model C Euler-Maruyama step, FP64, bit-exact to the reference.
 // Reads phi (field 0) and u (field 1) from `in`, writes both to `out` with
 // ghosts filled.  `tdev[slot]` holds the step's time (its bits are the noise

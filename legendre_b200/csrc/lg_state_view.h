@@ -27,6 +27,10 @@ struct StateView {
 int abi_state_view(const lg_state* st, StateView* v);
 int abi_fail(lg_ctx* ctx, int code, const std::string& msg);
 cudaStream_t abi_stream(lg_ctx* ctx);
+// the context's device error word (allocated and zeroed on first use; null
+// if that fails): kernels with bounded waits set it when a wait gives up,
+// and lg_sync / field downloads report it as LG_ERR_DEVICE
+int* abi_device_flag(lg_ctx* ctx);
 int abi_device(lg_ctx* ctx);
 void abi_count_launch(lg_ctx* ctx, int64_t n);
 

@@ -81,6 +81,8 @@ def _heat_pair(sched, orc, cells, block, periodic, h, kappa, dt, steps, graph=Fa
     ([24, 16, 8], [8, 8, 4], [False, True, False]),
     ([12, 8, 16], [12, 4, 8], [True, True, True]),   # one block along x: the periodic halo is the block itself
     ([8, 8, 40], [8, 8, 40], [False, False, True]),  # one block of 40 planes, split into z-ranges
+    ([9, 10, 12], [3, 5, 6], [True, False, False]),   # odd block width: the cp.async-staged form
+    ([32, 48, 48], [16, 16, 16], [False, True, False]),  # 16^3 blocks, tensor-copy staged, whole blocks per CTA
 ])
 def test_heat_bit_identical_to_oracle(sched, orc, cells, block, periodic):
     sim, os_, t = _heat_pair(sched, orc, cells, block, periodic, 0.1, 0.7, 0.5 / 6.0 * 0.01 / 0.7, 37)
