@@ -579,7 +579,7 @@ int lg_modelc_em_run(lg_state* st, const lg_modelc_params* p, double dt, uint64_
     if (st->grid->D != 2 || st->nfields < 2 || st->ghosts[0] != 1 || st->ghosts[1] != 1)
         return fail(ctx, LG_ERR_STATE, "Model C needs a 2-D state with phi and u of ghost width 1");
     if (nsteps < 0) return fail(ctx, LG_ERR_INVALID, "negative step count");
-    if (variant < 0 || variant % 1000 > 4) return fail(ctx, LG_ERR_INVALID, "unknown kernel variant");
+    if (variant < 0 || variant % 1000 > 7) return fail(ctx, LG_ERR_INVALID, "unknown kernel variant");
     cudaSetDevice(ctx->device);
     if (!st->ghosts_valid) {
         int rc = fill_all_ghosts(st);
@@ -616,8 +616,9 @@ int lg_modelc_em_run(lg_state* st, const lg_modelc_params* p, double dt, uint64_
              st->orient);
     const int64_t ncells = st->grid->nblocks * st->grid->block[0] * st->grid->block[1];
     // variant = kind + 1000 * rows: kind 0 library default, 1 one thread per
-    // cell in reference order, 2/3/4 warp strips with 2/3/4 CTAs per SM;
-    // rows fixes the strip height
+    // cell in reference order, 2/3/4 warp strips with 2/3/4 CTAs per SM, 5/6/7
+    // the same with two rows per pass of the row loop; rows fixes the strip
+    // height
     const int kind = variant % 1000, rows = variant / 1000;
     const bool tile = kind != 1 && lg::modelc_tile_supported(topo);
     const int minb = kind >= 2 ? kind : (st->dtype == LG_F32 ? 3 : 2);
@@ -684,7 +685,7 @@ int lg_modelc_autotune(lg_state* st, const lg_modelc_params* p, double dt, uint6
     ctx->tuned.erase(key);
     int best = 0;
     float best_t = 0.0f;
-    for (int kind : {2, 3, 4}) {
+    for (int kind : {2, 3, 4, 5, 6, 7}) {
         for (int rows : {0, 8, 16, 32}) {
             if (rc != LG_OK) break;
             const int v = kind + 1000 * rows;

@@ -395,10 +395,108 @@ __device__ __forceinline__ void strip_unit(const typename Ops::Params& m, uint64
     if (edge_x) flush_edges(out, g.L, nb, n0, n1, r0, r1, lane, col - lane == 0, cr == n0 - 1, eh);
 }
 
+// The paired form of one work unit (Euler-Maruyama, axis-aligned, units of
+// an even number of rows): each pass of the row loop steps rows j and j+1
+// together, so every lane carries two independent cells -- four face fluxes,
+// two Gaussians, two cell updates -- whose dependency chains the scheduler
+// interleaves; the y face between the two rows is computed once.  The window
+// holds phi rows j-1 .. j+2 with the prefetch of j+3 and j+4 in flight.
+// Same arithmetic per cell, in the same operand order, as strip_row.
+template <class T, class Ops, bool NOISE, int NX, bool FULL>
+__device__ __forceinline__ void strip_unit_pair(const typename Ops::Params& m, uint64_t seed, int key_block,
+                                                const TileArgs& g, const T* __restrict__ ph,
+                                                const T* __restrict__ uu, T* __restrict__ out, T* __restrict__ po,
+                                                T* __restrict__ uo, const Nbr2& nb, int r0, int r1, int lane,
+                                                int col, bool valid, int last_lane, int cr, bool edge_x, int n0,
+                                                int n1, int sy, double tnow, T dt, T scale_amp) {
+    uint64_t block_key = 0;
+    if (NOISE)
+        block_key = wiener_block_key(seed, (uint64_t)__double_as_longlong(tnow), kWienerStream0,
+                                     (uint64_t)key_block);
+    const bool ok = FULL || valid;
+    int off = ((FULL ? col : min(col, n0 - 1)) + 1) + (r0 + 1) * sy;
+    // rows r0-1 .. r0+2 (every unit has at least two rows, and rows up to n1
+    // -- the ghost row -- exist)
+    auto load_row = [&](int r, Row3<T>& w, T& uw) {
+        w = Row3<T>{};
+        uw = T(0);
+        if (r <= n1) {
+            const T* q = ph + off + (r - r0) * sy;
+            w = {__ldg(q - 1), __ldg(q), __ldg(q + 1)};
+            uw = __ldg(uu + off + (r - r0) * sy);
+        }
+    };
+    Row3<T> A, B, C, D, E, F;
+    T UA, UB, UC, UD, UE, UF;
+    load_row(r0 - 1, A, UA);
+    load_row(r0, B, UB);
+    load_row(r0 + 1, C, UC);
+    load_row(r0 + 2, D, UD);
+    T bnd = T(0);
+    {
+        const int r = r0 + lane;
+        if (r < r1) {
+            const T* q = ph + (cr + 1) + (r + 1) * sy;  // (column cr, row r)
+            const T c0m = __ldg(q - sy), c1m = __ldg(q - sy + 1);
+            const T c00 = __ldg(q), c10 = __ldg(q + 1);
+            const T c0p = __ldg(q + sy), c1p = __ldg(q + sy + 1);
+            bnd = Ops::xface(m, c10 - c00, c1p - c1m, c0p, c0m);
+        }
+    }
+    T jb = Ops::yface(m, B.b - A.b, B.c - B.a, A.c, A.a);
+    EdgeHold<T> eh{T(0), T(0), T(0), T(0)};
+#pragma unroll 1
+    for (int j = r0; j < r1; j += 2) {
+        // prefetch of rows j+3 and j+4
+        load_row(j + 3, E, UE);
+        load_row(j + 4, F, UF);
+        const T ul0 = __ldg(uu + off - 1), ur0 = __ldg(uu + off + 1);
+        const T ul1 = __ldg(uu + off + sy - 1), ur1 = __ldg(uu + off + sy + 1);
+        T nv0 = T(0), nv1 = T(0);
+        if (NOISE) {
+            nv0 = Ops::noise(splitmix64(block_key ^ (uint64_t)(col + j * n0)));
+            nv1 = Ops::noise(splitmix64(block_key ^ (uint64_t)(col + (j + 1) * n0)));
+        }
+        const T fl0 = Ops::xface(m, B.b - B.a, C.b - A.b, C.a, A.a);
+        const T jt0 = Ops::yface(m, C.b - B.b, C.c - C.a, B.c, B.a);
+        const T fl1 = Ops::xface(m, C.b - C.a, D.b - B.b, D.a, B.a);
+        const T jt1 = Ops::yface(m, D.b - C.b, D.c - D.a, C.c, C.a);
+        T fr0 = __shfl_down_sync(kFull, fl0, 1), fr1 = __shfl_down_sync(kFull, fl1, 1);
+        const T fb0 = __shfl_sync(kFull, bnd, (j - r0) & 31), fb1 = __shfl_sync(kFull, bnd, (j + 1 - r0) & 31);
+        if (lane == last_lane) {
+            fr0 = fb0;
+            fr1 = fb1;
+        }
+        T kphi0, ku0, kphi1, ku1;
+        Ops::cell(m, fr0, fl0, jt0, jb, B.b, B.c - B.a, C.b - A.b, UB, ul0, ur0, UC, UA, kphi0, ku0);
+        Ops::cell(m, fr1, fl1, jt1, jt0, C.b, C.c - C.a, D.b - B.b, UC, ul1, ur1, UD, UB, kphi1, ku1);
+        T phin0 = Ops::axpy(dt, kphi0, B.b), phin1 = Ops::axpy(dt, kphi1, C.b);
+        if (NOISE) {
+            phin0 = Ops::add_noise(phin0, scale_amp, nv0);
+            phin1 = Ops::add_noise(phin1, scale_amp, nv1);
+        }
+        const T un0 = Ops::axpy(dt, ku0, UB), un1 = Ops::axpy(dt, ku1, UC);
+        store_cell(out, po, uo, off, phin0, un0, ok, true, edge_x, j, r0, n0, n1, col, lane, last_lane, g.L, nb, eh);
+        store_cell(out, po, uo, off + sy, phin1, un1, ok, true, edge_x, j + 1, r0, n0, n1, col, lane, last_lane, g.L,
+                   nb, eh);
+        jb = jt1;
+        A = C;
+        B = D;
+        C = E;
+        D = F;
+        UA = UC;
+        UB = UD;
+        UC = UE;
+        UD = UF;
+        off += 2 * sy;
+    }
+    if (edge_x) flush_edges(out, g.L, nb, n0, n1, r0, r1, lane, col - lane == 0, cr == n0 - 1, eh);
+}
+
 // Rows per work unit are at most 32, so one batch of boundary faces (lanes
 // across rows) serves the whole unit.
 template <class T, class Ops, bool NOISE, int MINB, int NX, int PF, bool BATCH = false, bool TAIL = false,
-          bool ORIENT = false, int MODE = 0>
+          bool ORIENT = false, int MODE = 0, bool PAIR = false>
 __global__ void __launch_bounds__(256, MINB)
     modelc_strip_kernel(const T* __restrict__ in, T* __restrict__ out, TileArgs g, typename Ops::Params m0, T dt,
                         T scale_amp, BatchArgs bt, OrientArgs oa, RkArgs<T> rk) {
@@ -444,7 +542,20 @@ __global__ void __launch_bounds__(256, MINB)
         T* uo = out + slab_base(g.L, b, 1);
         Nbr2 nb;
         nb.load(topo, b);
-        if constexpr (BATCH) {
+        if constexpr (PAIR) {
+            static_assert(MODE == 0 && !ORIENT && !TAIL, "the paired rows serve the Euler-Maruyama step");
+            if constexpr (BATCH) {
+                const int inst = b / bt.bpi;
+                const typename Ops::Params mi = static_cast<const typename Ops::Params*>(bt.params)[inst];
+                strip_unit_pair<T, Ops, NOISE, NX, FULL>(mi, bt.seeds[inst], b - inst * bt.bpi, g, ph, uu, out, po, uo,
+                                                         nb, r0, r1, lane, col, valid, last_lane, cr, edge_x, n0, n1,
+                                                         sy, tnow, dt, scale_amp);
+            } else {
+                strip_unit_pair<T, Ops, NOISE, NX, FULL>(m0, g.seed, b, g, ph, uu, out, po, uo, nb, r0, r1, lane, col,
+                                                         valid, last_lane, cr, edge_x, n0, n1, sy, tnow, dt,
+                                                         scale_amp);
+            }
+        } else if constexpr (BATCH) {
             const int inst = b / bt.bpi;
             const typename Ops::Params mi = static_cast<const typename Ops::Params*>(bt.params)[inst];
             strip_unit<T, Ops, NOISE, NX, FULL, PF, TAIL, ORIENT, MODE>(
@@ -514,22 +625,25 @@ cudaError_t launch_strip_batch(const T* in, T* out, TileArgs g, BatchArgs bt, T 
     return cudaGetLastError();
 }
 
-template <class T, class Ops, bool NOISE, int MINB, int PF>
+template <class T, class Ops, bool NOISE, int MINB, int PF, bool PAIR = false>
 cudaError_t launch_strip_minb(const T* in, T* out, TileArgs g, const typename Ops::Params& m, T dt, T scale_amp,
                               cudaStream_t s) {
     const bool tail = strip_plan(g, PF + 3);
     const dim3 grid = strip_ctas(g), block(256);
-    if (tail) {
+    if (tail) {  // blocks lower than the row group: single rows (the paired form needs whole groups)
         modelc_strip_kernel<T, Ops, NOISE, MINB, 0, PF, false, true><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp, BatchArgs{}, OrientArgs{}, RkArgs<T>{});
         return cudaGetLastError();
     }
+    const BatchArgs nob{};
+    const OrientArgs noo{};
+    const RkArgs<T> nork{};
     switch (g.topo.n[0]) {  // block widths of the shipped configurations get a compile-time row stride
-        case 32: modelc_strip_kernel<T, Ops, NOISE, MINB, 32, PF><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp, BatchArgs{}, OrientArgs{}, RkArgs<T>{}); break;
-        case 64: modelc_strip_kernel<T, Ops, NOISE, MINB, 64, PF><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp, BatchArgs{}, OrientArgs{}, RkArgs<T>{}); break;
-        case 126: modelc_strip_kernel<T, Ops, NOISE, MINB, 126, PF><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp, BatchArgs{}, OrientArgs{}, RkArgs<T>{}); break;
-        case 128: modelc_strip_kernel<T, Ops, NOISE, MINB, 128, PF><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp, BatchArgs{}, OrientArgs{}, RkArgs<T>{}); break;
-        case 256: modelc_strip_kernel<T, Ops, NOISE, MINB, 256, PF><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp, BatchArgs{}, OrientArgs{}, RkArgs<T>{}); break;
-        default: modelc_strip_kernel<T, Ops, NOISE, MINB, 0, PF><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp, BatchArgs{}, OrientArgs{}, RkArgs<T>{});
+        case 32: modelc_strip_kernel<T, Ops, NOISE, MINB, 32, PF, false, false, false, 0, PAIR><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp, nob, noo, nork); break;
+        case 64: modelc_strip_kernel<T, Ops, NOISE, MINB, 64, PF, false, false, false, 0, PAIR><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp, nob, noo, nork); break;
+        case 126: modelc_strip_kernel<T, Ops, NOISE, MINB, 126, PF, false, false, false, 0, PAIR><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp, nob, noo, nork); break;
+        case 128: modelc_strip_kernel<T, Ops, NOISE, MINB, 128, PF, false, false, false, 0, PAIR><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp, nob, noo, nork); break;
+        case 256: modelc_strip_kernel<T, Ops, NOISE, MINB, 256, PF, false, false, false, 0, PAIR><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp, nob, noo, nork); break;
+        default: modelc_strip_kernel<T, Ops, NOISE, MINB, 0, PF, false, false, false, 0, PAIR><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp, nob, noo, nork);
     }
     return cudaGetLastError();
 }
@@ -567,15 +681,21 @@ cudaError_t launch_strip_rk(const T* in, T* out, TileArgs g, const typename Ops:
     return cudaGetLastError();
 }
 
-// occupancy: CTAs of 256 threads per SM the register allocation must allow
-// (2: up to 128 registers, 3: 80, 4: 64)
+// kind 2/3/4: single rows, CTAs of 256 threads per SM the register
+// allocation must allow (2: up to 128 registers, 3: 80, 4: 64); kind 5/6/7:
+// the paired rows (strip_unit_pair) at 2/3/4 CTAs per SM.
 // PF: rows of prefetch ahead of the row being computed
 template <class T, class Ops, bool NOISE, int PF>
 cudaError_t launch_strip_ops(const T* in, T* out, TileArgs g, const typename Ops::Params& m, T dt, T scale_amp,
-                             int minb, cudaStream_t s) {
-    if (minb == 3) return launch_strip_minb<T, Ops, NOISE, 3, PF>(in, out, g, m, dt, scale_amp, s);
-    if (minb == 4) return launch_strip_minb<T, Ops, NOISE, 4, PF>(in, out, g, m, dt, scale_amp, s);
-    return launch_strip_minb<T, Ops, NOISE, 2, PF>(in, out, g, m, dt, scale_amp, s);
+                             int kind, cudaStream_t s) {
+    switch (kind) {
+        case 3: return launch_strip_minb<T, Ops, NOISE, 3, PF>(in, out, g, m, dt, scale_amp, s);
+        case 4: return launch_strip_minb<T, Ops, NOISE, 4, PF>(in, out, g, m, dt, scale_amp, s);
+        case 5: return launch_strip_minb<T, Ops, NOISE, 2, PF, true>(in, out, g, m, dt, scale_amp, s);
+        case 6: return launch_strip_minb<T, Ops, NOISE, 3, PF, true>(in, out, g, m, dt, scale_amp, s);
+        case 7: return launch_strip_minb<T, Ops, NOISE, 4, PF, true>(in, out, g, m, dt, scale_amp, s);
+        default: return launch_strip_minb<T, Ops, NOISE, 2, PF>(in, out, g, m, dt, scale_amp, s);
+    }
 }
 
 }  // namespace lg

@@ -231,7 +231,8 @@ def test_dendrite_grows_and_stays_physical_on_gpu(sched, orc):
     assert -0.4 < u.max() < 0.05 and u.min() >= -0.75
 
 
-@pytest.mark.parametrize("variant", [1, 2, 2 + 1000 * 16, 2 + 1000 * 24, 2 + 1000 * 7, 2 + 1000 * 5000])
+@pytest.mark.parametrize("variant", [1, 2, 2 + 1000 * 16, 2 + 1000 * 24, 2 + 1000 * 7, 2 + 1000 * 5000,
+                                     5, 5 + 1000 * 8, 6 + 1000 * 16, 7 + 1000 * 32])
 @pytest.mark.parametrize("noise", [0.0, 0.05])
 def test_modelc_kernel_variants_bit_identical(sched, orc, variant, noise):
     # every kernel shape (reference order, column tiles of any height) gives
@@ -259,15 +260,16 @@ def test_modelc_tile_ragged_blocks(sched, orc, block):
     assert np.array_equal(sim.state.interior("u"), os_.interior(1))
 
 
-@pytest.mark.parametrize("block", [[33, 20], [126, 6], [126, 40]])
-def test_modelc_tile_ragged_blocks_noisy(sched, orc, block):
+@pytest.mark.parametrize("block", [[33, 20], [126, 6], [126, 40], [7, 3]])
+@pytest.mark.parametrize("paired", [2, 5])
+def test_modelc_tile_ragged_blocks_noisy(sched, orc, block, paired):
     # strips whose last lanes lie past the block edge: with noise, the strip
     # kernel gives the bits of the one-thread-per-cell kernel
     cells = [block[0] * 2, block[1] * 2]
     grid = L.CartesianGrid(cells, block, [0.0, 0.0], [H, H])
     model = L.ModelC(0.06, 3.19, 0.05)
     sims = []
-    for variant in (2, 1):
+    for variant in (paired, 1):
         sim = L.Simulation(grid, L.FiniteVolume(), model, L.EulerMaruyama(5), sched, L.CudaAllocator("f64"))
         model.initialize_grains(grid, sim.state, [L.Grain((cells[0] * H / 2, cells[1] * H / 2), 2.0)], 0.7)
         sim.run(model.stable_dt(grid.spacing), 30, variant=variant)
@@ -294,7 +296,7 @@ def test_autotune_restores_the_state_and_keeps_the_results(sched, orc, dtype):
     t0, k0 = sim.time(), sim.step_index()
     dt = sim.model.stable_dt(sim.grid.spacing)
     variant, ms = sim.autotune(dt, trial_steps=5)
-    assert variant % 1000 in (2, 3, 4) and ms > 0.0
+    assert variant % 1000 in (2, 3, 4, 5, 6, 7) and ms > 0.0
     for f, b in zip(("phi", "u"), before):
         assert np.array_equal(sim.state.download(f), b)
     assert sim.time() == t0 and sim.step_index() == k0
