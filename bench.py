@@ -90,6 +90,35 @@ NCU_PIPES = {("c2", "f64"): {"issue_active": 0.682, "fp64_pipe": 0.388, "capture
 
 NOMINAL_HBM_GBS = 8000.0  # a B200's nominal HBM3e bandwidth, the second denominator
 
+# Instruction mix of the dominant kernel per cell-update, from one ncu capture
+# each (smsp__inst_executed and the fp64 pipe's share, x 32 threads per warp
+# instruction, divided by the launch's cell-updates); the capture named is
+# the summary under profiles/.  Filled for the configurations captured.
+NCU_INST = {}
+
+
+def compute_roofline(peaks, sm_mhz, cells_per_s, ncu):
+    """The compute side of the roofline: the kernel's thread-instruction rate
+    against the issue ceiling (one warp instruction per SM sub-partition per
+    clock at the sampled SM clock) and its FP64 operation rate against the
+    measured FP64 FMA rate of the device (lg_measure_compute_peaks)."""
+    if peaks is None:
+        return None
+    clock = sm_mhz if sm_mhz else peaks["clock_mhz"]
+    issue_ceiling = peaks["sms"] * 4 * 32 * clock * 1e6
+    out = {"issue_ceiling_thread_inst_per_s": issue_ceiling, "clock_mhz": clock,
+           "measured": {k: peaks[k] for k in ("dfma_per_s", "ffma_per_s", "imad_per_s", "alu_per_s")},
+           "inst_per_cell": None, "issue_frac": None, "fp64_inst_per_cell": None, "fp64_frac": None,
+           "capture": None}
+    if ncu:
+        out["capture"] = ncu["capture"]
+        out["inst_per_cell"] = ncu["inst_per_cell"]
+        out["issue_frac"] = ncu["inst_per_cell"] * cells_per_s / issue_ceiling
+        if ncu.get("fp64_inst_per_cell") is not None:
+            out["fp64_inst_per_cell"] = ncu["fp64_inst_per_cell"]
+            out["fp64_frac"] = ncu["fp64_inst_per_cell"] * cells_per_s / peaks["dfma_per_s"]
+    return out
+
 
 def ncu_capture_config(args) -> bool:
     """True when the run is the configuration the ncu figures were taken on:
@@ -668,7 +697,8 @@ def run_ensemble(args, cfg):
         pg.destroy_process_group()
 
 
-def model_c_line(args, cfg, world, ms, clk, launches, tuned, e2e, observed, err, cpu, peak, peak_kind):
+def model_c_line(args, cfg, world, ms, clk, launches, tuned, e2e, observed, err, cpu, peak, peak_kind,
+                 compute_peaks=None):
     """The JSON line of a uniform-grid Model C run from its measured parts
     (device time of the K timed steps `ms`, sampled clocks, launch count,
     autotuner choice, end-to-end and observer blocks, FP32 error, CPU
@@ -696,7 +726,10 @@ def model_c_line(args, cfg, world, ms, clk, launches, tuned, e2e, observed, err,
                    "graph": True, "variant": args.variant, "autotuned_variant": tuned},
         "roofline": hbm_roofline(achieved, peak, peak_kind, traffic=traffic(args, cells),
                                  algorithmic_bytes_per_cell=bpc,
-                                 ncu_pipes=NCU_PIPES.get((args.config, args.dtype)) if captured_cfg else None),
+                                 ncu_pipes=NCU_PIPES.get((args.config, args.dtype)) if captured_cfg else None,
+                                 compute=compute_roofline(compute_peaks, clk.get("sm_mhz"), value * 1e9 / world,
+                                                          NCU_INST.get((args.config, args.dtype))
+                                                          if captured_cfg else None)),
         "cpu_baseline": cpu,
         "e2e": e2e,
         "fp32_error": err,
@@ -887,7 +920,8 @@ def run_model_c(args, cfg):
             cpu = {"value": rate, "unit": "Gcell-updates/s", "cores": threads, "kind": "port",
                    "sample": f"{steps_run} steps of the same {cfg['cells']}^2 grid after 1 warm-up step, "
                              "OpenMP over blocks"}
-        line = model_c_line(args, cfg, world, ms, clk, launches, tuned, e2e, observed, err, cpu, peak, peak_kind)
+        line = model_c_line(args, cfg, world, ms, clk, launches, tuned, e2e, observed, err, cpu, peak, peak_kind,
+                            compute_peaks=sched.compute_peaks())
         print(json.dumps(line), flush=True)
     sched.close()
     if pg is not None:

@@ -193,3 +193,19 @@ def test_reference_arm_maps_no_product_library(tmp_path):
     assert "PRODUCT_NOT_MAPPED" in out.stdout and "ORACLE_MAPPED" in out.stdout
     line = json.loads(out.stdout.strip().splitlines()[0])
     assert line["impl"] == "reference" and line["ms_per_step"] > 0
+
+
+def test_compute_roofline_fractions():
+    sys.path.insert(0, str(ROOT))
+    import bench
+
+    peaks = {"dfma_per_s": 20e12, "ffma_per_s": 70e12, "imad_per_s": 35e12, "alu_per_s": 35e12, "sms": 148,
+             "clock_mhz": 1965.0}
+    ncu = {"capture": "x", "inst_per_cell": 464.0, "fp64_inst_per_cell": 266.0}
+    r = bench.compute_roofline(peaks, 1965.0, 50e9, ncu)
+    ceiling = 148 * 4 * 32 * 1965e6
+    assert abs(r["issue_ceiling_thread_inst_per_s"] - ceiling) < 1.0
+    assert abs(r["issue_frac"] - 464.0 * 50e9 / ceiling) < 1e-12
+    assert abs(r["fp64_frac"] - 266.0 * 50e9 / 20e12) < 1e-12
+    assert bench.compute_roofline(peaks, None, 50e9, None)["issue_frac"] is None
+    assert bench.compute_roofline(None, 1965.0, 50e9, ncu) is None
