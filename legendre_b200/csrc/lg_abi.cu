@@ -423,13 +423,14 @@ int lg_state_create(lg_ctx* ctx, const lg_grid* grid, int dtype, int nfields, co
         }
         cudaMemsetAsync(st->arena[k], 0, bytes, ctx->stream);
     }
-    if (cudaMalloc(&st->d_t, 2 * sizeof(double)) != cudaSuccess) {
+    // two time slots, then the two work-list counters of the strip kernel
+    if (cudaMalloc(&st->d_t, 4 * sizeof(double)) != cudaSuccess) {
         cudaFree(st->arena[0]);
         cudaFree(st->arena[1]);
         delete st;
         return fail(ctx, LG_ERR_NOMEM, "time slot allocation failed");
     }
-    cudaMemsetAsync(st->d_t, 0, 2 * sizeof(double), ctx->stream);
+    cudaMemsetAsync(st->d_t, 0, 4 * sizeof(double), ctx->stream);
     cudaError_t e = cudaStreamSynchronize(ctx->stream);
     if (e != cudaSuccess) {
         lg_state_destroy(st);
@@ -579,7 +580,8 @@ int lg_modelc_em_run(lg_state* st, const lg_modelc_params* p, double dt, uint64_
     if (st->grid->D != 2 || st->nfields < 2 || st->ghosts[0] != 1 || st->ghosts[1] != 1)
         return fail(ctx, LG_ERR_STATE, "Model C needs a 2-D state with phi and u of ghost width 1");
     if (nsteps < 0) return fail(ctx, LG_ERR_INVALID, "negative step count");
-    if (variant < 0 || variant % 1000 > 7) return fail(ctx, LG_ERR_INVALID, "unknown kernel variant");
+    if (variant < 0 || variant % 1000 % 10 > 7 || variant % 1000 > 17 || (variant % 1000 >= 10 && variant % 10 < 2))
+        return fail(ctx, LG_ERR_INVALID, "unknown kernel variant");
     cudaSetDevice(ctx->device);
     if (!st->ghosts_valid) {
         int rc = fill_all_ghosts(st);
@@ -617,11 +619,16 @@ int lg_modelc_em_run(lg_state* st, const lg_modelc_params* p, double dt, uint64_
     const int64_t ncells = st->grid->nblocks * st->grid->block[0] * st->grid->block[1];
     // variant = kind + 1000 * rows: kind 0 library default, 1 one thread per
     // cell in reference order, 2/3/4 warp strips with 2/3/4 CTAs per SM, 5/6/7
-    // the same with two rows per pass of the row loop; rows fixes the strip
-    // height
-    const int kind = variant % 1000, rows = variant / 1000;
+    // the same with two rows per pass of the row loop, 12..17 those forms as
+    // a persistent work list; rows fixes the strip height
+    const int kind = variant % 1000 % 10, rows = variant / 1000;
+    const bool listed = variant % 1000 >= 10;
     const bool tile = kind != 1 && lg::modelc_tile_supported(topo);
     const int minb = kind >= 2 ? kind : (st->dtype == LG_F32 ? 3 : 2);
+    unsigned* work = listed ? reinterpret_cast<unsigned*>(st->d_t + 2) : nullptr;
+    // the run's first step takes its units from a cleared list (each step
+    // clears the other slot's list for the step after it)
+    if (work) LG_CUDA(ctx, cudaMemsetAsync(work + st->tslot, 0, sizeof(unsigned), ctx->stream));
     if (kind == 2 && !tile) return fail(ctx, LG_ERR_INVALID, "the strip kernel needs a 2-D grid");
     auto step = [&]() -> int {
         cudaError_t e;
@@ -637,12 +644,12 @@ int lg_modelc_em_run(lg_state* st, const lg_modelc_params* p, double dt, uint64_
                                                      static_cast<const float*>(st->orient), ncells, rows, ctx->stream);
         else if (st->dtype == LG_F64)
             e = tile ? lg::launch_modelc_tile_f64(static_cast<const double*>(in), static_cast<double*>(out), topo, L,
-                                                  m, dt, nz, st->d_t, st->tslot, rows, minb, ctx->stream)
+                                                  m, dt, nz, st->d_t, st->tslot, rows, minb, work, ctx->stream)
                      : lg::launch_modelc_step_f64(static_cast<const double*>(in), static_cast<double*>(out), topo, L,
                                                   m, dt, nz, st->d_t, st->tslot, variant, ctx->stream);
         else
             e = tile ? lg::launch_modelc_tile_f32(static_cast<const float*>(in), static_cast<float*>(out), topo, L,
-                                                  m, dt, nz, st->d_t, st->tslot, rows, minb, ctx->stream)
+                                                  m, dt, nz, st->d_t, st->tslot, rows, minb, work, ctx->stream)
                      : lg::launch_modelc_step_f32(static_cast<const float*>(in), static_cast<float*>(out), topo, L, m,
                                                   dt, nz, st->d_t, st->tslot, variant, ctx->stream);
         ctx->launches++;
@@ -685,7 +692,7 @@ int lg_modelc_autotune(lg_state* st, const lg_modelc_params* p, double dt, uint6
     ctx->tuned.erase(key);
     int best = 0;
     float best_t = 0.0f;
-    for (int kind : {2, 3, 4, 5, 6, 7}) {
+    for (int kind : {2, 3, 4, 5, 6, 7, 12, 13, 14, 15, 16, 17}) {
         for (int rows : {0, 8, 16, 32}) {
             if (rc != LG_OK) break;
             const int v = kind + 1000 * rows;

@@ -75,16 +75,19 @@ cudaError_t launch_heat_rk_stage(int mode, const double* in, double* out, const 
 
 // Warp-strip variants of the same steps (lg_modelc.cu, lg_modelc_f32.cu):
 // each face flux is evaluated once and shared by its two cells; `rows` rows
-// of one block per warp (0 = chosen from the grid); `minb` = CTAs per SM
-// the register allocation must allow (2, 3 or 4).  The FP64 results are
-// bit-identical to the reference-order kernel above.
+// of one block per warp (0 = chosen from the grid); `minb` = the form: 2, 3
+// or 4 CTAs per SM the register allocation must allow, 5, 6, 7 the same
+// with two rows per pass of the row loop.  With `work` (two counters, the
+// step's at `slot`) the launch is one wave of CTAs whose warps take further
+// units from the counter; null gives the static grid-stride schedule.  The
+// FP64 results are bit-identical to the reference-order kernel above.
 bool modelc_tile_supported(const CartTopo& topo);
 cudaError_t launch_modelc_tile_f64(const double* in, double* out, const CartTopo& topo, const SlabLayout& L,
                                    const ModelCDev& m, double dt, const NoiseDev& nz, double* tdev, int slot,
-                                   int rows, int minb, cudaStream_t s);
+                                   int rows, int minb, unsigned* work, cudaStream_t s);
 cudaError_t launch_modelc_tile_f32(const float* in, float* out, const CartTopo& topo, const SlabLayout& L,
                                    const ModelCDev& m, double dt, const NoiseDev& nz, double* tdev, int slot,
-                                   int rows, int minb, cudaStream_t s);
+                                   int rows, int minb, unsigned* work, cudaStream_t s);
 // The multi-grain step (lg_modelc.cu, lg_modelc_f32.cu): the strip schedule
 // with every cell's four faces in its own crystal frame; `trig` holds cos
 // theta0 of the ncells interior cells (blocks in order, dimension 0 fastest)

@@ -14,8 +14,8 @@ bool modelc_tile_supported(const CartTopo& topo) { return topo.D == 2 && topo.n[
 
 cudaError_t launch_modelc_tile_f64(const double* in, double* out, const CartTopo& topo, const SlabLayout& L,
                                    const ModelCDev& m, double dt, const NoiseDev& nz, double* tdev, int slot,
-                                   int rows, int minb, cudaStream_t s) {
-    TileArgs g{topo, L, dt, nz.seed, tdev, slot, rows, 0, 0, 0};
+                                   int rows, int minb, unsigned* work, cudaStream_t s) {
+    TileArgs g{topo, L, dt, nz.seed, tdev, slot, rows, 0, 0, 0, work};
     const MC<double> mc = to_mc<double>(m);
     const double scale_amp = std::sqrt(dt) * nz.amp;
     if (nz.on) return launch_strip_ops<double, OpsExact<double>, true, 1>(in, out, g, mc, dt, scale_amp, minb, s);

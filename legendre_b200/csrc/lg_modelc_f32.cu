@@ -140,8 +140,8 @@ Fast32 fast32_of(const ModelCDev& m) {
 
 cudaError_t launch_modelc_tile_f32(const float* in, float* out, const CartTopo& topo, const SlabLayout& L,
                                    const ModelCDev& m, double dt, const NoiseDev& nz, double* tdev, int slot,
-                                   int rows, int minb, cudaStream_t s) {
-    TileArgs g{topo, L, dt, nz.seed, tdev, slot, rows, 0, 0, 0};
+                                   int rows, int minb, unsigned* work, cudaStream_t s) {
+    TileArgs g{topo, L, dt, nz.seed, tdev, slot, rows, 0, 0, 0, work};
     const Fast32 f = fast32_of(m);
     const float scale_amp = (float)(std::sqrt(dt) * nz.amp);
     if (nz.on) return launch_strip_ops<float, OpsFast32, true, 1>(in, out, g, f, (float)dt, scale_amp, minb, s);

@@ -61,6 +61,10 @@ struct TileArgs {
     int strips;   // 32-column strips per block
     int chunks;   // row chunks per block
     int64_t units;
+    // persistent work list (null: a static grid-stride schedule): one wave
+    // of CTAs, each warp taking its first unit by position and every further
+    // one from work[slot]; the step clears work[slot ^ 1] for the next step
+    unsigned* work;
 };
 
 // Batched instances (BATCH kernels): block b belongs to instance b / bpi,
@@ -513,10 +517,13 @@ __global__ void __launch_bounds__(256, MINB)
     // writes t + dt to the other slot (simulation.rs:285), so a captured
     // sequence of steps needs no host-side time.
     const double tnow = g.tdev[g.slot];
-    if (MODE != 1 && blockIdx.x == 0 && threadIdx.x == 0) g.tdev[g.slot ^ 1] = tnow + g.dt64;
+    if (MODE != 1 && blockIdx.x == 0 && threadIdx.x == 0) {
+        g.tdev[g.slot ^ 1] = tnow + g.dt64;
+        if (g.work) g.work[g.slot ^ 1] = 0u;
+    }
 
-    for (int64_t unit = (int64_t)blockIdx.x * wpc + (threadIdx.x >> 5); unit < g.units;
-         unit += (int64_t)gridDim.x * wpc) {
+    const int64_t first_listed = (int64_t)gridDim.x * wpc;
+    for (int64_t unit = (int64_t)blockIdx.x * wpc + (threadIdx.x >> 5); unit < g.units;) {
         const int s = (int)(unit % g.strips);
         const int k = (int)((unit / g.strips) % g.chunks);
         const int b = (int)(unit / ((int64_t)g.strips * g.chunks));
@@ -568,6 +575,13 @@ __global__ void __launch_bounds__(256, MINB)
                                                                         r0, r1, lane, col, valid, last_lane, cr,
                                                                         edge_x, n0, n1, sy, tnow, dt, scale_amp,
                                                                         trig_b, oa.ncells, rk);
+        }
+        if (g.work) {  // the next unit of the list
+            unsigned n = 0;
+            if (lane == 0) n = atomicAdd(g.work + g.slot, 1u);
+            unit = first_listed + (int64_t)__shfl_sync(kFull, n, 0);
+        } else {
+            unit += first_listed;
         }
     }
 }
@@ -629,7 +643,10 @@ template <class T, class Ops, bool NOISE, int MINB, int PF, bool PAIR = false>
 cudaError_t launch_strip_minb(const T* in, T* out, TileArgs g, const typename Ops::Params& m, T dt, T scale_amp,
                               cudaStream_t s) {
     const bool tail = strip_plan(g, PF + 3);
-    const dim3 grid = strip_ctas(g), block(256);
+    dim3 grid = strip_ctas(g);
+    const dim3 block(256);
+    if (g.work)  // the work list: one wave, MINB CTAs per SM
+        grid.x = (unsigned)std::min<int64_t>(grid.x, (int64_t)device_sm_count() * MINB);
     if (tail) {  // blocks lower than the row group: single rows (the paired form needs whole groups)
         modelc_strip_kernel<T, Ops, NOISE, MINB, 0, PF, false, true><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp, BatchArgs{}, OrientArgs{}, RkArgs<T>{});
         return cudaGetLastError();

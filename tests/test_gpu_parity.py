@@ -232,7 +232,8 @@ def test_dendrite_grows_and_stays_physical_on_gpu(sched, orc):
 
 
 @pytest.mark.parametrize("variant", [1, 2, 2 + 1000 * 16, 2 + 1000 * 24, 2 + 1000 * 7, 2 + 1000 * 5000,
-                                     5, 5 + 1000 * 8, 6 + 1000 * 16, 7 + 1000 * 32])
+                                     5, 5 + 1000 * 8, 6 + 1000 * 16, 7 + 1000 * 32, 12, 13 + 1000 * 8,
+                                     15 + 1000 * 16, 17 + 1000 * 32])
 @pytest.mark.parametrize("noise", [0.0, 0.05])
 def test_modelc_kernel_variants_bit_identical(sched, orc, variant, noise):
     # every kernel shape (reference order, column tiles of any height) gives
@@ -261,7 +262,7 @@ def test_modelc_tile_ragged_blocks(sched, orc, block):
 
 
 @pytest.mark.parametrize("block", [[33, 20], [126, 6], [126, 40], [7, 3]])
-@pytest.mark.parametrize("paired", [2, 5])
+@pytest.mark.parametrize("paired", [2, 5, 15])
 def test_modelc_tile_ragged_blocks_noisy(sched, orc, block, paired):
     # strips whose last lanes lie past the block edge: with noise, the strip
     # kernel gives the bits of the one-thread-per-cell kernel
@@ -296,7 +297,7 @@ def test_autotune_restores_the_state_and_keeps_the_results(sched, orc, dtype):
     t0, k0 = sim.time(), sim.step_index()
     dt = sim.model.stable_dt(sim.grid.spacing)
     variant, ms = sim.autotune(dt, trial_steps=5)
-    assert variant % 1000 in (2, 3, 4, 5, 6, 7) and ms > 0.0
+    assert variant % 1000 in (2, 3, 4, 5, 6, 7, 12, 13, 14, 15, 16, 17) and ms > 0.0
     for f, b in zip(("phi", "u"), before):
         assert np.array_equal(sim.state.download(f), b)
     assert sim.time() == t0 and sim.step_index() == k0
@@ -305,3 +306,27 @@ def test_autotune_restores_the_state_and_keeps_the_results(sched, orc, dtype):
         os_.modelc_run(orc.modelc_params(eps4=0.06, lam=3.19, noise=0.0), t0, dt, 7, 30, wiener=True, threads=4)
         assert np.array_equal(sim.state.interior("phi"), os_.interior(0))
         assert np.array_equal(sim.state.interior("u"), os_.interior(1))
+
+
+@pytest.mark.parametrize("variant", [12, 15 + 1000 * 8])
+def test_modelc_work_list_across_runs_and_graphs(sched, orc, variant):
+    """The persistent work-list form keeps its per-step unit counters right
+    across calls (odd step counts, graph replays, a call after the tuner's
+    trial steps) and gives the static schedule's bits."""
+    cells, block = [96, 64], [32, 32]
+    grains = [(10.0, 12.0, 4.0), (30.0, 14.0, 3.0)]
+    grid = L.CartesianGrid(cells, block, [0.0, 0.0], [H, H])
+    model = L.ModelC(0.06, 3.19, 0.05)
+    sims = []
+    for v in (variant, 2):
+        sim = L.Simulation(grid, L.FiniteVolume(), model, L.EulerMaruyama(9), sched, L.CudaAllocator("f64"))
+        model.initialize_grains(grid, sim.state, [L.Grain((g[0], g[1]), g[2]) for g in grains], 0.7)
+        dt = model.stable_dt(grid.spacing)
+        sim.run(dt, 3, graph=True, variant=v)
+        if v == variant:
+            sim.autotune(dt, trial_steps=3)
+        sim.run(dt, 4, graph=True, variant=v)
+        sim.run(dt, 5, graph=False, variant=v)
+        sims.append(sim)
+    for f in ("phi", "u"):
+        assert np.array_equal(sims[0].state.download(f), sims[1].state.download(f))
