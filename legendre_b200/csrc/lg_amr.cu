@@ -185,8 +185,11 @@ constexpr int kWin = lg::amr::kTile + 2;
 
 // Stage the (w + 2) x (h + 2) window of a tile for NF fields: block interior
 // entries from `in`, block ghost entries from the tile's fill ops.
+// `pre`, when not null, is this thread's first fill op of the tile
+// (tfill[fill0 + threadIdx.x]), read before the launch's dependency wait.
 template <int NF>
-__device__ __forceinline__ void stage_tile(const TileArgs& a, const lg::amr::Tile& T, double* s0, double* s1) {
+__device__ __forceinline__ void stage_tile(const TileArgs& a, const lg::amr::Tile& T, double* s0, double* s1,
+                                           const GhostOp* pre) {
     const int P = T.w + 2, R = T.h + 2, sy = T.nx + 2;
     const double* g0 = a.in + T.off;
     for (int k = threadIdx.x; k < P * R; k += blockDim.x) {
@@ -197,13 +200,41 @@ __device__ __forceinline__ void stage_tile(const TileArgs& a, const lg::amr::Til
         s0[k] = g0[o];
         if (NF == 2) s1[k] = g0[T.stride + o];
     }
-    for (int k = T.fill0 + (int)threadIdx.x; k < T.fill1; k += blockDim.x) {
+    int k = T.fill0 + (int)threadIdx.x;
+    if (pre && k < T.fill1) {
+        s0[pre->dst] = ghost_value(*pre, a.in, a.cnew, a.cold, a.interp, a.alpha, 0);
+        if (NF == 2) s1[pre->dst] = ghost_value(*pre, a.in, a.cnew, a.cold, a.interp, a.alpha, 1);
+        k += blockDim.x;
+    }
+    for (; k < T.fill1; k += blockDim.x) {
         const GhostOp op = a.tfill[k];
         s0[op.dst] = ghost_value(op, a.in, a.cnew, a.cold, a.interp, a.alpha, 0);
         if (NF == 2) s1[op.dst] = ghost_value(op, a.in, a.cnew, a.cold, a.interp, a.alpha, 1);
     }
     __syncthreads();
 }
+
+// The tables of a CTA's first tile -- its descriptor and this thread's first
+// fill op -- are read-only between regrids, so they are read before the
+// launch's dependency wait (programmatic dependent launch), while the
+// previous launch of the chain drains.
+struct TilePrefetch {
+    lg::amr::Tile T;
+    GhostOp op;
+    bool have_tile, have_op;
+    __device__ __forceinline__ void load(const TileArgs& a) {
+        have_tile = (int64_t)blockIdx.x < a.ntiles;
+        have_op = false;
+        if (have_tile) {
+            T = a.tiles[blockIdx.x];
+            const int k = T.fill0 + (int)threadIdx.x;
+            if (k < T.fill1) {
+                op = a.tfill[k];
+                have_op = true;
+            }
+        }
+    }
+};
 
 // Model C Euler-Maruyama on the tiles of one level (the reference-order cell
 // update of phasefield.rs:353-422 with the Time and Wiener drivers,
@@ -214,10 +245,10 @@ __device__ __forceinline__ void stage_tile(const TileArgs& a, const lg::amr::Til
 // right face of cell i are the same expression of the same operands.
 template <bool NOISE>
 __device__ __forceinline__ void modelc_tile(const TileArgs& a, const lg::MC<double>& m, const lg::amr::Tile& T,
-                                            double t, double* sp, double* su) {
+                                            double t, double* sp, double* su, const GhostOp* pre) {
     using Ops = lg::OpsExact<double>;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-    stage_tile<2>(a, T, sp, su);
+    stage_tile<2>(a, T, sp, su, pre);
     const int P = T.w + 2;
     const int rpw = (T.h + nwarps - 1) / nwarps;
     const int r0 = warp * rpw, r1 = min(T.h, r0 + rpw);
@@ -277,18 +308,22 @@ template <bool NOISE>
 __global__ void __launch_bounds__(256) amr_modelc_tiles(TileArgs a, lg::MC<double> m) {
     __shared__ double sp[kWin * kWin], su[kWin * kWin];
     pdl_release();
+    TilePrefetch pf;
+    pf.load(a);
     pdl_wait();
     const double t0 = a.tdev[a.slot];
     if (a.write_t && blockIdx.x == 0 && threadIdx.x == 0) a.tdev[a.slot ^ 1] = t0 + a.dt0;
     const double t = NOISE ? chain_time(t0, a.chain) : 0.0;
-    for (int64_t ti = blockIdx.x; ti < a.ntiles; ti += gridDim.x) modelc_tile<NOISE>(a, m, a.tiles[ti], t, sp, su);
+    if (pf.have_tile) modelc_tile<NOISE>(a, m, pf.T, t, sp, su, pf.have_op ? &pf.op : nullptr);
+    for (int64_t ti = (int64_t)blockIdx.x + gridDim.x; ti < a.ntiles; ti += gridDim.x)
+        modelc_tile<NOISE>(a, m, a.tiles[ti], t, sp, su, nullptr);
 }
 
 // Heat on the tiles of one level: k = lap(u) kappa, u + dt k
 // (tests/amr.rs:324-339, finite_difference.rs:49-67, euler.rs:51-53).
 __device__ __forceinline__ void heat_tile(const TileArgs& a, double kappa, double ih0, double ih1,
-                                          const lg::amr::Tile& T, double* sp) {
-    stage_tile<1>(a, T, sp, nullptr);
+                                          const lg::amr::Tile& T, double* sp, const GhostOp* pre) {
+    stage_tile<1>(a, T, sp, nullptr, pre);
     const int P = T.w + 2;
     for (int k = threadIdx.x; k < T.w * T.h; k += blockDim.x) {
         const int ci = k % T.w, cj = k / T.w;
@@ -306,10 +341,14 @@ __device__ __forceinline__ void heat_tile(const TileArgs& a, double kappa, doubl
 __global__ void __launch_bounds__(256) amr_heat_tiles(TileArgs a, double kappa, double ih0, double ih1) {
     __shared__ double sp[kWin * kWin];
     pdl_release();
+    TilePrefetch pf;
+    pf.load(a);
     pdl_wait();
     const double t0 = a.tdev[a.slot];
     if (a.write_t && blockIdx.x == 0 && threadIdx.x == 0) a.tdev[a.slot ^ 1] = t0 + a.dt0;
-    for (int64_t ti = blockIdx.x; ti < a.ntiles; ti += gridDim.x) heat_tile(a, kappa, ih0, ih1, a.tiles[ti], sp);
+    if (pf.have_tile) heat_tile(a, kappa, ih0, ih1, pf.T, sp, pf.have_op ? &pf.op : nullptr);
+    for (int64_t ti = (int64_t)blockIdx.x + gridDim.x; ti < a.ntiles; ti += gridDim.x)
+        heat_tile(a, kappa, ih0, ih1, a.tiles[ti], sp, nullptr);
 }
 
 // restriction body shared by the launch-per-phase and persistent paths
@@ -467,9 +506,9 @@ __global__ void __launch_bounds__(256) amr_persistent(PersistArgs a) {
             const double tt = NOISE ? chain_time(t0, ph.chain) : 0.0;
             for (int64_t ti = blockIdx.x; ti < t.ntiles; ti += gridDim.x) {
                 if (MODEL == LG_MODEL_C)
-                    modelc_tile<NOISE>(t, a.mc[ph.level], t.tiles[ti], tt, sp, su);
+                    modelc_tile<NOISE>(t, a.mc[ph.level], t.tiles[ti], tt, sp, su, nullptr);
                 else
-                    heat_tile(t, a.kappa, a.mc[ph.level].ih0, a.mc[ph.level].ih1, t.tiles[ti], sp);
+                    heat_tile(t, a.kappa, a.mc[ph.level].ih0, a.mc[ph.level].ih1, t.tiles[ti], sp, nullptr);
             }
         } else {
             double* C = ph.cnew ? a.arena1 : a.arena0;
