@@ -418,16 +418,18 @@ __device__ __forceinline__ void strip_unit_pair(const typename Ops::Params& m, u
         block_key = wiener_block_key(seed, (uint64_t)__double_as_longlong(tnow), kWienerStream0,
                                      (uint64_t)key_block);
     const bool ok = FULL || valid;
-    int off = ((FULL ? col : min(col, n0 - 1)) + 1) + (r0 + 1) * sy;
-    // rows r0-1 .. r0+2 (every unit has at least two rows, and rows up to n1
-    // -- the ghost row -- exist)
+    // slab offset of (col, r0), fixed for the unit; `off` follows the row pair
+    const int off0 = ((FULL ? col : min(col, n0 - 1)) + 1) + (r0 + 1) * sy;
+    int off = off0;
+    // phi (columns col-1, col, col+1) and u of row r, for -1 <= r <= n1 (row
+    // n1 is the ghost row); rows past n1 read as zero and are never used
     auto load_row = [&](int r, Row3<T>& w, T& uw) {
         w = Row3<T>{};
         uw = T(0);
         if (r <= n1) {
-            const T* q = ph + off + (r - r0) * sy;
+            const T* q = ph + off0 + (r - r0) * sy;
             w = {__ldg(q - 1), __ldg(q), __ldg(q + 1)};
-            uw = __ldg(uu + off + (r - r0) * sy);
+            uw = __ldg(uu + off0 + (r - r0) * sy);
         }
     };
     Row3<T> A, B, C, D, E, F;
