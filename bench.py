@@ -605,9 +605,10 @@ def run_ensemble(args, cfg):
     ms_e2e = max_over_ranks(pg, 1e3 * (time.perf_counter() - t0))
     ens._destroy()
 
-    # value and gradient over the configuration's horizon against a target at
-    # perturbed eps4 and Delta, and the forward pass of the same horizon
-    T = min(args.steps, cfg["full_steps"])
+    # value and gradient over the configuration's horizon (its full 2000
+    # steps, whatever --steps says) against a target at perturbed eps4 and
+    # Delta, and the forward pass of the same horizon
+    T = cfg["full_steps"]
     tgt = fresh([e + 0.005 for e in eps4], [d + 0.01 for d in delta])
     tgt.run(dt, T, graph=True)
     target = tgt.get("phi")

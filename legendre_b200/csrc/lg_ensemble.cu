@@ -58,6 +58,7 @@ struct lg_ensemble {
     int64_t acc_cap = 0;  // doubles held by d_acc
     double* d_loss = nullptr;
     double* d_target = nullptr;
+    double* d_usum = nullptr;  // per instance: the sum of the u cotangents (the Delta gradient's)
     int adj_kernel = lg::adj::kAdjointStrip;
 };
 
@@ -177,7 +178,8 @@ void free_workspace(lg_ensemble* e) {
     cudaFree(e->d_acc);
     cudaFree(e->d_loss);
     cudaFree(e->d_target);
-    e->d_acc = e->d_loss = e->d_target = nullptr;
+    cudaFree(e->d_usum);
+    e->d_acc = e->d_loss = e->d_target = e->d_usum = nullptr;
 }
 
 void free_all(lg_ensemble* e) {
@@ -208,9 +210,49 @@ int alloc_states(lg_ensemble* e, std::vector<void*>& v, size_t n) {
     return LG_OK;
 }
 
-double host_value(const lg_ensemble* e, const std::vector<char>& img, int64_t o) {
-    return e->dtype == LG_F64 ? reinterpret_cast<const double*>(img.data())[o]
-                              : (double)reinterpret_cast<const float*>(img.data())[o];
+// The sum of field f's interior cells of every instance, in a fixed order
+// (the same bits on every call): CTA i takes instance i, thread t the cells
+// t, t + 256, ... in (block, row, column) order, then a fixed shuffle tree
+// and the warps in order.
+template <class T>
+__global__ void __launch_bounds__(256) instance_field_sum_kernel(const T* __restrict__ arena, int64_t slab_stride,
+                                                                 int bpi, int n0, int n1, int f, double* out) {
+    const int64_t per_block = (int64_t)n0 * n1, cells = per_block * bpi;
+    const T* base = arena + (int64_t)blockIdx.x * bpi * 2 * slab_stride;
+    double s = 0.0;
+    for (int64_t c = threadIdx.x; c < cells; c += blockDim.x) {
+        const int b = (int)(c / per_block);
+        const int rem = (int)(c - (int64_t)b * per_block);
+        const int y = rem / n0, x = rem - y * n0;
+        s += (double)base[((int64_t)b * 2 + f) * slab_stride + (x + 1) + (int64_t)(y + 1) * (n0 + 2)];
+    }
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    __shared__ double w[8];
+    if ((threadIdx.x & 31) == 0) w[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int k = 0; k < (int)(blockDim.x >> 5); ++k) t += w[k];
+        out[blockIdx.x] = t;
+    }
+}
+
+// interior rows of one field of every instance, from a host image of the
+// arena into the instance-major, row-major host layout
+template <class T>
+void gather_rows(const lg_ensemble* e, const std::vector<char>& img, int f, double* host) {
+    const T* a = reinterpret_cast<const T*>(img.data());
+    for (int64_t i = 0; i < e->ninst; ++i)
+        for (int by = 0; by < e->nb1; ++by)
+            for (int bx = 0; bx < e->nb0; ++bx) {
+                const int64_t b = i * e->bpi + bx + (int64_t)by * e->nb0;
+                const T* slab = a + (b * 2 + f) * e->slab_stride;
+                for (int y = 0; y < e->n1; ++y) {
+                    const T* src = slab + 1 + (int64_t)(y + 1) * (e->n0 + 2);
+                    double* dst = host + (i * e->N1 + (int64_t)by * e->n1 + y) * e->N0 + (int64_t)bx * e->n0;
+                    for (int x = 0; x < e->n0; ++x) dst[x] = (double)src[x];
+                }
+            }
 }
 
 }  // namespace
@@ -342,10 +384,10 @@ int lg_ensemble_download(lg_ensemble* e, int field, double* host, int64_t n) {
     std::vector<char> img(state_bytes(e));
     ENS_CUDA(e, cudaMemcpyAsync(img.data(), e->state[e->cur], img.size(), cudaMemcpyDeviceToHost, st));
     ENS_CUDA(e, cudaStreamSynchronize(st));
-    for (int64_t i = 0; i < e->ninst; ++i)
-        for (int Y = 0; Y < e->N1; ++Y)
-            for (int X = 0; X < e->N0; ++X)
-                host[(i * e->N1 + Y) * e->N0 + X] = host_value(e, img, slab_index(e, i, X, Y, field));
+    if (e->dtype == LG_F64)
+        gather_rows<double>(e, img, field, host);
+    else
+        gather_rows<float>(e, img, field, host);
     return LG_OK;
 }
 
@@ -444,6 +486,7 @@ int lg_ensemble_value_and_grad(lg_ensemble* e, double dt, int64_t nsteps, int64_
         for (void*& q : e->adj) ENS_CUDA(e, cudaMalloc(&q, state_bytes(e)));
         ENS_CUDA(e, cudaMalloc(&e->d_loss, loss_n * sizeof(double)));
         ENS_CUDA(e, cudaMalloc(&e->d_target, cells * sizeof(double)));
+        ENS_CUDA(e, cudaMalloc(&e->d_usum, e->ninst * sizeof(double)));
     }
     if (e->acc_cap < acc_n) {
         cudaFree(e->d_acc);
@@ -522,16 +565,38 @@ int lg_ensemble_value_and_grad(lg_ensemble* e, double dt, int64_t nsteps, int64_
     }
     // the device time slot of the state holds the state's time again
     ENS_CUDA(e, cudaMemcpyAsync(e->d_t + e->tslot, &e->t, sizeof(double), cudaMemcpyHostToDevice, st));
-    // results
-    std::vector<double> acc((size_t)acc_n), lossv((size_t)loss_n);
+    // results: the parameter partials, the loss, the Delta gradient as the
+    // device's fixed-order sum of the u cotangents (u_0 = -Delta on every
+    // cell); the cell cotangents cross to the host only when asked for
+    if (e->dtype == LG_F64)
+        instance_field_sum_kernel<double><<<(unsigned)e->ninst, 256, 0, st>>>(
+            static_cast<const double*>(e->adj[a]), e->slab_stride, e->bpi, e->n0, e->n1, 1, e->d_usum);
+    else
+        instance_field_sum_kernel<float><<<(unsigned)e->ninst, 256, 0, st>>>(
+            static_cast<const float*>(e->adj[a]), e->slab_stride, e->bpi, e->n0, e->n1, 1, e->d_usum);
+    lg::abi_count_launch(e->ctx, 1);
+    ENS_CUDA(e, cudaGetLastError());
+    std::vector<double> acc((size_t)acc_n), lossv((size_t)loss_n), usum((size_t)e->ninst);
     ENS_CUDA(e, cudaMemcpyAsync(acc.data(), e->d_acc, acc_n * sizeof(double), cudaMemcpyDeviceToHost, st));
     ENS_CUDA(e, cudaMemcpyAsync(lossv.data(), e->d_loss, loss_n * sizeof(double), cudaMemcpyDeviceToHost, st));
-    std::vector<char> img(state_bytes(e));
-    ENS_CUDA(e, cudaMemcpyAsync(img.data(), e->adj[a], img.size(), cudaMemcpyDeviceToHost, st));
+    ENS_CUDA(e, cudaMemcpyAsync(usum.data(), e->d_usum, e->ninst * sizeof(double), cudaMemcpyDeviceToHost, st));
+    std::vector<char> img;
+    if (grad_phi0 || grad_u0) {
+        img.resize(state_bytes(e));
+        ENS_CUDA(e, cudaMemcpyAsync(img.data(), e->adj[a], img.size(), cudaMemcpyDeviceToHost, st));
+    }
     ENS_CUDA(e, cudaStreamSynchronize(st));
+    for (int f = 0; f < 2; ++f) {
+        double* dst = f == 0 ? grad_phi0 : grad_u0;
+        if (!dst) continue;
+        if (e->dtype == LG_F64)
+            gather_rows<double>(e, img, f, dst);
+        else
+            gather_rows<float>(e, img, f, dst);
+    }
     const int64_t acc_tiles = acc_n / 3 / e->ninst, loss_tiles = loss_n / e->ninst;
     for (int64_t i = 0; i < e->ninst; ++i) {  // fixed summation order: reproducible
-        double l = 0.0, g0 = 0.0, g1 = 0.0, g2 = 0.0, gd = 0.0;
+        double l = 0.0, g0 = 0.0, g1 = 0.0, g2 = 0.0;
         for (int64_t k = 0; k < loss_tiles; ++k) l += lossv[(size_t)(i * loss_tiles + k)];
         for (int64_t k = 0; k < acc_tiles; ++k) {
             const double* q = &acc[(size_t)(3 * (i * acc_tiles + k))];
@@ -539,14 +604,7 @@ int lg_ensemble_value_and_grad(lg_ensemble* e, double dt, int64_t nsteps, int64_
             g1 += q[1];
             g2 += q[2];
         }
-        for (int Y = 0; Y < e->N1; ++Y)
-            for (int X = 0; X < e->N0; ++X) {
-                const double pb = host_value(e, img, slab_index(e, i, X, Y, 0));
-                const double ub = host_value(e, img, slab_index(e, i, X, Y, 1));
-                gd -= ub;  // u_0 = -Delta on every cell
-                if (grad_phi0) grad_phi0[(i * e->N1 + Y) * e->N0 + X] = pb;
-                if (grad_u0) grad_u0[(i * e->N1 + Y) * e->N0 + X] = ub;
-            }
+        const double gd = -usum[(size_t)i];
         loss[i] = l;
         grad_params[4 * i + 0] = g0;
         grad_params[4 * i + 1] = g1;
