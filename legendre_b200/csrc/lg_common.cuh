@@ -62,14 +62,95 @@ __host__ __device__ __forceinline__ double unit_open(uint64_t bits) {
 
 constexpr double kTau = 6.283185307179586476925286766559;
 
-// Box-Muller cosine branch from one key (src/util/rng.rs:43-49).  Device
-// log/cos are within 2 ulp of glibc; the integer stream is exact.
+// ln u for the Box-Muller radius, u in [2^-53, 1], to about 1e-15 relative
+// (table-free, division-light; the Gaussian is held to 1e-12 of glibc's).
+// u = 2^e f with f in [sqrt(1/2), sqrt(2)): ln u = e ln 2 + 2 atanh(s),
+// s = (f - 1)/(f + 1), |s| <= 0.1716, by the atanh Taylor series to s^19
+// (truncation below 2e-15 of the sum).  f - 1 is exact (Sterbenz); s comes
+// from the hardware's approximate reciprocal, two Newton steps and one
+// residual correction of the quotient; ln 2 is split so that e ln2_hi is
+// exact for every exponent here.  u = 1 gives exactly 0.
+__device__ __forceinline__ double log_unit_interval(double u) {
+    const long long bu = __double_as_longlong(u);
+    int e = (int)((bu >> 52) & 0x7ff) - 1023;
+    double f = __longlong_as_double((bu & 0x000fffffffffffffLL) | 0x3ff0000000000000LL);
+    if (f > 1.4142135623730951) {
+        f = 0.5 * f;
+        e += 1;
+    }
+    const double num = f - 1.0, den = f + 1.0;
+    double r;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(den));
+    r = fma(r, fma(-den, r, 1.0), r);
+    r = fma(r, fma(-den, r, 1.0), r);
+    const double q0 = num * r;
+    const double s = fma(fma(-den, q0, num), r, q0);
+    const double z = s * s;
+    double p = 1.0 / 19.0;
+    p = fma(p, z, 1.0 / 17.0);
+    p = fma(p, z, 1.0 / 15.0);
+    p = fma(p, z, 1.0 / 13.0);
+    p = fma(p, z, 1.0 / 11.0);
+    p = fma(p, z, 1.0 / 9.0);
+    p = fma(p, z, 1.0 / 7.0);
+    p = fma(p, z, 1.0 / 5.0);
+    p = fma(p, z, 1.0 / 3.0);
+    const double t = 2.0 * s;
+    const double lnf = fma(t * z, p, t);
+    const double ln2_hi = 0x1.62e42fefa3800p-1, ln2_lo = 0x1.ef35793c76730p-45;
+    return fma((double)e, ln2_hi, fma((double)e, ln2_lo, lnf));
+}
+
+// cos x for the Box-Muller angle, x = fl(2 pi v) in (0, 2 pi], to about
+// 1e-15 relative also next to the zeros of cos: Cody-Waite reduction
+// r = x - k pi/2 with pi/2 in three parts (the first two of 33 bits, so
+// k C1 and k C2 are exact and the two leading subtractions cancel exactly),
+// then the sine or cosine Taylor polynomial of r (|r| <= pi/4, truncated at
+// r^15 / r^16) and the quadrant's sign.
+__device__ __forceinline__ double cos_full_turn(double x) {
+    const double t = x * 0x1.45f306dc9c883p-1;  // x 2/pi
+    const double magic = 0x1.8p52;               // t + magic rounds t to an integer (ties to even)
+    const double kq = t + magic;
+    const int q = __double2loint(kq) & 3;
+    const double kd = kq - magic;
+    double r = fma(-kd, 0x1.921fb544p+0, x);
+    r = fma(-kd, 0x1.0b4611a6p-34, r);
+    r = fma(-kd, 0x1.3198a2e037073p-69, r);
+    const double z = r * r;
+    double v;
+    if (q & 1) {  // r - r^3/3! + r^5/5! - ... to r^15
+        double sp = 1.0 / 1307674368000.0;
+        sp = fma(sp, z, -1.0 / 6227020800.0);
+        sp = fma(sp, z, 1.0 / 39916800.0);
+        sp = fma(sp, z, -1.0 / 362880.0);
+        sp = fma(sp, z, 1.0 / 5040.0);
+        sp = fma(sp, z, -1.0 / 120.0);
+        sp = fma(sp, z, 1.0 / 6.0);
+        v = fma(-(r * z), sp, r);
+    } else {  // 1 - r^2/2! + r^4/4! - ... to r^16
+        double cp = 1.0 / 20922789888000.0;
+        cp = fma(cp, z, -1.0 / 87178291200.0);
+        cp = fma(cp, z, 1.0 / 479001600.0);
+        cp = fma(cp, z, -1.0 / 3628800.0);
+        cp = fma(cp, z, 1.0 / 40320.0);
+        cp = fma(cp, z, -1.0 / 720.0);
+        cp = fma(cp, z, 1.0 / 24.0);
+        cp = fma(cp, z, -0.5);
+        v = fma(z, cp, 1.0);
+    }
+    return (q == 1 || q == 2) ? -v : v;
+}
+
+// Box-Muller cosine branch from one key (src/util/rng.rs:43-49): the
+// integer stream and the uniforms are exact; the transcendental factors
+// (log_unit_interval, cos_full_turn and the square root) are within about
+// 1e-15 of glibc's, the Gaussian within 1e-12 relative as required.
 __device__ __forceinline__ double standard_normal(uint64_t key) {
     uint64_t a = splitmix64(key);
     uint64_t b = splitmix64(a ^ 0xD1B54A32D192ED03ull);
     double u = unit_open(a);
     double v = unit_open(b);
-    return sqrt(-2.0 * log(u)) * cos(kTau * v);
+    return sqrt(-2.0 * log_unit_interval(u)) * cos_full_turn(kTau * v);
 }
 
 // Single-precision Gaussian from the same two uniforms, for the FP32 path.

@@ -330,3 +330,49 @@ def test_modelc_work_list_across_runs_and_graphs(sched, orc, variant):
         sims.append(sim)
     for f in ("phi", "u"):
         assert np.array_equal(sims[0].state.download(f), sims[1].state.download(f))
+
+
+_M64 = (1 << 64) - 1
+
+
+def _unxorshift(y, s):
+    z = y
+    for _ in range(64 // s + 1):
+        z = y ^ (z >> s)
+    return z & _M64
+
+
+def _splitmix64_inverse(y):
+    """The key whose SplitMix64 output is y (each step of the finalizer is a
+    bijection of 64-bit words)."""
+    z = _unxorshift(y, 31)
+    z = (z * pow(0x94D049BB133111EB, -1, 1 << 64)) & _M64
+    z = _unxorshift(z, 27)
+    z = (z * pow(0xBF58476D1CE4E5B9, -1, 1 << 64)) & _M64
+    z = _unxorshift(z, 30)
+    return (z - 0x9E3779B97F4A7C15) & _M64
+
+
+def test_standard_normal_within_1e12_at_the_hard_arguments(sched, orc):
+    """Keys chosen through the inverse generator so that the radius uniform u
+    sits next to 1 (ln u tiny) and the angle uniform v next to 1/4, 1/2, 3/4
+    and 1 (cos(2 pi v) next to its zeros and extremes)."""
+    from legendre_b200.rng import splitmix64
+
+    assert all(splitmix64(_splitmix64_inverse(y)) == y for y in (0, 1, 2**63, _M64, 0x123456789ABCDEF))
+    keys = []
+    for m in range(1, 2000):  # u = 1 - m 2^-53: a's top 53 bits near all ones
+        keys.append(_splitmix64_inverse(((1 << 53) - m) << 11))
+    for center in (1 << 51, 1 << 52, 3 << 51, (1 << 53) - 1):  # v near 1/4, 1/2, 3/4, 1
+        for d in range(-300, 300):
+            b = ((center + d) % (1 << 53)) << 11
+            a = _splitmix64_inverse(b) ^ 0xD1B54A32D192ED03
+            keys.append(_splitmix64_inverse(a))
+    keys = np.array(keys, dtype=np.uint64)
+    import ctypes as C
+    out = np.empty(keys.size)
+    L._native.check(L._native.lib.lg_standard_normal(sched.handle, keys.ctypes.data_as(C.POINTER(C.c_uint64)),
+                                                     keys.size, out.ctypes.data_as(C.POINTER(C.c_double))),
+                    sched.handle)
+    ref = orc.standard_normal(keys)
+    assert np.all(np.abs(out - ref) <= 1e-12 * np.abs(ref)), np.max(np.abs(out - ref) / np.abs(ref))
