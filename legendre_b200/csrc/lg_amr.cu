@@ -594,8 +594,15 @@ struct lg_amr_sim {
     int* d_err = nullptr;
     long long barrier_spin_limit = 4000000;  // polls of >= 128 ns: well over a second
     int coop_grid[2] = {0, 0};  // per model kind (noise-free / noisy) once measured
-    std::vector<double> host_old, host_new;  // regrid staging
+    std::vector<double> host_old, host_new;  // host staging of whole states (get/set)
     std::vector<TileShape> tile_shapes;      // per level
+    // regrid migration on the device: the old state's image and the old
+    // hierarchy's patch tables (grow-only)
+    double* d_mig_old = nullptr;
+    int64_t mig_old_cap = 0;
+    char* d_mig_tab = nullptr;
+    size_t mig_tab_cap = 0;
+    int* d_mig_err = nullptr;
 };
 
 namespace {
@@ -1189,11 +1196,223 @@ std::vector<Ptr> slab_ptrs(const lg::amr::Plans& P, Vec& base, int64_t first, in
     return out;
 }
 
+// ------------------------------------------------- migration on the device
+// BergerOliger::migrate / sample (adapt.rs:323-402) evaluated for every
+// interior cell of the new hierarchy's refined blocks, from an image of the
+// old state: a cell covered by an old patch of its level takes that value;
+// otherwise the bilinear fold, from zero and in corner order, of the four
+// coarser cells around it (reflected into the coarser domain), each sampled
+// the same way -- the recursion ends at level 0, which covers everything.
+// The expressions and their order are the host restatement's (compiled
+// without contraction), so the migrated state is the same bits.
+struct MigPatch {
+    int64_t lo[2], hi[2];
+    int64_t off;     // field 0's slab in the old image
+    int64_t stride;  // between fields
+};
+struct MigLevel {
+    int64_t dom[2];       // the level's domain [0, dom)
+    int64_t side, nbx;    // the old layout's bucket index of the level
+    int64_t s0, i0;       // its bucket starts and items in the shared arrays
+    double ratio_below;   // refinement ratio between this level and the next coarser one
+};
+struct MigBlock {  // one refined block of the new hierarchy
+    int64_t lo[2];
+    int nx, ny, level, pad;
+    int64_t off, stride;  // its slabs in the new arena
+};
+struct MigArgs {
+    const double* old;
+    const MigPatch* patches;
+    const MigLevel* levels;
+    const uint32_t* starts;
+    const uint32_t* items;
+    int old_levels;
+    const MigBlock* blocks;
+    int nblocks;
+    double* out;
+    int nfields;
+    int* err;  // set when a sample found no level-0 block (not expected)
+};
+
+__device__ __forceinline__ int mig_find(const MigArgs& a, int level, int64_t x, int64_t y) {
+    if (level >= a.old_levels) return -1;
+    const MigLevel& L = a.levels[level];
+    if (x < 0 || y < 0 || x >= L.dom[0] || y >= L.dom[1]) return -1;
+    const int64_t k = x / L.side + (y / L.side) * L.nbx;
+    for (uint32_t q = a.starts[L.s0 + k]; q < a.starts[L.s0 + k + 1]; ++q) {
+        const uint32_t b = a.items[L.i0 + q];
+        const MigPatch& P = a.patches[b];
+        if (P.lo[0] <= x && x < P.hi[0] && P.lo[1] <= y && y < P.hi[1]) return (int)b;
+    }
+    return -1;
+}
+
+__device__ __forceinline__ int64_t mig_reflect(int64_t c, int64_t lo, int64_t hi) {
+    if (c < lo) return 2 * lo - 1 - c;
+    if (c >= hi) return 2 * hi - 1 - c;
+    return c;
+}
+
+template <int DEPTH>
+__device__ double mig_sample(const MigArgs& a, int level, int64_t x, int64_t y, int f) {
+    const int b = mig_find(a, level, x, y);
+    if (b >= 0) {
+        const MigPatch& P = a.patches[b];
+        return a.old[P.off + (int64_t)f * P.stride + (x - P.lo[0] + 1) + (y - P.lo[1] + 1) * (P.hi[0] - P.lo[0] + 2)];
+    }
+    if constexpr (DEPTH == 0) {
+        atomicExch(a.err, 1);
+        return 0.0;
+    } else {
+        if (level == 0) {
+            atomicExch(a.err, 1);
+            return 0.0;
+        }
+        const double r = a.levels[level].ratio_below;
+        const int64_t cdx = a.levels[level - 1].dom[0], cdy = a.levels[level - 1].dom[1];
+        const int64_t cell[2] = {x, y};
+        int64_t c0[2];
+        double w[2];
+        for (int d = 0; d < 2; ++d) {
+            const double pc = ((double)cell[d] + 0.5) / r - 0.5;
+            const double fl = floor(pc);
+            c0[d] = (int64_t)fl;
+            w[d] = pc - fl;
+        }
+        double acc = 0.0;
+#pragma unroll 1
+        for (unsigned corner = 0; corner < 4; ++corner) {
+            int64_t cc[2] = {c0[0], c0[1]};
+            double weight = 1.0;
+            for (int d = 0; d < 2; ++d) {
+                if ((corner >> d) & 1) {
+                    cc[d] += 1;
+                    weight *= w[d];
+                } else {
+                    weight *= 1.0 - w[d];
+                }
+            }
+            if (weight == 0.0) continue;
+            cc[0] = mig_reflect(cc[0], 0, cdx);
+            cc[1] = mig_reflect(cc[1], 0, cdy);
+            acc += mig_sample<DEPTH - 1>(a, level - 1, cc[0], cc[1], f) * weight;
+        }
+        return acc;
+    }
+}
+
+__global__ void __launch_bounds__(256) amr_migrate_kernel(MigArgs a) {
+    for (int bi = blockIdx.x; bi < a.nblocks; bi += gridDim.x) {
+        const MigBlock B = a.blocks[bi];
+        for (int c = threadIdx.x; c < B.nx * B.ny; c += blockDim.x) {
+            const int i = c % B.nx, j = c / B.nx;
+            const int64_t o = B.off + (i + 1) + (int64_t)(j + 1) * (B.nx + 2);
+            for (int f = 0; f < a.nfields; ++f)
+                a.out[o + (int64_t)f * B.stride] = mig_sample<kMaxDepth - 1>(a, B.level, B.lo[0] + i, B.lo[1] + j, f);
+        }
+    }
+}
+
+// Copy the old state into the migration image (each level's slabs from its
+// current buffer, at the old plans' offsets) and upload the old hierarchy's
+// patch tables and the new hierarchy's refined blocks; fills the kernel
+// arguments but the output arena.
+int prepare_migration(lg_amr_sim* s, const lg::amr::Layout& ng, const lg::amr::Plans& np, MigArgs* a) {
+    cudaStream_t st = lg::abi_stream(s->ctx);
+    const lg::amr::Layout& g = s->layout;
+    const int64_t elems = s->plans.arena_elems;
+    if (elems > s->mig_old_cap) {
+        cudaFree(s->d_mig_old);
+        s->d_mig_old = nullptr;
+        s->mig_old_cap = 0;
+        const int64_t cap = elems + elems / 4;
+        AMR_CUDA(s, cudaMalloc(&s->d_mig_old, (size_t)cap * sizeof(double)));
+        s->mig_old_cap = cap;
+    }
+    for (int l = 0; l < g.num_levels(); ++l) {
+        const auto r = level_range(s, l);
+        if (r.second > r.first)
+            AMR_CUDA(s, cudaMemcpyAsync(s->d_mig_old + r.first, s->arena[s->cur[l]] + r.first,
+                                        (size_t)(r.second - r.first) * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    }
+    std::vector<MigPatch> patches((size_t)g.num_blocks());
+    for (int b = 0; b < g.num_blocks(); ++b) {
+        const auto& bx = g.patches[(size_t)b].bx;
+        patches[(size_t)b] = MigPatch{{bx.lo[0], bx.lo[1]}, {bx.hi[0], bx.hi[1]}, s->plans.blocks[(size_t)b].off,
+                                      s->plans.blocks[(size_t)b].stride};
+    }
+    // every level the hierarchy may hold (a regrid can add one): domains and
+    // ratios for all, bucket indices for the old layout's levels
+    std::vector<MigLevel> levels((size_t)g.max_levels());
+    std::vector<uint32_t> starts, items;
+    for (int l = 0; l < g.max_levels(); ++l) {
+        const auto d = g.domain(l);
+        MigLevel L{{d.hi[0], d.hi[1]}, 1, 0, 0, 0, l > 0 ? (double)g.ratios[(size_t)l - 1] : 1.0};
+        if (l < g.num_levels()) {
+            const auto& ix = g.index[(size_t)l];
+            L.side = ix.side;
+            L.nbx = ix.nbx;
+            L.s0 = (int64_t)starts.size();
+            L.i0 = (int64_t)items.size();
+            starts.insert(starts.end(), ix.start.begin(), ix.start.end());
+            items.insert(items.end(), ix.items.begin(), ix.items.end());
+        }
+        levels[(size_t)l] = L;
+    }
+    std::vector<MigBlock> blocks;
+    for (uint32_t b = ng.num_levels() > 1 ? ng.level_start[1] : (uint32_t)ng.num_blocks(); b < (uint32_t)ng.num_blocks();
+         ++b) {
+        const auto& bx = ng.patches[b].bx;
+        const auto& d = np.blocks[b];
+        blocks.push_back(MigBlock{{bx.lo[0], bx.lo[1]}, d.nx, d.ny, ng.patches[b].level, 0, d.off, d.stride});
+    }
+    size_t off = 0;
+    auto reserve = [&](size_t bytes) {
+        const size_t o = off;
+        off += (bytes + 255) / 256 * 256;
+        return o;
+    };
+    const size_t o_p = reserve(patches.size() * sizeof(MigPatch)), o_l = reserve(levels.size() * sizeof(MigLevel)),
+                 o_s = reserve(starts.size() * sizeof(uint32_t)), o_i = reserve(std::max<size_t>(1, items.size()) * 4),
+                 o_b = reserve(blocks.size() * sizeof(MigBlock));
+    std::vector<char> blob(std::max<size_t>(off, 256), 0);
+    if (!blocks.empty()) std::memcpy(blob.data() + o_b, blocks.data(), blocks.size() * sizeof(MigBlock));
+    std::memcpy(blob.data() + o_p, patches.data(), patches.size() * sizeof(MigPatch));
+    std::memcpy(blob.data() + o_l, levels.data(), levels.size() * sizeof(MigLevel));
+    std::memcpy(blob.data() + o_s, starts.data(), starts.size() * sizeof(uint32_t));
+    if (!items.empty()) std::memcpy(blob.data() + o_i, items.data(), items.size() * sizeof(uint32_t));
+    if (blob.size() > s->mig_tab_cap) {
+        cudaFree(s->d_mig_tab);
+        s->d_mig_tab = nullptr;
+        s->mig_tab_cap = 0;
+        const size_t cap = blob.size() + blob.size() / 4;
+        AMR_CUDA(s, cudaMalloc(&s->d_mig_tab, cap));
+        s->mig_tab_cap = cap;
+    }
+    if (!s->d_mig_err) AMR_CUDA(s, cudaMalloc(&s->d_mig_err, sizeof(int)));
+    AMR_CUDA(s, cudaMemsetAsync(s->d_mig_err, 0, sizeof(int), st));
+    AMR_CUDA(s, cudaMemcpyAsync(s->d_mig_tab, blob.data(), blob.size(), cudaMemcpyHostToDevice, st));
+    // the host blob must outlive the copy
+    AMR_CUDA(s, cudaStreamSynchronize(st));
+    a->old = s->d_mig_old;
+    a->patches = (const MigPatch*)(s->d_mig_tab + o_p);
+    a->levels = (const MigLevel*)(s->d_mig_tab + o_l);
+    a->starts = (const uint32_t*)(s->d_mig_tab + o_s);
+    a->items = (const uint32_t*)(s->d_mig_tab + o_i);
+    a->old_levels = g.num_levels();
+    a->blocks = (const MigBlock*)(s->d_mig_tab + o_b);
+    a->nblocks = (int)blocks.size();
+    a->nfields = s->nfields;
+    a->err = s->d_mig_err;
+    return LG_OK;
+}
+
 // BergerOliger::regrid (adapt.rs:152-237): prepare (restrict + fill of the
 // tagged field), tag every level on the device, build boxes on the host,
 // keep the hierarchy if acceptable, else rebuild and migrate.  The level-0
-// slabs stay on the device (the base tiling never changes); refined levels
-// are sampled on the host from one download of the state.
+// slabs stay where they are (the base tiling never changes); the refined
+// levels are sampled on the device from an image of the old state.
 int maybe_regrid(lg_amr_sim* s) {
     if (!s->has_policy || s->step_index % s->policy.every != 0) return LG_OK;
     const int f = s->policy.field;
@@ -1221,70 +1440,28 @@ int maybe_regrid(lg_amr_sim* s) {
     shapes[0] = s->tile_shapes[0];  // level 0's plans are kept
     lg::amr::Plans np = lg::amr::build_plans(ng, s->nfields, 1024, 1, rows_of(shapes));
     if (!np.error.empty()) return fail(s, LG_ERR_STATE, np.error);
-    // download the slabs the sampling can reach: every refined slab, and the
-    // level-0 blocks within two coarse cells of a new level-1 patch (all of
-    // them, should the sampling still miss one)
-    std::vector<char> want(s->layout.num_blocks(), 0);
-    for (uint32_t b = s->layout.level_start[1]; b < (uint32_t)s->layout.num_blocks(); ++b) want[b] = 1;
-    {
-        const auto& base = s->layout.base;
-        const int64_t nbx = base.cells[0] / base.block[0], nby = base.cells[1] / base.block[1];
-        const int64_t r = ng.num_levels() > 1 ? ng.ratios[0] : 1;
-        for (uint32_t b = ng.num_levels() > 1 ? ng.level_start[1] : 0; ng.num_levels() > 1 && b < ng.level_start[2];
-             ++b) {
-            const auto& bx = ng.patches[b].bx;
-            int64_t lo[2], hi[2];
-            for (int d = 0; d < 2; ++d) {
-                lo[d] = std::max<int64_t>(0, bx.lo[d] / r - 2) / base.block[d];
-                hi[d] = std::min<int64_t>(base.cells[d] - 1, (bx.hi[d] + r - 1) / r + 1) / base.block[d];
-            }
-            for (int64_t by = lo[1]; by <= hi[1] && by < nby; ++by)
-                for (int64_t bx2 = lo[0]; bx2 <= hi[0] && bx2 < nbx; ++bx2) want[(size_t)(bx2 + by * nbx)] = 1;
-        }
-    }
-    s->host_old.resize((size_t)s->plans.arena_elems);
-    int rc = LG_OK;
-    for (int attempt = 0; attempt < 2; ++attempt) {
-        cudaStream_t st = lg::abi_stream(s->ctx);
-        const int nb = s->layout.num_blocks();
-        for (int b = 0; b < nb;) {  // runs of wanted blocks of one level are contiguous in the arena
-            if (!want[b]) {
-                ++b;
-                continue;
-            }
-            int e = b;
-            while (e + 1 < nb && want[e + 1] && s->plans.blocks[e + 1].level == s->plans.blocks[b].level) ++e;
-            const auto& first = s->plans.blocks[b];
-            const auto& last = s->plans.blocks[e];
-            const int64_t a0 = first.off, a1 = last.off + last.stride * s->nfields;
-            AMR_CUDA(s, cudaMemcpyAsync(s->host_old.data() + a0, s->arena[s->cur[first.level]] + a0,
-                                        (size_t)(a1 - a0) * sizeof(double), cudaMemcpyDeviceToHost, st));
-            b = e + 1;
-        }
-        AMR_CUDA(s, cudaStreamSynchronize(st));
-        const int64_t l0 = level0_elems(s);
-        s->host_new.assign((size_t)(np.arena_elems - l0), 0.0);
-        bool complete = true;
-        for (int k = 0; k < s->nfields; ++k) {
-            auto old = slab_ptrs<const double*>(s->plans, s->host_old, 0, k);
-            for (int b = 0; b < nb; ++b)
-                if (!want[b]) old[b] = nullptr;
-            const auto out = slab_ptrs<double*>(np, s->host_new, l0, k);
-            complete = complete && lg::amr::migrate_field(s->layout, old, ng, out, false);
-        }
-        if (complete) break;
-        if (attempt == 1) return fail(s, LG_ERR_STATE, "migration needs a slab that was not downloaded");
-        std::fill(want.begin(), want.end(), 1);
-    }
+    // the old state's image and tables, then the new arenas (level 0 keeps
+    // its slabs), zeroed refined slabs and one migration launch
+    MigArgs ma{};
+    int rc = prepare_migration(s, ng, np, &ma);
+    if (rc != LG_OK) return rc;
     const int64_t l0 = level0_elems(s);
     int keep = 0;
     rc = ensure_arenas(s, np.arena_elems, l0, s->cur[0], &keep);
     if (rc != LG_OK) return rc;
-    if (!s->host_new.empty()) {
+    if (np.arena_elems > l0) {
         cudaStream_t st = lg::abi_stream(s->ctx);
-        AMR_CUDA(s, cudaMemcpyAsync(s->arena[keep] + l0, s->host_new.data(), s->host_new.size() * sizeof(double),
-                                    cudaMemcpyHostToDevice, st));
+        AMR_CUDA(s, cudaMemsetAsync(s->arena[keep] + l0, 0, (size_t)(np.arena_elems - l0) * sizeof(double), st));
+        ma.out = s->arena[keep];
+        if (ma.nblocks > 0) {
+            amr_migrate_kernel<<<(unsigned)std::min(ma.nblocks, 65535), 256, 0, st>>>(ma);
+            lg::abi_count_launch(s->ctx, 1);
+            AMR_CUDA(s, cudaGetLastError());
+        }
+        int merr = 0;
+        AMR_CUDA(s, cudaMemcpyAsync(&merr, s->d_mig_err, sizeof merr, cudaMemcpyDeviceToHost, st));
         AMR_CUDA(s, cudaStreamSynchronize(st));
+        if (merr) return fail(s, LG_ERR_STATE, "migration found a cell outside every level-0 block");
     }
     s->layout = std::move(ng);
     s->plans = std::move(np);
@@ -1393,6 +1570,9 @@ int lg_amr_sim_destroy(lg_amr_sim* s) {
     cudaFree(s->d_err);
     cudaFree(s->d_tags);
     cudaFree(s->d_count);
+    cudaFree(s->d_mig_old);
+    cudaFree(s->d_mig_tab);
+    cudaFree(s->d_mig_err);
     delete s;
     return LG_OK;
 }

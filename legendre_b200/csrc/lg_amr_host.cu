@@ -3,8 +3,6 @@
 #include <cmath>
 #include <cstdlib>
 #include <system_error>
-#include <thread>
-#include <unordered_map>
 
 #include "../../include/legendre_b200.h"
 #include "lg_amr_host.h"
@@ -524,121 +522,6 @@ Plans build_plans(const Layout& g, int nfields, int unit_cells, int first_level,
     }
     P.unit_start.push_back((int64_t)P.units.size());
     return P;
-}
-
-// ----------------------------------------------------------- migrate -----
-namespace {
-
-// sample (adapt.rs:323-402) with the bilinear values of the coarser cells it
-// recurses into memoised: sample is a pure function of (level, cell), and
-// neighbouring fine cells share coarse corners.
-struct Sampler {
-    const Layout& g;
-    const std::vector<const double*>& s;
-    std::vector<std::unordered_map<uint64_t, double>> memo;
-    std::vector<int> last;  // per level, the patch of the previous hit (patches of a level are disjoint)
-    bool missing = false;
-
-    Sampler(const Layout& g_, const std::vector<const double*>& s_)
-        : g(g_), s(s_), memo(g_.max_levels()), last(g_.max_levels(), -1) {}
-
-    double at(int level, int64_t x, int64_t y, bool keep) {
-        if (level < g.num_levels()) {
-            int b = last[level];
-            if (b < 0 || !g.patches[b].bx.contains(x, y)) {
-                b = g.find(level, x, y);
-                if (b >= 0) last[level] = b;
-            }
-            if (b >= 0) {
-                if (!s[b]) {
-                    missing = true;
-                    return 0.0;
-                }
-                const Box& bx = g.patches[b].bx;
-                return s[b][(size_t)((x - bx.lo[0] + 1) + (y - bx.lo[1] + 1) * (bx.extent(0) + 2))];
-            }
-        }
-        const uint64_t key = ((uint64_t)x << 32) | (uint64_t)y;  // cells of a level domain: below 2^31
-        if (keep) {
-            auto it = memo[level].find(key);
-            if (it != memo[level].end()) return it->second;
-        }
-        const double r = (double)g.ratios[level - 1];
-        const Box cd = g.domain(level - 1);
-        const int64_t cell[2] = {x, y};
-        int64_t c0[2];
-        double w[2];
-        for (int d = 0; d < 2; ++d) {
-            const double pc = ((double)cell[d] + 0.5) / r - 0.5;
-            const double fl = std::floor(pc);
-            c0[d] = (int64_t)fl;
-            w[d] = pc - fl;
-        }
-        double acc = 0.0;
-        for (unsigned corner = 0; corner < 4; ++corner) {
-            int64_t cc[2] = {c0[0], c0[1]};
-            double weight = 1.0;
-            for (int d = 0; d < 2; ++d) {
-                if ((corner >> d) & 1) {
-                    cc[d] += 1;
-                    weight *= w[d];
-                } else {
-                    weight *= 1.0 - w[d];
-                }
-            }
-            if (weight == 0.0) continue;
-            for (int d = 0; d < 2; ++d) cc[d] = reflect(cc[d], cd.lo[d], cd.hi[d]);
-            acc += at(level - 1, cc[0], cc[1], true) * weight;
-        }
-        if (keep) memo[level].emplace(key, acc);
-        return acc;
-    }
-};
-
-}  // namespace
-
-bool migrate_field(const Layout& og, const std::vector<const double*>& old, const Layout& ng,
-                   const std::vector<double*>& out, bool copy_level0) {
-    if (copy_level0)  // the base tiling never changes
-        for (uint32_t b = ng.level_start[0]; b < ng.level_start[1]; ++b) {
-            const Box& bx = ng.patches[b].bx;
-            if (!old[b]) return false;
-            std::copy(old[b], old[b] + (size_t)(bx.extent(0) + 2) * (size_t)(bx.extent(1) + 2), out[b]);
-        }
-    // The refined blocks: each is sampled on its own (sample is a pure
-    // function of the old hierarchy), so blocks b0 + t, b0 + t + nt, ... go
-    // to thread t with its own memo, and the result is the same for any
-    // thread count.
-    const uint32_t b0 = ng.num_levels() > 1 ? ng.level_start[1] : (uint32_t)ng.num_blocks();
-    const uint32_t b1 = (uint32_t)ng.num_blocks();
-    uint64_t cells = 0;
-    for (uint32_t b = b0; b < b1; ++b) cells += ng.patches[b].bx.cells();
-    auto work = [&](unsigned t, unsigned nt, char* missing) {
-        Sampler smp(og, old);
-        for (uint32_t b = b0 + t; b < b1; b += nt) {
-            const int level = ng.patches[b].level;
-            const Box& bx = ng.patches[b].bx;
-            for (int64_t j = 0; j < bx.extent(1); ++j)
-                for (int64_t i = 0; i < bx.extent(0); ++i)
-                    out[b][(size_t)((i + 1) + (j + 1) * (bx.extent(0) + 2))] =
-                        smp.at(level, bx.lo[0] + i, bx.lo[1] + j, false);
-        }
-        *missing = smp.missing ? 1 : 0;
-    };
-    unsigned nt = std::min(std::max(1u, std::thread::hardware_concurrency()), 16u);
-    nt = (unsigned)std::min<uint64_t>(nt, std::max<uint64_t>(1, cells / 8192));  // >= 8192 cells a thread
-    std::vector<char> missing(nt, 0);
-    std::vector<std::thread> pool;
-    unsigned started = 1;
-    try {
-        for (; started < nt; ++started) pool.emplace_back(work, started, nt, &missing[started]);
-    } catch (const std::system_error&) {
-        // no more threads: this one takes the remaining shares
-    }
-    work(0, nt, &missing[0]);
-    for (unsigned t = started; t < nt; ++t) work(t, nt, &missing[t]);
-    for (std::thread& th : pool) th.join();
-    return std::find(missing.begin(), missing.end(), 1) == missing.end();
 }
 
 }  // namespace amr

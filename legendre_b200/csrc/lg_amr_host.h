@@ -155,14 +155,5 @@ struct Plans {
 Plans build_plans(const Layout& g, int nfields, int unit_cells, int first_level = 0,
                   const std::vector<int>& tile_rows = {});
 
-// migrate / sample (adapt.rs:323-402) on host slabs: old[b] / out[b] point
-// at the ghost-inclusive slabs of one field, block order.  Refined blocks'
-// interiors are sampled; level-0 slabs are copied verbatim when
-// `copy_level0` (the base tiling never changes, so a caller may move them
-// itself).  A null old[b] marks a slab the caller did not provide; the
-// function returns false if the sampling needed one.
-bool migrate_field(const Layout& og, const std::vector<const double*>& old, const Layout& ng,
-                   const std::vector<double*>& out, bool copy_level0);
-
 }  // namespace amr
 }  // namespace lg
