@@ -71,30 +71,32 @@ CONFIGS = {
 BYTES_PER_CELL = {"f64": 32, "f32": 16}  # read phi, u; write phi, u
 
 # DRAM bytes (read + write) per cell-update of the dominant kernel, from one
-# ncu capture each of the kernel as it now is (profiles/): the FP64 strip
-# kernel on 4096^2 (502 MB per 16.8M-cell launch) and the 3-D heat kernel on
-# 256^3 (319 MB per 16.8M cells; the 512^3 run has the same per-block work,
-# so its traffic scales with the cell count).  Other workloads, the FP32
-# strip kernel among them (its capture predates its rolled row loop),
-# report null.
-TRAFFIC_PER_CELL = {("c2", "f64"): 502.4e6 / 4096 ** 2, ("c1big", "f64"): 318.7e6 / 256 ** 3}
-
-
-# ncu pipe use of the dominant kernel, reported beside its HBM fraction (one
-# capture each, named after its summary in profiles/): issue slots and the
-# FP64 pipe, fractions of peak sustained while active.  The multi-grain
-# figures come from the same block shape on 5040^2.
-NCU_PIPES = {("c2", "f64"): {"issue_active": 0.682, "fp64_pipe": 0.388, "capture": "modelc_strip_f64_4096sq"},
-             ("c3o", "f64"): {"issue_active": 0.568, "fp64_pipe": 0.332,
-                              "capture": "modelc_oriented_f64_5040sq_126blocks"}}
+# ncu capture each of the kernel as it now is (the summaries under
+# profiles/ named in NCU_INST): the FP64 and FP32 strip kernels in the
+# variant the autotuner picks on 10080^2 (CAPTURED_VARIANT), captured on
+# 5040^2 of the same 126^2 blocks (833.3 MB and 375.4 MB per 25.4M-cell
+# launch), and the TMA-staged 3-D heat kernel on 256^3 (319.7 MB per 16.8M
+# cells; 512^3 has the same per-block work).  Traffic grows with the cell
+# count, so a launch of the full grid moves the per-cell figure times its
+# cells.  Other workloads report null.
+TRAFFIC_PER_CELL = {("c3", "f64"): 833.3e6 / 5040 ** 2, ("c3", "f32"): 375.4e6 / 5040 ** 2,
+                    ("c1big", "f64"): 319.7e6 / 256 ** 3}
 
 NOMINAL_HBM_GBS = 8000.0  # a B200's nominal HBM3e bandwidth, the second denominator
 
-# Instruction mix of the dominant kernel per cell-update, from one ncu capture
-# each (smsp__inst_executed and the fp64 pipe's share, x 32 threads per warp
-# instruction, divided by the launch's cell-updates); the capture named is
-# the summary under profiles/.  Filled for the configurations captured.
-NCU_INST = {}
+# Instruction mix of the dominant kernel per cell-update, from the same
+# captures (smsp__inst_executed and the fp64 pipe's share, x 32 threads per
+# warp instruction, divided by the launch's cell-updates); the capture named
+# is the summary under profiles/.
+NCU_INST = {("c3", "f64"): {"inst_per_cell": 487.5, "fp64_inst_per_cell": 141.0,
+                            "capture": "modelc_strip_f64_5040sq_126blocks"},
+            ("c3", "f32"): {"inst_per_cell": 285.2, "fp64_inst_per_cell": None,
+                            "capture": "modelc_strip_f32_5040sq_126blocks"},
+            ("c1big", "f64"): {"inst_per_cell": 103.7, "fp64_inst_per_cell": None,
+                               "capture": "heat3d_tma_256cube"}}
+
+# the strip-kernel variant the captures ran (the autotuner's choice on 10080^2)
+CAPTURED_VARIANT = 32015
 
 
 def compute_roofline(peaks, sm_mhz, cells_per_s, ncu):
@@ -122,8 +124,10 @@ def compute_roofline(peaks, sm_mhz, cells_per_s, ncu):
 
 def ncu_capture_config(args) -> bool:
     """True when the run is the configuration the ncu figures were taken on:
-    no size, noise, integrator or kernel-variant override."""
-    return args.cells is None and args.noise is None and args.integrator == "em" and args.variant in (0, 32002)
+    no size, noise, integrator or kernel-variant override (variant 0 runs the
+    autotuner's choice, which on the captured grids is CAPTURED_VARIANT)."""
+    return (args.cells is None and args.noise is None and args.integrator == "em"
+            and args.variant in (0, CAPTURED_VARIANT))
 
 
 def traffic(args, cells_per_step):
@@ -509,7 +513,11 @@ def run_other(args, cfg):
             "config": dict({"workload": cfg["workload"], "parallelism": f"replicas{world}", "graph": True}, **extra),
             "roofline": hbm_roofline(achieved, peak, peak_kind,
                                      traffic=traffic(args, cells) if cfg["kind"] == "heat" else None,
-                                     algorithmic_bytes_per_cell=bytes_per_cell),
+                                     algorithmic_bytes_per_cell=bytes_per_cell,
+                                     compute=compute_roofline(sched.compute_peaks(), clk.get("sm_mhz"),
+                                                              value * 1e9 / world,
+                                                              NCU_INST.get((args.config, "f64"))
+                                                              if ncu_capture_config(args) else None)),
             "cpu_baseline": None, "e2e": None,
             "gpu_launches": sched.kernel_launches - launches0,
             "clocks": {"sm_mhz": clk["sm_mhz"], "sm_max_mhz": clk["sm_max_mhz"], "reasons": clk["reasons"],
@@ -729,7 +737,6 @@ def model_c_line(args, cfg, world, ms, clk, launches, tuned, e2e, observed, err,
                    "graph": True, "variant": args.variant, "autotuned_variant": tuned},
         "roofline": hbm_roofline(achieved, peak, peak_kind, traffic=traffic(args, cells),
                                  algorithmic_bytes_per_cell=bpc,
-                                 ncu_pipes=NCU_PIPES.get((args.config, args.dtype)) if captured_cfg else None,
                                  compute=compute_roofline(compute_peaks, clk.get("sm_mhz"), value * 1e9 / world,
                                                           NCU_INST.get((args.config, args.dtype))
                                                           if captured_cfg else None)),

@@ -55,17 +55,20 @@ def test_roofline_object_carries_both_denominators_and_the_captured_figures():
     sys.path.insert(0, str(ROOT))
     import bench
 
-    a = types.SimpleNamespace(cells=None, noise=None, integrator="em", variant=0, config="c2", dtype="f64")
-    r = bench.hbm_roofline(1600.0, 6400.0, "measured", traffic=bench.traffic(a, 4096 ** 2),
+    a = types.SimpleNamespace(cells=None, noise=None, integrator="em", variant=0, config="c3", dtype="f64")
+    r = bench.hbm_roofline(1600.0, 6400.0, "measured", traffic=bench.traffic(a, 10080 ** 2),
                            algorithmic_bytes_per_cell=32)
     assert r["bound"] == "hbm" and r["unit"] == "GB/s"
     assert r["frac"] == 0.25 and r["frac_nominal"] == 1600.0 / 8000.0 and r["peak_kind"] == "measured"
-    assert r["traffic"] == bench.TRAFFIC_PER_CELL[("c2", "f64")] * 4096 ** 2
-    assert bench.NCU_PIPES[("c2", "f64")]["fp64_pipe"] > 0
+    assert r["traffic"] == bench.TRAFFIC_PER_CELL[("c3", "f64")] * 10080 ** 2
+    # the captured traffic is close to the algorithmic 32 B per cell
+    assert 28.0 < bench.TRAFFIC_PER_CELL[("c3", "f64")] < 36.0
+    assert bench.NCU_INST[("c3", "f64")]["fp64_inst_per_cell"] > 0
+    assert bench.ncu_capture_config(types.SimpleNamespace(**dict(vars(a), variant=bench.CAPTURED_VARIANT)))
     # the ncu figures belong to the captured configuration only
     for over in (dict(cells=512), dict(noise=0.0), dict(integrator="rk4"), dict(variant=3)):
         b = types.SimpleNamespace(**dict(vars(a), **over))
-        assert not bench.ncu_capture_config(b) and bench.traffic(b, 4096 ** 2) is None
+        assert not bench.ncu_capture_config(b) and bench.traffic(b, 10080 ** 2) is None
 
 
 def test_tip_extents_find_each_grains_four_tips():
