@@ -497,6 +497,7 @@ def run_other(args, cfg):
     run(args.steps)
     e1.record(stream)
     torch.cuda.synchronize()
+    launches = sched.kernel_launches - launches0
     barrier(pg)
     clk = clocks.stop()
     c1 = cells_per_step()
@@ -519,7 +520,7 @@ def run_other(args, cfg):
                                                               NCU_INST.get((args.config, "f64"))
                                                               if ncu_capture_config(args) else None)),
             "cpu_baseline": None, "e2e": None,
-            "gpu_launches": sched.kernel_launches - launches0,
+            "gpu_launches": launches,
             "clocks": {"sm_mhz": clk["sm_mhz"], "sm_max_mhz": clk["sm_max_mhz"], "reasons": clk["reasons"],
                        "samples": clk["samples"]},
         }

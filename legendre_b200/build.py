@@ -52,10 +52,12 @@ def _nvcc() -> str:
 
 
 def _digest(deps, extra: str) -> str:
+    # source names relative to the repository root, so that a copy of the
+    # tree at another path (with its built libraries) is not stale
     h = hashlib.sha256(extra.encode())
-    for d in sorted(map(str, deps)):
+    for d in sorted(Path(p).resolve().relative_to(ROOT).as_posix() for p in deps):
         h.update(d.encode())
-        h.update(Path(d).read_bytes())
+        h.update((ROOT / d).read_bytes())
     return h.hexdigest()
 
 

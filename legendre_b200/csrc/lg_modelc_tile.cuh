@@ -403,8 +403,12 @@ __device__ __forceinline__ void strip_unit(const typename Ops::Params& m, uint64
 // an even number of rows): each pass of the row loop steps rows j and j+1
 // together, so every lane carries two independent cells -- four face fluxes,
 // two Gaussians, two cell updates -- whose dependency chains the scheduler
-// interleaves; the y face between the two rows is computed once.  The window
-// holds phi rows j-1 .. j+2 with the prefetch of j+3 and j+4 in flight.
+// interleaves; the y face between the two rows is computed once.  Each pass
+// reads its four phi and u rows j-1 .. j+2 from L1, where the previous pass
+// prefetched them, instead of carrying a six-row window in registers: the
+// unit needs fewer registers (no spills at 3 CTAs per SM) and no register
+// moves to shift the window.  Units are a multiple of four rows ending at
+// or before the ghost row n1, so every row read lies inside the slab.
 // Same arithmetic per cell, in the same operand order, as strip_row.
 template <class T, class Ops, bool NOISE, int NX, bool FULL>
 __device__ __forceinline__ void strip_unit_pair(const typename Ops::Params& m, uint64_t seed, int key_block,
@@ -432,12 +436,10 @@ __device__ __forceinline__ void strip_unit_pair(const typename Ops::Params& m, u
             uw = __ldg(uu + off0 + (r - r0) * sy);
         }
     };
-    Row3<T> A, B, C, D, E, F;
-    T UA, UB, UC, UD, UE, UF;
+    Row3<T> A, B, C, D;
+    T UA, UB, UC, UD;
     load_row(r0 - 1, A, UA);
     load_row(r0, B, UB);
-    load_row(r0 + 1, C, UC);
-    load_row(r0 + 2, D, UD);
     T bnd = T(0);
     {
         const int r = r0 + lane;
@@ -453,9 +455,25 @@ __device__ __forceinline__ void strip_unit_pair(const typename Ops::Params& m, u
     EdgeHold<T> eh{T(0), T(0), T(0), T(0)};
 #pragma unroll 1
     for (int j = r0; j < r1; j += 2) {
-        // prefetch of rows j+3 and j+4
-        load_row(j + 3, E, UE);
-        load_row(j + 4, F, UF);
+        // the four rows of this pass (j-1 .. j+2 <= n1) from L1, and an L1
+        // prefetch of the next pass's two new rows
+        {
+            const T* q = ph + off - sy;
+            A = {__ldg(q - 1), __ldg(q), __ldg(q + 1)};
+            B = {__ldg(q + sy - 1), __ldg(q + sy), __ldg(q + sy + 1)};
+            C = {__ldg(q + 2 * sy - 1), __ldg(q + 2 * sy), __ldg(q + 2 * sy + 1)};
+            D = {__ldg(q + 3 * sy - 1), __ldg(q + 3 * sy), __ldg(q + 3 * sy + 1)};
+            const T* w = uu + off - sy;
+            UA = __ldg(w);
+            UB = __ldg(w + sy);
+            UC = __ldg(w + 2 * sy);
+            UD = __ldg(w + 3 * sy);
+            const int64_t p3 = (int64_t)(min(j + 3, n1) - j) * sy, p4 = (int64_t)(min(j + 4, n1) - j) * sy;
+            asm volatile("prefetch.global.L1 [%0];" ::"l"(ph + off + p3));
+            asm volatile("prefetch.global.L1 [%0];" ::"l"(ph + off + p4));
+            asm volatile("prefetch.global.L1 [%0];" ::"l"(uu + off + p3));
+            asm volatile("prefetch.global.L1 [%0];" ::"l"(uu + off + p4));
+        }
         const T ul0 = __ldg(uu + off - 1), ur0 = __ldg(uu + off + 1);
         const T ul1 = __ldg(uu + off + sy - 1), ur1 = __ldg(uu + off + sy + 1);
         T nv0 = T(0), nv1 = T(0);
@@ -486,14 +504,6 @@ __device__ __forceinline__ void strip_unit_pair(const typename Ops::Params& m, u
         store_cell(out, po, uo, off + sy, phin1, un1, ok, true, edge_x, j + 1, r0, n0, n1, col, lane, last_lane, g.L,
                    nb, eh);
         jb = jt1;
-        A = C;
-        B = D;
-        C = E;
-        D = F;
-        UA = UC;
-        UB = UD;
-        UC = UE;
-        UD = UF;
         off += 2 * sy;
     }
     if (edge_x) flush_edges(out, g.L, nb, n0, n1, r0, r1, lane, col - lane == 0, cr == n0 - 1, eh);

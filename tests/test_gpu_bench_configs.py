@@ -16,7 +16,7 @@ parameters (needs a GPU).
   their own eps4, Delta and seed and b = 0.005: sampled instances against
   their own oracle runs.
 * Heat 96^3 periodic as 6^3 blocks of 16^3 for its full 2000 steps:
-  bitwise.
+  bitwise; heat 512^3 as 32^3 blocks of 16^3, 6 steps: bitwise.
 
 The oracle follows src/physics/phasefield.rs:353-422 (the Model C drift),
 src/core/driver.rs:117-185 (the Euler-Maruyama update),
@@ -218,3 +218,24 @@ def test_heat_benchmark_config_full_run(sched, orc):
     t = os_.heat_run(0, 1.0, 0.0, dt, 2000, THREADS)
     assert np.array_equal(sim.state.interior("u"), os_.interior(0))
     assert sim.time() == t
+
+
+def test_heat_large_cube_against_oracle(sched, orc):
+    """512^3 periodic as 32^3 blocks of 16^3 (the bench's large heat
+    workload, on the tensor-copy kernel), a random field, 6 steps: bitwise."""
+    n, b, steps = 512, 16, 6
+    h = 1.0 / n
+    grid = L.CartesianGrid([n] * 3, [b] * 3, [0.0] * 3, [h] * 3).with_periodic([True] * 3)
+    sim = L.Simulation(grid, L.FiniteDifference(), L.Heat(1.0), L.ForwardEuler(), sched, L.CudaAllocator("f64"))
+    og = orc.Grid([n] * 3, [b] * 3, [0.0] * 3, [h] * 3, [True] * 3)
+    os_ = orc.State(og, [1])
+    u0 = np.random.default_rng(5).standard_normal((og.num_blocks(),) + og.slab_shape(1))
+    sim.state.upload("u", u0)
+    os_.set(0, u0)
+    del u0
+    dt = 0.15 * h * h
+    sim.run(dt, steps, graph=True)
+    t = os_.heat_run(0, 1.0, 0.0, dt, steps, THREADS)
+    assert np.array_equal(sim.state.interior("u"), os_.interior(0))
+    assert sim.time() == t
+    del sim, os_

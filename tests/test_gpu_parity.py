@@ -83,6 +83,11 @@ def _heat_pair(sched, orc, cells, block, periodic, h, kappa, dt, steps, graph=Fa
     ([8, 8, 40], [8, 8, 40], [False, False, True]),  # one block of 40 planes, split into z-ranges
     ([9, 10, 12], [3, 5, 6], [True, False, False]),   # odd block width: the cp.async-staged form
     ([32, 48, 48], [16, 16, 16], [False, True, False]),  # 16^3 blocks, tensor-copy staged, whole blocks per CTA
+    # the tensor-copy form on 64 and 512 blocks of 16^3 and on 64 blocks split into z-ranges
+    ([64, 64, 64], [16, 16, 16], [True, True, True]),
+    ([64, 64, 64], [16, 16, 16], None),
+    ([128, 128, 128], [16, 16, 16], [True, False, True]),
+    ([32, 32, 160], [8, 8, 40], [False, True, True]),
 ])
 def test_heat_bit_identical_to_oracle(sched, orc, cells, block, periodic):
     sim, os_, t = _heat_pair(sched, orc, cells, block, periodic, 0.1, 0.7, 0.5 / 6.0 * 0.01 / 0.7, 37)
