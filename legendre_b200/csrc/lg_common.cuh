@@ -12,6 +12,8 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include "lg_log_table.h"
+
 #define LG_MAX_DIM 3
 
 namespace lg {
@@ -62,14 +64,17 @@ __host__ __device__ __forceinline__ double unit_open(uint64_t bits) {
 
 constexpr double kTau = 6.283185307179586476925286766559;
 
-// ln u for the Box-Muller radius, u in [2^-53, 1], to about 1e-15 relative
-// (table-free, division-light; the Gaussian is held to 1e-12 of glibc's).
-// u = 2^e f with f in [sqrt(1/2), sqrt(2)): ln u = e ln 2 + 2 atanh(s),
-// s = (f - 1)/(f + 1), |s| <= 0.1716, by the atanh Taylor series to s^19
-// (truncation below 2e-15 of the sum).  f - 1 is exact (Sterbenz); s comes
-// from the hardware's approximate reciprocal, two Newton steps and one
-// residual correction of the quotient; ln 2 is split so that e ln2_hi is
-// exact for every exponent here.  u = 1 gives exactly 0.
+// ln u for the Box-Muller radius, u in [2^-53, 1], within 3.5e-16 relative
+// of the exact logarithm (the Gaussian is held to 1e-12 of glibc's).  A
+// table-driven reduction (the method of Tang, ACM TOMS 16, 1990, with the
+// table holding the logarithm of its own rounded reciprocals): u = 2^e f
+// with f in [sqrt(1/2), sqrt(2)), F_j = 1 + j/128 the nearest centre
+// (j = rint((f - 1) 128), f - 1 exact), r = f RN(1/F_j) - 1 by one fma
+// (|r| <= 0.0055), and ln u = e ln 2 + L_j + log1p(r) with
+// L_j = -ln RN(1/F_j) from lg_log_table.h and log1p by its Taylor series to
+// r^7 (truncation below 2e-17 relative).  The centre F_0 = 1 makes r = f - 1
+// exact next to u = 1, where ln u is tiny; ln 2 is split so that e ln2_hi
+// is exact.  u = 1 gives exactly +0.
 __device__ __forceinline__ double log_unit_interval(double u) {
     const long long bu = __double_as_longlong(u);
     int e = (int)((bu >> 52) & 0x7ff) - 1023;
@@ -78,27 +83,18 @@ __device__ __forceinline__ double log_unit_interval(double u) {
         f = 0.5 * f;
         e += 1;
     }
-    const double num = f - 1.0, den = f + 1.0;
-    double r;
-    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(den));
-    r = fma(r, fma(-den, r, 1.0), r);
-    r = fma(r, fma(-den, r, 1.0), r);
-    const double q0 = num * r;
-    const double s = fma(fma(-den, q0, num), r, q0);
-    const double z = s * s;
-    double p = 1.0 / 19.0;
-    p = fma(p, z, 1.0 / 17.0);
-    p = fma(p, z, 1.0 / 15.0);
-    p = fma(p, z, 1.0 / 13.0);
-    p = fma(p, z, 1.0 / 11.0);
-    p = fma(p, z, 1.0 / 9.0);
-    p = fma(p, z, 1.0 / 7.0);
-    p = fma(p, z, 1.0 / 5.0);
-    p = fma(p, z, 1.0 / 3.0);
-    const double t = 2.0 * s;
-    const double lnf = fma(t * z, p, t);
+    const int j = __double2int_rn((f - 1.0) * 128.0);
+    const double2 E = __ldg(&kLogTable[j - kLogTableMin]);
+    const double r = fma(f, E.x, -1.0);
+    double q = 1.0 / 7.0;
+    q = fma(q, r, -1.0 / 6.0);
+    q = fma(q, r, 1.0 / 5.0);
+    q = fma(q, r, -0.25);
+    q = fma(q, r, 1.0 / 3.0);
+    q = fma(q, r, -0.5);
+    const double p = fma(r * r, q, r);
     const double ln2_hi = 0x1.62e42fefa3800p-1, ln2_lo = 0x1.ef35793c76730p-45;
-    return fma((double)e, ln2_hi, fma((double)e, ln2_lo, lnf));
+    return fma((double)e, ln2_hi, E.y) + fma((double)e, ln2_lo, p);
 }
 
 // cos x for the Box-Muller angle, x = fl(2 pi v) in (0, 2 pi], to about
