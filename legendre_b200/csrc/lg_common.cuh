@@ -113,27 +113,26 @@ __device__ __forceinline__ double cos_full_turn(double x) {
     r = fma(-kd, 0x1.0b4611a6p-34, r);
     r = fma(-kd, 0x1.3198a2e037073p-69, r);
     const double z = r * r;
-    double v;
-    if (q & 1) {  // r - r^3/3! + r^5/5! - ... to r^15
-        double sp = 1.0 / 1307674368000.0;
-        sp = fma(sp, z, -1.0 / 6227020800.0);
-        sp = fma(sp, z, 1.0 / 39916800.0);
-        sp = fma(sp, z, -1.0 / 362880.0);
-        sp = fma(sp, z, 1.0 / 5040.0);
-        sp = fma(sp, z, -1.0 / 120.0);
-        sp = fma(sp, z, 1.0 / 6.0);
-        v = fma(-(r * z), sp, r);
-    } else {  // 1 - r^2/2! + r^4/4! - ... to r^16
-        double cp = 1.0 / 20922789888000.0;
-        cp = fma(cp, z, -1.0 / 87178291200.0);
-        cp = fma(cp, z, 1.0 / 479001600.0);
-        cp = fma(cp, z, -1.0 / 3628800.0);
-        cp = fma(cp, z, 1.0 / 40320.0);
-        cp = fma(cp, z, -1.0 / 720.0);
-        cp = fma(cp, z, 1.0 / 24.0);
-        cp = fma(cp, z, -0.5);
-        v = fma(z, cp, 1.0);
-    }
+    // both polynomials, then a select (the lanes of a warp draw random
+    // quadrants, so a branch would run both anyway, in two halves)
+    double sp = 1.0 / 1307674368000.0;  // r - r^3/3! + r^5/5! - ... to r^15
+    sp = fma(sp, z, -1.0 / 6227020800.0);
+    sp = fma(sp, z, 1.0 / 39916800.0);
+    sp = fma(sp, z, -1.0 / 362880.0);
+    sp = fma(sp, z, 1.0 / 5040.0);
+    sp = fma(sp, z, -1.0 / 120.0);
+    sp = fma(sp, z, 1.0 / 6.0);
+    const double sv = fma(-(r * z), sp, r);
+    double cp = 1.0 / 20922789888000.0;  // 1 - r^2/2! + r^4/4! - ... to r^16
+    cp = fma(cp, z, -1.0 / 87178291200.0);
+    cp = fma(cp, z, 1.0 / 479001600.0);
+    cp = fma(cp, z, -1.0 / 3628800.0);
+    cp = fma(cp, z, 1.0 / 40320.0);
+    cp = fma(cp, z, -1.0 / 720.0);
+    cp = fma(cp, z, 1.0 / 24.0);
+    cp = fma(cp, z, -0.5);
+    const double cv = fma(z, cp, 1.0);
+    const double v = (q & 1) ? sv : cv;
     return (q == 1 || q == 2) ? -v : v;
 }
 

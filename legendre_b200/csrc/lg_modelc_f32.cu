@@ -30,6 +30,7 @@ __device__ __forceinline__ float rcp_approx(float x) {
 
 struct OpsFast32 {
     using Params = Fast32;
+    static constexpr bool kFarPass = false;  // its anisotropy has no branches to decide
 
     static __device__ __forceinline__ void aniso(float dx, float dy, float a_bar, float a1pe, float two_ae,
                                                  float tol, float& a, float& inv) {

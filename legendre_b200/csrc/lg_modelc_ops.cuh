@@ -73,15 +73,14 @@ __device__ __forceinline__ double normal_t(uint64_t key, double) { return standa
 // followed by one correction with the exact residual r = x - c q (an fma),
 // RN(q + r y), is the correctly rounded x / c (Markstein's theorem; the
 // same bits as the division, checked against it on 3.8e9 operands over
-// 600 divisors, half of them next to rounding midpoints).  Zeros, tiny and
-// huge x take the division.
+// 600 divisors, half of them next to rounding midpoints).  Zeros are x y
+// (their sign kept); tiny and huge x take the division.
 __device__ __forceinline__ double div_far(double x, double c, double y) {
     const double ax = fabs(x);
-    if (ax >= 0x1p-960 && ax <= 0x1p+960) {
-        const double q = x * y;
-        return fma(fma(-q, c, x), y, q);
-    }
-    return x / c;
+    const double q = x * y;
+    const double qc = fma(fma(-q, c, x), y, q);
+    if (ax >= 0x1p-960 && ax <= 0x1p+960) return qc;
+    return x == 0.0 ? q : x / c;  // +-0 / c = +-0 = +-0 y (y > 0)
 }
 __device__ __forceinline__ float div_far(float x, float c, float) { return x / c; }
 __device__ __forceinline__ float normal_t(uint64_t key, float) { return standard_normal_f32(key); }
@@ -94,6 +93,7 @@ __device__ __forceinline__ float normal_t(uint64_t key, float) { return standard
 template <class T>
 struct OpsExact {
     using Params = MC<T>;
+    static constexpr bool kFarPass = true;  // the paired rows test for the far field first (quarter, *_far)
 
     // x face: KarmaRappelFlux::face(derx, dery) and j = a (a derx - da dery)
     static __device__ __forceinline__ T xface(const MC<T>& m, T dn, T d1, T c, T e) {
@@ -108,6 +108,39 @@ struct OpsExact {
         T a, da;
         kr_face(m, dt, dn, a, da);
         return a * (a * dn + da * dt);
+    }
+    // The far-field forms: the face fluxes and the cell update with the
+    // anisotropy branches decided (kr_face and center_anisotropy both flat),
+    // the same expressions as the branches they stand for, so their bits.
+    // `quarter` is the transverse quarter sum of xface / yface and the
+    // *_mag2 the |grad|^4 those branches test.
+    static __device__ __forceinline__ T quarter(T d1, T c, T e) { return T(0.25) * (d1 + c - e); }
+    static __device__ __forceinline__ T face_mag2(T dx, T dy) {
+        const T dx2 = dx * dx;
+        const T dy2 = dy * dy;
+        const T sum = dx2 + dy2;
+        return sum * sum;
+    }
+    static __device__ __forceinline__ T center_mag2(T cdx, T cdy) { return face_mag2(T(0.5) * cdx, T(0.5) * cdy); }
+    static __device__ __forceinline__ T xface_far(const MC<T>& m, T dn, T dt) {
+        const T a = m.f_a_bar, da = T(0);
+        return a * (a * dn - da * dt);
+    }
+    static __device__ __forceinline__ T yface_far(const MC<T>& m, T dn, T dt) {
+        const T a = m.f_a_bar, da = T(0);
+        return a * (a * dn + da * dt);
+    }
+    static __device__ __forceinline__ void cell_far(const MC<T>& m, T jr, T jl, T jt, T jb, T p, T uc, T ul, T ur,
+                                                    T up, T um, T& kphi, T& ku) {
+        const T flux = (jr - jl + jt - jb) * m.inv_h2_flux;
+        const T g_prime = fma_t(p * p, p, -p);
+        const T one_m_p2 = fma_t(p, -p, T(1));
+        const T p_prime = one_m_p2 * one_m_p2;
+        kphi = div_far(fma_t(m.lambda * uc, -p_prime, flux - g_prime), m.c_far, m.inv_c_far);
+        T acc = T(0);
+        acc += ((ur - (uc + uc)) + ul) * m.ih0;
+        acc += ((up - (uc + uc)) + um) * m.ih1;
+        ku = fma_t(acc, m.d_thermal, T(0.5) * kphi);
     }
     static __device__ __forceinline__ void cell(const MC<T>& m, T jr, T jl, T jt, T jb, T p, T cdx, T cdy, T uc,
                                                 T ul, T ur, T up, T um, T& kphi, T& ku) {

@@ -476,30 +476,74 @@ __device__ __forceinline__ void strip_unit_pair(const typename Ops::Params& m, u
         }
         const T ul0 = __ldg(uu + off - 1), ur0 = __ldg(uu + off + 1);
         const T ul1 = __ldg(uu + off + sy - 1), ur1 = __ldg(uu + off + sy + 1);
+        // the Gaussians of the pass, drawn inside each body below so that
+        // their integer and FP64 chains share a block with the face and cell
+        // arithmetic
         T nv0 = T(0), nv1 = T(0);
-        if (NOISE) {
-            nv0 = Ops::noise(splitmix64(block_key ^ (uint64_t)(col + j * n0)));
-            nv1 = Ops::noise(splitmix64(block_key ^ (uint64_t)(col + (j + 1) * n0)));
-        }
-        const T fl0 = Ops::xface(m, B.b - B.a, C.b - A.b, C.a, A.a);
-        const T jt0 = Ops::yface(m, C.b - B.b, C.c - C.a, B.c, B.a);
-        const T fl1 = Ops::xface(m, C.b - C.a, D.b - B.b, D.a, B.a);
-        const T jt1 = Ops::yface(m, D.b - C.b, D.c - D.a, C.c, C.a);
-        T fr0 = __shfl_down_sync(kFull, fl0, 1), fr1 = __shfl_down_sync(kFull, fl1, 1);
+        auto draw = [&]() {
+            if (NOISE) {
+                nv0 = Ops::noise(splitmix64(block_key ^ (uint64_t)(col + j * n0)));
+                nv1 = Ops::noise(splitmix64(block_key ^ (uint64_t)(col + (j + 1) * n0)));
+            }
+        };
         const T fb0 = __shfl_sync(kFull, bnd, (j - r0) & 31), fb1 = __shfl_sync(kFull, bnd, (j + 1 - r0) & 31);
-        if (lane == last_lane) {
-            fr0 = fb0;
-            fr1 = fb1;
+        T phin0, phin1, un0, un1, jt1;
+        {
+            T fl0, jt0, fl1;
+            T kphi0, ku0, kphi1, ku1;
+            bool far = false;
+            if constexpr (Ops::kFarPass) {
+                // the four faces' and two centres' anisotropy tests; where
+                // they are all flat across the warp (the far field) the pass
+                // runs without branches, the same expressions as the general
+                // path
+                const T xn0 = B.b - B.a, xt0 = Ops::quarter(C.b - A.b, C.a, A.a);
+                const T yn0 = C.b - B.b, yt0 = Ops::quarter(C.c - C.a, B.c, B.a);
+                const T xn1 = C.b - C.a, xt1 = Ops::quarter(D.b - B.b, D.a, B.a);
+                const T yn1 = D.b - C.b, yt1 = Ops::quarter(D.c - D.a, C.c, C.a);
+                const bool flat = Ops::face_mag2(xn0, xt0) <= m.f_tol && Ops::face_mag2(yt0, yn0) <= m.f_tol &&
+                                  Ops::face_mag2(xn1, xt1) <= m.f_tol && Ops::face_mag2(yt1, yn1) <= m.f_tol &&
+                                  Ops::center_mag2(B.c - B.a, C.b - A.b) <= m.tol &&
+                                  Ops::center_mag2(C.c - C.a, D.b - B.b) <= m.tol;
+                far = __all_sync(kFull, flat);
+                if (far) {
+                    draw();
+                    fl0 = Ops::xface_far(m, xn0, xt0);
+                    jt0 = Ops::yface_far(m, yn0, yt0);
+                    fl1 = Ops::xface_far(m, xn1, xt1);
+                    jt1 = Ops::yface_far(m, yn1, yt1);
+                    T fr0 = __shfl_down_sync(kFull, fl0, 1), fr1 = __shfl_down_sync(kFull, fl1, 1);
+                    if (lane == last_lane) {
+                        fr0 = fb0;
+                        fr1 = fb1;
+                    }
+                    Ops::cell_far(m, fr0, fl0, jt0, jb, B.b, UB, ul0, ur0, UC, UA, kphi0, ku0);
+                    Ops::cell_far(m, fr1, fl1, jt1, jt0, C.b, UC, ul1, ur1, UD, UB, kphi1, ku1);
+                }
+            }
+            if (!far) {
+                draw();
+                fl0 = Ops::xface(m, B.b - B.a, C.b - A.b, C.a, A.a);
+                jt0 = Ops::yface(m, C.b - B.b, C.c - C.a, B.c, B.a);
+                fl1 = Ops::xface(m, C.b - C.a, D.b - B.b, D.a, B.a);
+                jt1 = Ops::yface(m, D.b - C.b, D.c - D.a, C.c, C.a);
+                T fr0 = __shfl_down_sync(kFull, fl0, 1), fr1 = __shfl_down_sync(kFull, fl1, 1);
+                if (lane == last_lane) {
+                    fr0 = fb0;
+                    fr1 = fb1;
+                }
+                Ops::cell(m, fr0, fl0, jt0, jb, B.b, B.c - B.a, C.b - A.b, UB, ul0, ur0, UC, UA, kphi0, ku0);
+                Ops::cell(m, fr1, fl1, jt1, jt0, C.b, C.c - C.a, D.b - B.b, UC, ul1, ur1, UD, UB, kphi1, ku1);
+            }
+            phin0 = Ops::axpy(dt, kphi0, B.b);
+            phin1 = Ops::axpy(dt, kphi1, C.b);
+            if (NOISE) {
+                phin0 = Ops::add_noise(phin0, scale_amp, nv0);
+                phin1 = Ops::add_noise(phin1, scale_amp, nv1);
+            }
+            un0 = Ops::axpy(dt, ku0, UB);
+            un1 = Ops::axpy(dt, ku1, UC);
         }
-        T kphi0, ku0, kphi1, ku1;
-        Ops::cell(m, fr0, fl0, jt0, jb, B.b, B.c - B.a, C.b - A.b, UB, ul0, ur0, UC, UA, kphi0, ku0);
-        Ops::cell(m, fr1, fl1, jt1, jt0, C.b, C.c - C.a, D.b - B.b, UC, ul1, ur1, UD, UB, kphi1, ku1);
-        T phin0 = Ops::axpy(dt, kphi0, B.b), phin1 = Ops::axpy(dt, kphi1, C.b);
-        if (NOISE) {
-            phin0 = Ops::add_noise(phin0, scale_amp, nv0);
-            phin1 = Ops::add_noise(phin1, scale_amp, nv1);
-        }
-        const T un0 = Ops::axpy(dt, ku0, UB), un1 = Ops::axpy(dt, ku1, UC);
         store_cell(out, po, uo, off, phin0, un0, ok, true, edge_x, j, r0, n0, n1, col, lane, last_lane, g.L, nb, eh);
         store_cell(out, po, uo, off + sy, phin1, un1, ok, true, edge_x, j + 1, r0, n0, n1, col, lane, last_lane, g.L,
                    nb, eh);
