@@ -112,7 +112,11 @@ struct OpsFast32 {
         const uint64_t b = splitmix64(a ^ 0xD1B54A32D192ED03ull);
         const float u = __ull2float_rn((a >> 11) + 1) * 0x1p-53f;
         const float v = __ull2float_rn((b >> 11) + 1) * 0x1p-53f;
-        return -sqrtf(-2.0f * __logf(u)) * __cosf(6.28318530717958647692f * (v - 0.5f));
+        // the hardware's approximate square root (sqrt.approx; +0 and -0 map to
+        // themselves): the IEEE sqrtf cost 5 % of the step
+        float r;
+        asm("sqrt.approx.f32 %0, %1;" : "=f"(r) : "f"(-2.0f * __logf(u)));
+        return -r * __cosf(6.28318530717958647692f * (v - 0.5f));
     }
 };
 

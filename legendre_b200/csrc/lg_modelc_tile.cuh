@@ -476,9 +476,9 @@ __device__ __forceinline__ void strip_unit_pair(const typename Ops::Params& m, u
         }
         const T ul0 = __ldg(uu + off - 1), ur0 = __ldg(uu + off + 1);
         const T ul1 = __ldg(uu + off + sy - 1), ur1 = __ldg(uu + off + sy + 1);
-        // the Gaussians of the pass, drawn inside each body below so that
-        // their integer and FP64 chains share a block with the face and cell
-        // arithmetic
+        // the Gaussians of the pass, drawn as soon as its loads are issued:
+        // their integer and FP64 chains fill the loads' latency and the
+        // anisotropy tests that follow, and are needed only at the end
         T nv0 = T(0), nv1 = T(0);
         auto draw = [&]() {
             if (NOISE) {
@@ -486,6 +486,7 @@ __device__ __forceinline__ void strip_unit_pair(const typename Ops::Params& m, u
                 nv1 = Ops::noise(splitmix64(block_key ^ (uint64_t)(col + (j + 1) * n0)));
             }
         };
+        draw();
         const T fb0 = __shfl_sync(kFull, bnd, (j - r0) & 31), fb1 = __shfl_sync(kFull, bnd, (j + 1 - r0) & 31);
         T phin0, phin1, un0, un1, jt1;
         {
@@ -507,7 +508,6 @@ __device__ __forceinline__ void strip_unit_pair(const typename Ops::Params& m, u
                                   Ops::center_mag2(C.c - C.a, D.b - B.b) <= m.tol;
                 far = __all_sync(kFull, flat);
                 if (far) {
-                    draw();
                     fl0 = Ops::xface_far(m, xn0, xt0);
                     jt0 = Ops::yface_far(m, yn0, yt0);
                     fl1 = Ops::xface_far(m, xn1, xt1);
@@ -522,7 +522,6 @@ __device__ __forceinline__ void strip_unit_pair(const typename Ops::Params& m, u
                 }
             }
             if (!far) {
-                draw();
                 fl0 = Ops::xface(m, B.b - B.a, C.b - A.b, C.a, A.a);
                 jt0 = Ops::yface(m, C.b - B.b, C.c - C.a, B.c, B.a);
                 fl1 = Ops::xface(m, C.b - C.a, D.b - B.b, D.a, B.a);
