@@ -88,9 +88,9 @@ NOMINAL_HBM_GBS = 8000.0  # a B200's nominal HBM3e bandwidth, the second denomin
 # captures (smsp__inst_executed and the fp64 pipe's share, x 32 threads per
 # warp instruction, divided by the launch's cell-updates); the capture named
 # is the summary under profiles/.
-NCU_INST = {("c3", "f64"): {"inst_per_cell": 406.8, "fp64_inst_per_cell": 126.8,
+NCU_INST = {("c3", "f64"): {"inst_per_cell": 406.4, "fp64_inst_per_cell": 126.2,
                             "capture": "modelc_strip_f64_5040sq_126blocks"},
-            ("c3", "f32"): {"inst_per_cell": 274.0, "fp64_inst_per_cell": None,
+            ("c3", "f32"): {"inst_per_cell": 268.3, "fp64_inst_per_cell": None,
                             "capture": "modelc_strip_f32_5040sq_126blocks"},
             ("c1big", "f64"): {"inst_per_cell": 103.7, "fp64_inst_per_cell": None,
                                "capture": "heat3d_tma_256cube"}}
