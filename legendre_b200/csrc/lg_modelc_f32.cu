@@ -30,7 +30,7 @@ __device__ __forceinline__ float rcp_approx(float x) {
 
 struct OpsFast32 {
     using Params = Fast32;
-    static constexpr bool kFarPass = false;  // its anisotropy has no branches to decide
+    static constexpr bool kFarPass = true;  // the paired rows test for the far field first (quarter, *_far)
 
     static __device__ __forceinline__ void aniso(float dx, float dy, float a_bar, float a1pe, float two_ae,
                                                  float tol, float& a, float& inv) {
@@ -98,6 +98,38 @@ struct OpsFast32 {
         float dac;
         const float a = oaniso(m, c0 * dx + s0 * dy, c0 * dy - s0 * dx, dac);
         kphi = ((flux - g_prime) - m.lambda * uc * p_prime) * rcp_approx(a * a);
+        const float lap = ((ur + ul) - 2.0f * uc) * m.ih0 + ((up + um) - 2.0f * uc) * m.ih1;
+        ku = lap * m.d_thermal + 0.5f * kphi;
+    }
+    // The far-field forms (every anisotropy of a pass flat): a = a_bar and no
+    // reciprocal per face; the cell's 1/a_bar^2 by the same approximate
+    // reciprocal the general form takes.  Same values as the general forms
+    // with the flat selects taken.
+    static __device__ __forceinline__ float quarter(float d1, float c, float e) { return 0.25f * ((d1 + c) - e); }
+    static __device__ __forceinline__ float face_mag2(float dx, float dy) {
+        const float s = dx * dx + dy * dy;
+        return s * s;
+    }
+    static __device__ __forceinline__ bool face_flat(const Fast32& m, float dx, float dy) {
+        return face_mag2(dx, dy) <= m.f_tol;
+    }
+    static __device__ __forceinline__ bool center_flat(const Fast32& m, float cdx, float cdy) {
+        return face_mag2(0.5f * cdx, 0.5f * cdy) <= m.c_tol;
+    }
+    static __device__ __forceinline__ float xface_far(const Fast32& m, float dn, float) {
+        return m.f_a_bar * (m.f_a_bar * dn);
+    }
+    static __device__ __forceinline__ float yface_far(const Fast32& m, float dn, float) {
+        return m.f_a_bar * (m.f_a_bar * dn);
+    }
+    static __device__ __forceinline__ void cell_far(const Fast32& m, float jr, float jl, float jt, float jb, float p,
+                                                    float uc, float ul, float ur, float up, float um, float& kphi,
+                                                    float& ku) {
+        const float flux = ((jr - jl) + (jt - jb)) * m.inv_h2_flux;
+        const float g_prime = p * p * p - p;
+        const float one_m_p2 = 1.0f - p * p;
+        const float p_prime = one_m_p2 * one_m_p2;
+        kphi = ((flux - g_prime) - m.lambda * uc * p_prime) * rcp_approx(m.c_a_bar * m.c_a_bar);
         const float lap = ((ur + ul) - 2.0f * uc) * m.ih0 + ((up + um) - 2.0f * uc) * m.ih1;
         ku = lap * m.d_thermal + 0.5f * kphi;
     }

@@ -122,6 +122,10 @@ struct OpsExact {
         return sum * sum;
     }
     static __device__ __forceinline__ T center_mag2(T cdx, T cdy) { return face_mag2(T(0.5) * cdx, T(0.5) * cdy); }
+    static __device__ __forceinline__ bool face_flat(const MC<T>& m, T dx, T dy) { return face_mag2(dx, dy) <= m.f_tol; }
+    static __device__ __forceinline__ bool center_flat(const MC<T>& m, T cdx, T cdy) {
+        return center_mag2(cdx, cdy) <= m.tol;
+    }
     static __device__ __forceinline__ T xface_far(const MC<T>& m, T dn, T dt) {
         const T a = m.f_a_bar, da = T(0);
         return a * (a * dn - da * dt);
