@@ -410,13 +410,19 @@ __device__ __forceinline__ void strip_unit(const typename Ops::Params& m, uint64
 // moves to shift the window.  Units are a multiple of four rows ending at
 // or before the ghost row n1, so every row read lies inside the slab.
 // Same arithmetic per cell, in the same operand order, as strip_row.
-template <class T, class Ops, bool NOISE, int NX, bool FULL>
+//
+// ORIENT: the multi-grain faces (strip_row's ORIENT branch, for two rows):
+// each face in the frame of the cell being updated, shared with the
+// neighbour only where the neighbour's cos/sin theta0 are the same bits,
+// else evaluated again in this cell's frame.
+template <class T, class Ops, bool NOISE, int NX, bool FULL, bool ORIENT = false>
 __device__ __forceinline__ void strip_unit_pair(const typename Ops::Params& m, uint64_t seed, int key_block,
                                                 const TileArgs& g, const T* __restrict__ ph,
                                                 const T* __restrict__ uu, T* __restrict__ out, T* __restrict__ po,
                                                 T* __restrict__ uo, const Nbr2& nb, int r0, int r1, int lane,
                                                 int col, bool valid, int last_lane, int cr, bool edge_x, int n0,
-                                                int n1, int sy, double tnow, T dt, T scale_amp) {
+                                                int n1, int sy, double tnow, T dt, T scale_amp,
+                                                const T* __restrict__ trig_b = nullptr, int64_t ncells = 0) {
     uint64_t block_key = 0;
     if (NOISE)
         block_key = wiener_block_key(seed, (uint64_t)__double_as_longlong(tnow), kWienerStream0,
@@ -448,10 +454,26 @@ __device__ __forceinline__ void strip_unit_pair(const typename Ops::Params& m, u
             const T c0m = __ldg(q - sy), c1m = __ldg(q - sy + 1);
             const T c00 = __ldg(q), c10 = __ldg(q + 1);
             const T c0p = __ldg(q + sy), c1p = __ldg(q + sy + 1);
-            bnd = Ops::xface(m, c10 - c00, c1p - c1m, c0p, c0m);
+            if constexpr (ORIENT) {  // in the frame of the strip's last cell of the row
+                const int64_t ci = (int64_t)r * n0 + cr;
+                bnd = Ops::oxface(m, __ldg(trig_b + ci), __ldg(trig_b + ncells + ci), c10 - c00,
+                                  T(0.25) * (c1p - c1m + c0p - c0m));
+            } else {
+                bnd = Ops::xface(m, c10 - c00, c1p - c1m, c0p, c0m);
+            }
         }
     }
-    T jb = Ops::yface(m, B.b - A.b, B.c - B.a, A.c, A.a);
+    const int ccol = FULL ? col : min(col, n0 - 1);
+    T cprev = T(0), sprev = T(0);  // multi-grain: cos/sin theta0 of the row below the pass
+    T jb;
+    if constexpr (ORIENT) {  // the bottom face of the first row in its own frame
+        const int64_t ci = (int64_t)r0 * n0 + ccol;
+        cprev = __ldg(trig_b + ci);
+        sprev = __ldg(trig_b + ncells + ci);
+        jb = Ops::oyface(m, cprev, sprev, T(0.25) * (B.c - B.a + A.c - A.a), B.b - A.b);
+    } else {
+        jb = Ops::yface(m, B.b - A.b, B.c - B.a, A.c, A.a);
+    }
     EdgeHold<T> eh{T(0), T(0), T(0), T(0)};
 #pragma unroll 1
     for (int j = r0; j < r1; j += 2) {
@@ -476,6 +498,14 @@ __device__ __forceinline__ void strip_unit_pair(const typename Ops::Params& m, u
         }
         const T ul0 = __ldg(uu + off - 1), ur0 = __ldg(uu + off + 1);
         const T ul1 = __ldg(uu + off + sy - 1), ur1 = __ldg(uu + off + sy + 1);
+        T c0 = T(0), s0 = T(0), c1 = T(0), s1 = T(0);  // multi-grain: frames of rows j and j+1
+        if constexpr (ORIENT) {
+            const int64_t ci = (int64_t)j * n0 + ccol;
+            c0 = __ldg(trig_b + ci);
+            s0 = __ldg(trig_b + ncells + ci);
+            c1 = __ldg(trig_b + ci + n0);
+            s1 = __ldg(trig_b + ncells + ci + n0);
+        }
         // the Gaussians of the pass, drawn as soon as its loads are issued:
         // their integer and FP64 chains fill the loads' latency and the
         // anisotropy tests that follow, and are needed only at the end
@@ -489,7 +519,43 @@ __device__ __forceinline__ void strip_unit_pair(const typename Ops::Params& m, u
         draw();
         const T fb0 = __shfl_sync(kFull, bnd, (j - r0) & 31), fb1 = __shfl_sync(kFull, bnd, (j + 1 - r0) & 31);
         T phin0, phin1, un0, un1, jt1;
-        {
+        if constexpr (ORIENT) {
+            const T q = T(0.25);
+            const T jl0 = Ops::oxface(m, c0, s0, B.b - B.a, q * (C.b - A.b + C.a - A.a));
+            const T jt0 = Ops::oyface(m, c0, s0, q * (C.c - C.a + B.c - B.a), C.b - B.b);
+            const T jl1 = Ops::oxface(m, c1, s1, C.b - C.a, q * (D.b - B.b + D.a - B.a));
+            jt1 = Ops::oyface(m, c1, s1, q * (D.c - D.a + C.c - C.a), D.b - C.b);
+            T jr0 = __shfl_down_sync(kFull, jl0, 1), jr1 = __shfl_down_sync(kFull, jl1, 1);
+            const T c0n = __shfl_down_sync(kFull, c0, 1), s0n = __shfl_down_sync(kFull, s0, 1);
+            const T c1n = __shfl_down_sync(kFull, c1, 1), s1n = __shfl_down_sync(kFull, s1, 1);
+            if (lane == last_lane) {
+                jr0 = fb0;
+                jr1 = fb1;
+            } else {
+                if (!(same_bits(c0n, c0) && same_bits(s0n, s0)))
+                    jr0 = Ops::oxface(m, c0, s0, B.c - B.b, q * (C.c - A.c + C.b - A.b));
+                if (!(same_bits(c1n, c1) && same_bits(s1n, s1)))
+                    jr1 = Ops::oxface(m, c1, s1, C.c - C.b, q * (D.c - B.c + D.b - B.b));
+            }
+            T jbot0 = jb, jbot1 = jt0;
+            if (!(same_bits(cprev, c0) && same_bits(sprev, s0)))
+                jbot0 = Ops::oyface(m, c0, s0, q * (B.c - B.a + A.c - A.a), B.b - A.b);
+            if (!(same_bits(c0, c1) && same_bits(s0, s1)))
+                jbot1 = Ops::oyface(m, c1, s1, q * (C.c - C.a + B.c - B.a), C.b - B.b);
+            T kphi0, ku0, kphi1, ku1;
+            Ops::ocell(m, jr0, jl0, jt0, jbot0, B.b, B.c - B.a, C.b - A.b, c0, s0, UB, ul0, ur0, UC, UA, kphi0, ku0);
+            Ops::ocell(m, jr1, jl1, jt1, jbot1, C.b, C.c - C.a, D.b - B.b, c1, s1, UC, ul1, ur1, UD, UB, kphi1, ku1);
+            phin0 = Ops::axpy(dt, kphi0, B.b);
+            phin1 = Ops::axpy(dt, kphi1, C.b);
+            if (NOISE) {
+                phin0 = Ops::add_noise(phin0, scale_amp, nv0);
+                phin1 = Ops::add_noise(phin1, scale_amp, nv1);
+            }
+            un0 = Ops::axpy(dt, ku0, UB);
+            un1 = Ops::axpy(dt, ku1, UC);
+            cprev = c1;
+            sprev = s1;
+        } else {
             T fl0, jt0, fl1;
             T kphi0, ku0, kphi1, ku1;
             bool far = false;
@@ -502,10 +568,10 @@ __device__ __forceinline__ void strip_unit_pair(const typename Ops::Params& m, u
                 const T yn0 = C.b - B.b, yt0 = Ops::quarter(C.c - C.a, B.c, B.a);
                 const T xn1 = C.b - C.a, xt1 = Ops::quarter(D.b - B.b, D.a, B.a);
                 const T yn1 = D.b - C.b, yt1 = Ops::quarter(D.c - D.a, C.c, C.a);
-                const bool flat = Ops::face_mag2(xn0, xt0) <= m.f_tol && Ops::face_mag2(yt0, yn0) <= m.f_tol &&
-                                  Ops::face_mag2(xn1, xt1) <= m.f_tol && Ops::face_mag2(yt1, yn1) <= m.f_tol &&
-                                  Ops::center_mag2(B.c - B.a, C.b - A.b) <= m.tol &&
-                                  Ops::center_mag2(C.c - C.a, D.b - B.b) <= m.tol;
+                const bool flat = Ops::face_flat(m, xn0, xt0) && Ops::face_flat(m, yt0, yn0) &&
+                                  Ops::face_flat(m, xn1, xt1) && Ops::face_flat(m, yt1, yn1) &&
+                                  Ops::center_flat(m, B.c - B.a, C.b - A.b) &&
+                                  Ops::center_flat(m, C.c - C.a, D.b - B.b);
                 far = __all_sync(kFull, flat);
                 if (far) {
                     fl0 = Ops::xface_far(m, xn0, xt0);
@@ -605,7 +671,7 @@ __global__ void __launch_bounds__(256, MINB)
         Nbr2 nb;
         nb.load(topo, b);
         if constexpr (PAIR) {
-            static_assert(MODE == 0 && !ORIENT && !TAIL, "the paired rows serve the Euler-Maruyama step");
+            static_assert(MODE == 0 && !TAIL && !(ORIENT && BATCH), "the paired rows serve the Euler-Maruyama step");
             if constexpr (BATCH) {
                 const int inst = b / bt.bpi;
                 const typename Ops::Params mi = static_cast<const typename Ops::Params*>(bt.params)[inst];
@@ -613,9 +679,10 @@ __global__ void __launch_bounds__(256, MINB)
                                                          nb, r0, r1, lane, col, valid, last_lane, cr, edge_x, n0, n1,
                                                          sy, tnow, dt, scale_amp);
             } else {
-                strip_unit_pair<T, Ops, NOISE, NX, FULL>(m0, g.seed, b, g, ph, uu, out, po, uo, nb, r0, r1, lane, col,
-                                                         valid, last_lane, cr, edge_x, n0, n1, sy, tnow, dt,
-                                                         scale_amp);
+                const T* trig_b = ORIENT ? static_cast<const T*>(oa.trig) + (int64_t)b * n0 * n1 : nullptr;
+                strip_unit_pair<T, Ops, NOISE, NX, FULL, ORIENT>(m0, g.seed, b, g, ph, uu, out, po, uo, nb, r0, r1,
+                                                                 lane, col, valid, last_lane, cr, edge_x, n0, n1, sy,
+                                                                 tnow, dt, scale_amp, trig_b, oa.ncells);
             }
         } else if constexpr (BATCH) {
             const int inst = b / bt.bpi;
@@ -722,19 +789,19 @@ cudaError_t launch_strip_minb(const T* in, T* out, TileArgs g, const typename Op
 
 // the multi-grain step: block widths 126 (the 101.6M-cell configuration)
 // and 256 get a compile-time row stride
-template <class T, class Ops, bool NOISE, int MINB>
+template <class T, class Ops, bool NOISE, int MINB, bool PAIR = false>
 cudaError_t launch_strip_oriented(const T* in, T* out, TileArgs g, const typename Ops::Params& m, T dt, T scale_amp,
                                   OrientArgs oa, cudaStream_t s) {
     const bool tail = strip_plan(g, 1 + 3);
     const dim3 grid = strip_ctas(g), block(256);
-    if (tail) {
+    if (tail) {  // blocks lower than the row group: single rows
         modelc_strip_kernel<T, Ops, NOISE, MINB, 0, 1, false, true, true><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp, BatchArgs{}, oa, RkArgs<T>{});
         return cudaGetLastError();
     }
     switch (g.topo.n[0]) {
-        case 126: modelc_strip_kernel<T, Ops, NOISE, MINB, 126, 1, false, false, true><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp, BatchArgs{}, oa, RkArgs<T>{}); break;
-        case 256: modelc_strip_kernel<T, Ops, NOISE, MINB, 256, 1, false, false, true><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp, BatchArgs{}, oa, RkArgs<T>{}); break;
-        default: modelc_strip_kernel<T, Ops, NOISE, MINB, 0, 1, false, false, true><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp, BatchArgs{}, oa, RkArgs<T>{});
+        case 126: modelc_strip_kernel<T, Ops, NOISE, MINB, 126, 1, false, false, true, 0, PAIR><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp, BatchArgs{}, oa, RkArgs<T>{}); break;
+        case 256: modelc_strip_kernel<T, Ops, NOISE, MINB, 256, 1, false, false, true, 0, PAIR><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp, BatchArgs{}, oa, RkArgs<T>{}); break;
+        default: modelc_strip_kernel<T, Ops, NOISE, MINB, 0, 1, false, false, true, 0, PAIR><<<grid, block, 0, s>>>(in, out, g, m, dt, scale_amp, BatchArgs{}, oa, RkArgs<T>{});
     }
     return cudaGetLastError();
 }
