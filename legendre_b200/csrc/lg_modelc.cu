@@ -29,8 +29,8 @@ cudaError_t launch_modelc_oriented_f64(const double* in, double* out, const Cart
     const MC<double> mc = to_mc<double>(m);
     const double scale_amp = std::sqrt(dt) * nz.amp;
     const OrientArgs oa{trig, ncells};
-    if (nz.on) return launch_strip_oriented<double, OpsExact<double>, true, 2>(in, out, g, mc, dt, scale_amp, oa, s);
-    return launch_strip_oriented<double, OpsExact<double>, false, 2>(in, out, g, mc, dt, scale_amp, oa, s);
+    if (nz.on) return launch_strip_oriented<double, OpsExact<double>, true, 2, true>(in, out, g, mc, dt, scale_amp, oa, s);
+    return launch_strip_oriented<double, OpsExact<double>, false, 2, true>(in, out, g, mc, dt, scale_amp, oa, s);
 }
 
 cudaError_t launch_modelc_rk_stage_f64(int mode, const double* in, double* out, const CartTopo& topo,

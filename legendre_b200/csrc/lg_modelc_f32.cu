@@ -192,8 +192,8 @@ cudaError_t launch_modelc_oriented_f32(const float* in, float* out, const CartTo
     const Fast32 f = fast32_of(m);
     const float scale_amp = (float)(std::sqrt(dt) * nz.amp);
     const OrientArgs oa{trig, ncells};
-    if (nz.on) return launch_strip_oriented<float, OpsFast32, true, 2>(in, out, g, f, (float)dt, scale_amp, oa, s);
-    return launch_strip_oriented<float, OpsFast32, false, 2>(in, out, g, f, (float)dt, scale_amp, oa, s);
+    if (nz.on) return launch_strip_oriented<float, OpsFast32, true, 2, true>(in, out, g, f, (float)dt, scale_amp, oa, s);
+    return launch_strip_oriented<float, OpsFast32, false, 2, true>(in, out, g, f, (float)dt, scale_amp, oa, s);
 }
 
 cudaError_t launch_modelc_rk_stage_f32(int mode, const float* in, float* out, const CartTopo& topo,
