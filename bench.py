@@ -92,7 +92,7 @@ NCU_INST = {("c3", "f64"): {"inst_per_cell": 406.4, "fp64_inst_per_cell": 126.2,
                             "capture": "modelc_strip_f64_5040sq_126blocks"},
             ("c3", "f32"): {"inst_per_cell": 268.3, "fp64_inst_per_cell": None,
                             "capture": "modelc_strip_f32_5040sq_126blocks"},
-            ("c1big", "f64"): {"inst_per_cell": 103.7, "fp64_inst_per_cell": None,
+            ("c1big", "f64"): {"inst_per_cell": 70.6, "fp64_inst_per_cell": None,
                                "capture": "heat3d_tma_256cube"}}
 
 # the strip-kernel variant the captures ran (the autotuner's choice on 10080^2)

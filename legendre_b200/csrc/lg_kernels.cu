@@ -449,22 +449,39 @@ __global__ void __launch_bounds__(1024) heat3d_tma_kernel(const __grid_constant_
             // slab columns the x halos came from: left = neighbour's n0 (or
             // own 1), right = neighbour's 1 (or own n0); index within the pair
             const int il = (nb[0] >= 0 ? n0 : 1) & 1, ih = (nb[1] >= 0 ? 1 : n0) & 1;
-            double* o = out + slab_base(L, b, field);
+            // a thread walks its (x, y) column up the planes: the z
+            // neighbours slide through registers (zm <- uc <- zp) and every
+            // address advances by its stride, the arithmetic unchanged
+            const int plane = n1 * W;
+            const double* q = S + (size_t)y * W + (x + 1);
+            const double* xl = XL + (size_t)y * 2 + il;
+            const double* xh = XH + (size_t)y * 2 + ih;
+            const double* yl = YL + (x + 1);
+            const double* yh = YH + (x + 1);
+            double* op = out + slab_base(L, b, field) + (int64_t)(x + 1) + (int64_t)(y + 1) * sy +
+                         (int64_t)(z0 + 1) * sz;
+            double zm = ZL[(size_t)y * W + x + 1];
+            double uc = q[0];
             for (int r = 0; r < nz; ++r) {
-                const double* q = S + ((size_t)r * n1 + y) * W + (x + 1);
-                const double uc = q[0];
-                const double xm = x == 0 ? XL[((size_t)r * n1 + y) * 2 + il] : q[-1];
-                const double xp = x == n0 - 1 ? XH[((size_t)r * n1 + y) * 2 + ih] : q[1];
-                const double ym = y == 0 ? YL[(size_t)r * W + x + 1] : q[-W];
-                const double yp = y == n1 - 1 ? YH[(size_t)r * W + x + 1] : q[W];
-                const double zm = r == 0 ? ZL[(size_t)y * W + x + 1] : q[-(int64_t)n1 * W];
-                const double zp = r == nz - 1 ? ZH[(size_t)y * W + x + 1] : q[(int64_t)n1 * W];
+                const double xm = x == 0 ? *xl : q[-1];
+                const double xp = x == n0 - 1 ? *xh : q[1];
+                const double ym = y == 0 ? *yl : q[-W];
+                const double yp = y == n1 - 1 ? *yh : q[W];
+                const double zp = r == nz - 1 ? ZH[(size_t)y * W + x + 1] : q[plane];
                 double acc = 0.0;
                 acc += ((xp - (uc + uc)) + xm) * ih0;
                 acc += ((yp - (uc + uc)) + ym) * ih1;
                 acc += ((zp - (uc + uc)) + zm) * ih2;
                 const double k = acc * kappa;
-                o[(int64_t)(x + 1) + (y + 1) * sy + (z0 + r + 1) * sz] = uc + dt * k;
+                *op = uc + dt * k;
+                zm = uc;
+                uc = zp;
+                q += plane;
+                xl += 2 * n1;
+                xh += 2 * n1;
+                yl += W;
+                yh += W;
+                op += sz;
             }
         }
         // every thread is done with the stage before the next item's copies
