@@ -58,8 +58,8 @@ cudaError_t launch_modelc_batch_f64(const double* in, double* out, const CartTop
     TileArgs g{topo, L, dt, 0, tdev, slot, rows, 0, 0, 0};
     const BatchArgs bt{params, seeds, bpi};
     const double scale_amp = std::sqrt(dt) * amp;
-    if (amp != 0.0) return launch_strip_batch<double, OpsExact<double>, true, 2>(in, out, g, bt, dt, scale_amp, s);
-    return launch_strip_batch<double, OpsExact<double>, false, 2>(in, out, g, bt, dt, scale_amp, s);
+    if (amp != 0.0) return launch_strip_batch<double, OpsExact<double>, true, 2, true>(in, out, g, bt, dt, scale_amp, s);
+    return launch_strip_batch<double, OpsExact<double>, false, 2, true>(in, out, g, bt, dt, scale_amp, s);
 }
 
 }  // namespace lg

@@ -221,8 +221,8 @@ cudaError_t launch_modelc_batch_f32(const float* in, float* out, const CartTopo&
     TileArgs g{topo, L, dt, 0, tdev, slot, rows, 0, 0, 0};
     const BatchArgs bt{params, seeds, bpi};
     const float scale_amp = (float)(std::sqrt(dt) * amp);
-    if (amp != 0.0) return launch_strip_batch<float, OpsFast32, true, 3>(in, out, g, bt, (float)dt, scale_amp, s);
-    return launch_strip_batch<float, OpsFast32, false, 3>(in, out, g, bt, (float)dt, scale_amp, s);
+    if (amp != 0.0) return launch_strip_batch<float, OpsFast32, true, 2, true>(in, out, g, bt, (float)dt, scale_amp, s);
+    return launch_strip_batch<float, OpsFast32, false, 2, true>(in, out, g, bt, (float)dt, scale_amp, s);
 }
 
 }  // namespace lg
