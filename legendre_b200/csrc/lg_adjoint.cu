@@ -556,27 +556,51 @@ __global__ void __launch_bounds__(256) adjoint_strip_kernel(const T* __restrict_
             const bool cin = rin && xin;
             const bool orow = r >= Y0 && r < Y1;
             const T p0c = shfl_dn1(p0b), ppc = shfl_dn1(ppb);
-            // x face left of X in row r
-            T xJ, xn_raw, xt_raw, xe_raw;
+            // the x face left of X and the y face above X in row r, and the
+            // centre anisotropy's derivatives.  Where all three are flat across
+            // the warp (the far field) their derivatives are constants: the
+            // branch-free body below gives the general path's values.
+            const T dnx = p0b - p0a, dtx = T(0.25) * (((ppb - pmb) + ppa) - pma);
+            const T dny = ppb - p0b, dty = T(0.25) * (((ppc - ppa) + p0c) - p0a);
+            const T chx = T(0.5) * (p0c - p0a), chy = T(0.5) * (ppb - pmb);
+            T xJ, xn_raw, xt_raw, xe_raw, yJ, yn_raw, yt_raw, ye_raw;
+            CentreDer<T> c;
             {
-                const T dn = p0b - p0a;
-                const T dtr = T(0.25) * (((ppb - pmb) + ppa) - pma);
-                const FaceDer<T> f = face_der(dn, dtr, m.f_a_bar, m.f_ae, m.f_a12, m.f_tol);
-                xJ = f.a * (f.a * dn - f.da * dtr);
-                xn_raw = T(2) * f.a * f.ax * dn + f.a * f.a - (f.ax * f.da + f.a * f.dax) * dtr;
-                xt_raw = T(2) * f.a * f.ay * dn - (f.ay * f.da + f.a * f.day) * dtr - f.a * f.da;
-                xe_raw = (T(2) * f.a * dn - f.da * dtr) * f.ae - f.a * dtr * f.dae;
-            }
-            // y face above X in row r (between rows r and r + 1)
-            T yJ, yn_raw, yt_raw, ye_raw;
-            {
-                const T dn = ppb - p0b;
-                const T dtr = T(0.25) * (((ppc - ppa) + p0c) - p0a);
-                const FaceDer<T> f = face_der(dtr, dn, m.f_a_bar, m.f_ae, m.f_a12, m.f_tol);
-                yJ = f.a * (f.a * dn + f.da * dtr);
-                yn_raw = T(2) * f.a * f.ay * dn + f.a * f.a + (f.ay * f.da + f.a * f.day) * dtr;
-                yt_raw = T(2) * f.a * f.ax * dn + (f.ax * f.da + f.a * f.dax) * dtr + f.a * f.da;
-                ye_raw = (T(2) * f.a * dn + f.da * dtr) * f.ae + f.a * dtr * f.dae;
+                auto mag2 = [](T a, T b) {
+                    const T sq = a * a + b * b;
+                    return sq * sq;
+                };
+                const bool flat = mag2(dnx, dtx) <= m.f_tol && mag2(dty, dny) <= m.f_tol && mag2(chx, chy) <= m.c_tol;
+                if (__all_sync(0xffffffffu, flat)) {
+                    const T a = m.f_a_bar;
+                    xJ = a * (a * dnx);
+                    xn_raw = a * a;
+                    xt_raw = T(0);
+                    xe_raw = T(-6) * a * dnx;  // (2 a dn - da dt) ae - a dt dae, da = dae = 0, ae = -3
+                    yJ = a * (a * dny);
+                    yn_raw = a * a;
+                    yt_raw = T(0);
+                    ye_raw = T(-6) * a * dny;
+                    c.a = m.c_a_bar;
+                    c.ax = c.ay = T(0);
+                    c.ae = T(-3);
+                } else {
+                    {
+                        const FaceDer<T> f = face_der(dnx, dtx, m.f_a_bar, m.f_ae, m.f_a12, m.f_tol);
+                        xJ = f.a * (f.a * dnx - f.da * dtx);
+                        xn_raw = T(2) * f.a * f.ax * dnx + f.a * f.a - (f.ax * f.da + f.a * f.dax) * dtx;
+                        xt_raw = T(2) * f.a * f.ay * dnx - (f.ay * f.da + f.a * f.day) * dtx - f.a * f.da;
+                        xe_raw = (T(2) * f.a * dnx - f.da * dtx) * f.ae - f.a * dtx * f.dae;
+                    }
+                    {
+                        const FaceDer<T> f = face_der(dty, dny, m.f_a_bar, m.f_ae, m.f_a12, m.f_tol);
+                        yJ = f.a * (f.a * dny + f.da * dty);
+                        yn_raw = T(2) * f.a * f.ay * dny + f.a * f.a + (f.ay * f.da + f.a * f.day) * dty;
+                        yt_raw = T(2) * f.a * f.ax * dny + (f.ax * f.da + f.a * f.dax) * dty + f.a * f.da;
+                        ye_raw = (T(2) * f.a * dny + f.da * dty) * f.ae + f.a * dty * f.dae;
+                    }
+                    c = centre_der(chx, chy, m.c_a_bar, m.c_ae, m.c_tol);
+                }
             }
             // cell (X, r): N^, A^ and nu
             const T xJr = shfl_dn1(xJ);
@@ -588,8 +612,6 @@ __global__ void __launch_bounds__(256) adjoint_strip_kernel(const T* __restrict_
                 const T pp = omp * omp;
                 const T gp = ph * ph * ph - ph;
                 const T Nn = -m.lambda * uc * pp + (flux - gp);
-                const CentreDer<T> c =
-                    centre_der(T(0.5) * (p0c - p0a), T(0.5) * (ppb - pmb), m.c_a_bar, m.c_ae, m.c_tol);
                 const T ia = recip(c.a);
                 const T iq = ia * ia;
                 const T kphi = Nn * iq;
