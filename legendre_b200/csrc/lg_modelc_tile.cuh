@@ -217,14 +217,17 @@ __device__ __forceinline__ void strip_row(const typename Ops::Params& m, const T
                                           uint64_t block_key, T bnd, const Row3<T>& A, const Row3<T>& B,
                                           const Row3<T>& C, Row3<T>& P, T UA, T UB, T UC, T& UP, T& jb, T dt,
                                           T scale_amp, const T* __restrict__ trig_b, int64_t ncells, T& cprev,
-                                          T& sprev, T& cnext, T& snext, const RkArgs<T>& rk, EdgeHold<T>& eh) {
+                                          T& sprev, T& cnext, T& snext, const RkArgs<T>& rk, EdgeHold<T>& eh,
+                                          int rs) {
     const int sy = NX > 0 ? NX + 2 : g.L.gdim[0];
     // lanes past the block's last column (valid false) run the same code on
     // a clamped column and only skip the stores: no branch splits the face,
     // noise and cell arithmetic.  Unit heights are whole groups of NB rows,
     // so the row loop has no separately unrolled tail; only blocks of fewer
     // than NB rows (TAIL) run rows past the unit's end, without stores.
-    const bool live = !TAIL || j < r1;
+    // rows below rs belong to the unit below (a block's last unit overlaps
+    // it): computed for their faces, stored only by their own unit
+    const bool live = (!TAIL || j < r1) && j >= rs;
     const bool ok = (FULL || valid) && live;
     if (j + 1 + PF <= n1) {
         const T* q = ph + off + (1 + PF) * sy;
@@ -304,7 +307,8 @@ __device__ __forceinline__ void strip_unit(const typename Ops::Params& m, uint64
                                            T* __restrict__ out, T* __restrict__ po, T* __restrict__ uo,
                                            const Nbr2& nb, int r0, int r1, int lane, int col, bool valid,
                                            int last_lane, int cr, bool edge_x, int n0, int n1, int sy, double tnow,
-                                           T dt, T scale_amp, const T* __restrict__ trig_b, int64_t ncells, const RkArgs<T>& rk) {
+                                           T dt, T scale_amp, const T* __restrict__ trig_b, int64_t ncells, const RkArgs<T>& rk,
+                                           int rs) {
     constexpr int NB = PF + 3;
     uint64_t block_key = 0;
     if (NOISE)
@@ -371,7 +375,7 @@ __device__ __forceinline__ void strip_unit(const typename Ops::Params& m, uint64
                                        uo, nb, edge_x, block_key, bnd, w[(Q) % NB], w[((Q) + 1) % NB],          \
                                        w[((Q) + 2) % NB], w[((Q) + 2 + PF) % NB], uw[(Q) % NB],                \
                                        uw[((Q) + 1) % NB], uw[((Q) + 2) % NB], uw[((Q) + 2 + PF) % NB], jb, dt, \
-                                       scale_amp, trig_b, ncells, cpv, spv, cnx, snx, rk, eh);                                                              \
+                                       scale_amp, trig_b, ncells, cpv, spv, cnx, snx, rk, eh, rs);                                                          \
     off += sy
     if constexpr (sizeof(T) == 8 || !ORIENT) {
         // one copy of the row code: the window shifts down by one row
@@ -397,7 +401,7 @@ __device__ __forceinline__ void strip_unit(const typename Ops::Params& m, uint64
         }
     }
 #undef LG_ROW
-    if (edge_x) flush_edges(out, g.L, nb, n0, n1, r0, r1, lane, col - lane == 0, cr == n0 - 1, eh);
+    if (edge_x) flush_edges(out, g.L, nb, n0, n1, r0, r1, lane, col - lane == 0, cr == n0 - 1, eh, rs);
 }
 
 // The paired form of one work unit (Euler-Maruyama, axis-aligned, units of
@@ -695,14 +699,14 @@ __global__ void __launch_bounds__(256, MINB)
             const typename Ops::Params mi = static_cast<const typename Ops::Params*>(bt.params)[inst];
             strip_unit<T, Ops, NOISE, NX, FULL, PF, TAIL, ORIENT, MODE>(
                 mi, bt.seeds[inst], b - inst * bt.bpi, g, ph, uu, out, po, uo, nb, r0, r1, lane, col, valid, last_lane,
-                cr, edge_x, n0, n1, sy, tnow, dt, scale_amp, nullptr, 0, rk);
+                cr, edge_x, n0, n1, sy, tnow, dt, scale_amp, nullptr, 0, rk, rs);
         } else {
             // multi-grain: this block's cos theta0 (sin theta0 follows ncells later)
             const T* trig_b = ORIENT ? static_cast<const T*>(oa.trig) + (int64_t)b * n0 * n1 : nullptr;
             strip_unit<T, Ops, NOISE, NX, FULL, PF, TAIL, ORIENT, MODE>(m0, g.seed, b, g, ph, uu, out, po, uo, nb,
                                                                         r0, r1, lane, col, valid, last_lane, cr,
                                                                         edge_x, n0, n1, sy, tnow, dt, scale_amp,
-                                                                        trig_b, oa.ncells, rk);
+                                                                        trig_b, oa.ncells, rk, rs);
         }
         if (g.work) {  // the next unit of the list
             unsigned n = 0;

@@ -140,17 +140,19 @@ def _f32_sim(sched, orc, cells, block, oriented):
     return sim, model, grid
 
 
-@pytest.mark.parametrize("oriented", [False, True])
-def test_fp32_paired_runs_repeat_bit_for_bit(sched, orc, oriented):
+@pytest.mark.parametrize("oriented,variant", [(False, 5 + 1000 * 32), (False, 2 + 1000 * 32),
+                                              (True, 5 + 1000 * 32)])
+def test_fp32_runs_repeat_bit_for_bit(sched, orc, oriented, variant):
     """FP32 (contraction allowed) with noise on 40-row blocks in 32-row
     units, so each block's last unit overlaps the one below it: two runs
-    from the same state give the same bits, because every cell is stored by
-    the one unit that owns it (two warps computing a row with differently
-    contracted arithmetic could otherwise store different values)."""
+    from the same state give the same bits, paired or single rows, because
+    every cell is stored by the one unit that owns it (two warps computing a
+    row with differently contracted arithmetic could otherwise store
+    different values)."""
     outs = []
     for _ in range(2):
         sim, model, grid = _f32_sim(sched, orc, [252, 80], [126, 40], oriented)
-        sim.run(model.stable_dt(grid.spacing), 40, variant=5 + 1000 * 32)
+        sim.run(model.stable_dt(grid.spacing), 40, variant=variant)
         outs.append([sim.state.download(f) for f in ("phi", "u")])
     for a, b in zip(*outs):
         assert np.array_equal(a, b)
