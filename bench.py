@@ -79,8 +79,8 @@ BYTES_PER_CELL = {"f64": 32, "f32": 16}  # read phi, u; write phi, u
 # cells; 512^3 has the same per-block work).  Traffic grows with the cell
 # count, so a launch of the full grid moves the per-cell figure times its
 # cells.  Other workloads report null.
-TRAFFIC_PER_CELL = {("c3", "f64"): 833.3e6 / 5040 ** 2, ("c3", "f32"): 375.4e6 / 5040 ** 2,
-                    ("c1big", "f64"): 319.7e6 / 256 ** 3}
+TRAFFIC_PER_CELL = {("c3", "f64"): 827.2e6 / 5040 ** 2, ("c3", "f32"): 377.0e6 / 5040 ** 2,
+                    ("c1big", "f64"): 274.3e6 / 256 ** 3}
 
 NOMINAL_HBM_GBS = 8000.0  # a B200's nominal HBM3e bandwidth, the second denominator
 
@@ -88,11 +88,11 @@ NOMINAL_HBM_GBS = 8000.0  # a B200's nominal HBM3e bandwidth, the second denomin
 # captures (smsp__inst_executed and the fp64 pipe's share, x 32 threads per
 # warp instruction, divided by the launch's cell-updates); the capture named
 # is the summary under profiles/.
-NCU_INST = {("c3", "f64"): {"inst_per_cell": 406.4, "fp64_inst_per_cell": 126.2,
+NCU_INST = {("c3", "f64"): {"inst_per_cell": 408.7, "fp64_inst_per_cell": 126.8,
                             "capture": "modelc_strip_f64_5040sq_126blocks"},
-            ("c3", "f32"): {"inst_per_cell": 268.3, "fp64_inst_per_cell": None,
+            ("c3", "f32"): {"inst_per_cell": 242.4, "fp64_inst_per_cell": None,
                             "capture": "modelc_strip_f32_5040sq_126blocks"},
-            ("c1big", "f64"): {"inst_per_cell": 70.6, "fp64_inst_per_cell": None,
+            ("c1big", "f64"): {"inst_per_cell": 73.3, "fp64_inst_per_cell": None,
                                "capture": "heat3d_tma_256cube"}}
 
 # the strip-kernel variant the captures ran (the autotuner's choice on 10080^2)

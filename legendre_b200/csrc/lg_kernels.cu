@@ -474,6 +474,14 @@ __global__ void __launch_bounds__(1024) heat3d_tma_kernel(const __grid_constant_
                 acc += ((zp - (uc + uc)) + zm) * ih2;
                 const double k = acc * kappa;
                 *op = uc + dt * k;
+                // the row's ghost columns too, with the halo values at hand,
+                // so that the warp's two rows cover whole 32-byte sectors (a
+                // partly written sector costs the DRAM a read; 256^3: DRAM
+                // reads 208 -> 164 MB a step): ghost entries are read by no
+                // step of a run and refilled at its end.  Writing the ghost
+                // rows and corners as well saved 3 MB more and ran slower.
+                if (x == 0) op[-1] = xm;
+                if (x == n0 - 1) op[1] = xp;
                 zm = uc;
                 uc = zp;
                 q += plane;
