@@ -427,6 +427,11 @@ __global__ void __launch_bounds__(256) loss_seed_kernel(const T* __restrict__ x,
 // interior row, as the ghost columns X = -1 and X = N0 fold into columns 0
 // and N0 - 1 across lanes.  Quantities of cells outside the instance are
 // zero (selected, so that no value of a halo lane leaks in).
+//
+// A lane sums its share of the unit's parameter partials in the adjoint's
+// arithmetic type and the warp adds the lanes in FP64 into the unit's slot,
+// so the sums do not depend on which warp ran the unit.  Units past the
+// grid's first wave come from a work list (see launch_adjoint_strip).
 constexpr int SW = 29;  // output columns per strip
 
 // Slab-offset row terms of consecutive rows: the division by the block
@@ -471,11 +476,12 @@ __global__ void __launch_bounds__(256) adjoint_strip_kernel(const T* __restrict_
                                                             T* __restrict__ lam_out,
                                                             const AdjParams<T>* __restrict__ prm, Geo g, T dt,
                                                             double* __restrict__ acc, int rows, int strips,
-                                                            int chunks) {
+                                                            int chunks, unsigned long long* __restrict__ work,
+                                                            unsigned long long work_base) {
     const int lane = threadIdx.x & 31;
     const int64_t units = g.ninst * strips * chunks;
-    for (int64_t unit = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; unit < units;
-         unit += ((int64_t)gridDim.x * blockDim.x) >> 5) {
+    const int64_t first_listed = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t unit = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; unit < units;) {
         const int s = (int)(unit % strips);
         const int k = (int)((unit / strips) % chunks);
         const int64_t inst = unit / ((int64_t)strips * chunks);
@@ -531,7 +537,9 @@ __global__ void __launch_bounds__(256) adjoint_strip_kernel(const T* __restrict_
         // neighbour-lane copies kept for the next rows: xt of the right lane
         // (rows r-2, r-1), yt of the face (r-2, r-1) of both neighbours
         T xtR_pm = T(0), xtR_prev = T(0), ytL_pm = T(0), ytR_pm = T(0);
-        double acc_l = 0.0, acc_d = 0.0, acc_e = 0.0;
+        // the parameter partials of the unit, per lane, in the adjoint's
+        // arithmetic type (one FP64 sum per unit below)
+        T acc_l = T(0), acc_d = T(0), acc_e = T(0);
         // row terms of rows r - 1, r and r + 1 (mirrored outside the instance,
         // where no cotangent is loaded or stored)
         int64_t rt_m = t_m, rt_0 = t_0, rt_p = rw.term;
@@ -625,9 +633,9 @@ __global__ void __launch_bounds__(256) adjoint_strip_kernel(const T* __restrict_
                 const T uL = shfl_up1(u0), uR = shfl_dn1(u0);
                 if (xo && orow) {
                     const T lap = ((uR - T(2) * uc) + uL) * m.ih0 + ((up - T(2) * uc) + um) * m.ih1;
-                    acc_l += (double)(nbar * (-uc * pp));
-                    acc_d += (double)(dt * ub * lap);
-                    acc_e += (double)(abar * c.ae);
+                    acc_l += nbar * (-uc * pp);
+                    acc_d += dt * ub * lap;
+                    acc_e += abar * c.ae;
                 }
             }
             // cotangent of the x face left of X (cells X-1 and X of row r)
@@ -636,11 +644,11 @@ __global__ void __launch_bounds__(256) adjoint_strip_kernel(const T* __restrict_
             const T jbx = (nbl - nb) * m.inv_h2_flux;
             const T xn = xn_raw * jbx, xt = xt_raw * jbx;
             // the face is counted by the cell on its right, or by the last cell for the face into the ghost column
-            if (orow && ((xo) || (X == g.N0 && lane >= 2 && lane <= SW + 1))) acc_e += (double)(jbx * xe_raw);
+            if (orow && ((xo) || (X == g.N0 && lane >= 2 && lane <= SW + 1))) acc_e += jbx * xe_raw;
             // cotangent of the y face (r-1, r)
             const T jby = (nb_prev - nb) * m.inv_h2_flux;
             const T yn_f = yn_raw_prev * jby, yt_f = yt_raw_prev * jby;
-            if (xo && (orow || (r == g.N1 && r - 1 >= Y0 && r - 1 < Y1))) acc_e += (double)(jby * ye_raw_prev);
+            if (xo && (orow || (r == g.N1 && r - 1 >= Y0 && r - 1 < Y1))) acc_e += jby * ye_raw_prev;
 
             // neighbour copies of this row's face terms (used now and by the next two gathers)
             const T xtR = shfl_dn1(xt);
@@ -738,13 +746,22 @@ __global__ void __launch_bounds__(256) adjoint_strip_kernel(const T* __restrict_
             nu_pm = nu_prev;
             nu_prev = nu;
         }
-        acc_l = warp_sum<T>(acc_l);
-        acc_d = warp_sum<T>(acc_d);
-        acc_e = warp_sum<T>(acc_e);
+        const double sl = warp_sum<T>((double)acc_l), sd = warp_sum<T>((double)acc_d),
+                     se = warp_sum<T>((double)acc_e);
         if (lane == 0) {
-            acc[3 * unit + 0] += acc_l;
-            acc[3 * unit + 1] += acc_d;
-            acc[3 * unit + 2] += acc_e;
+            acc[3 * unit + 0] += sl;
+            acc[3 * unit + 1] += sd;
+            acc[3 * unit + 2] += se;
+        }
+        // the next unit: from the work list (units past the grid's first
+        // wave, in order, to whichever warp is free), or the grid stride
+        if (work) {
+            unsigned long long n = 0;
+            if (lane == 0) n = atomicAdd(work, 1ull) - work_base;
+            n = __shfl_sync(0xffffffffu, n, 0);
+            unit = n < (unsigned long long)units ? first_listed + (int64_t)n : units;  // no wrapped value runs
+        } else {
+            unit += first_listed;
         }
     }
 }
@@ -769,15 +786,30 @@ cudaError_t launch_adjoint(const T* x, const T* lam_in, T* lam_out, const void* 
 }
 
 
+// With a work list the grid is one wave of resident CTAs and each warp
+// takes its next unit from the counter when it finishes one, so the strips
+// that cross an interface (the general derivative path) and the flat ones
+// (the far-field body, about a quarter of the instructions fewer) share the
+// SMs evenly; without one every warp runs one unit and a CTA holds its SM
+// slot until its slowest warp is done.
 template <class T>
 cudaError_t launch_adjoint_strip(const T* x, const T* lam_in, T* lam_out, const void* prm, const Geo& g, double dt,
-                                 double* acc, cudaStream_t s) {
+                                 double* acc, unsigned long long* work, unsigned long long base, cudaStream_t s) {
     const int strips = adjoint_strips(g), rows = adjoint_strip_rows(g);
     const int chunks = (g.N1 + rows - 1) / rows;
     const int64_t units = g.ninst * strips * chunks;
-    const unsigned grid = (unsigned)std::min<int64_t>((units + 7) / 8, (int64_t)1 << 30);
-    adjoint_strip_kernel<T><<<grid, 256, 0, s>>>(x, lam_in, lam_out, static_cast<const AdjParams<T>*>(prm), g, (T)dt,
-                                                 acc, rows, strips, chunks);
+    int64_t grid = std::min<int64_t>((units + 7) / 8, (int64_t)1 << 30);
+    if (work) {
+        static const int per_sm = [] {
+            int n = 0;
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, adjoint_strip_kernel<T>, 256, 0) != cudaSuccess)
+                n = 1;
+            return std::max(n, 1);
+        }();
+        grid = std::min<int64_t>(grid, (int64_t)lg::device_sm_count() * per_sm);
+    }
+    adjoint_strip_kernel<T><<<(unsigned)grid, 256, 0, s>>>(x, lam_in, lam_out, static_cast<const AdjParams<T>*>(prm),
+                                                           g, (T)dt, acc, rows, strips, chunks, work, base);
     return cudaGetLastError();
 }
 
@@ -788,23 +820,28 @@ int adjoint_tile_rows(int dtype) { return dtype == 0 ? 8 : 16; }
 int adjoint_strips(const Geo& g) { return (g.N0 + SW - 1) / SW; }
 
 // rows per strip unit: the whole instance height, halved while the launch
-// would hold fewer than 32 warps per SM (down to 16 rows); each unit
-// completes two rows beyond the ones it gathers
+// would hold fewer units than one wave of 16 warps per SM (down to 16 rows).
+// Each unit completes two rows beyond the ones it gathers, so tall units
+// waste least; the work list evens out the rest (on 256 instances of 256^2,
+// 128-row units ran the step 2.5 % faster than 64-row ones, 32-row units
+// 2 % slower)
 int adjoint_strip_rows(const Geo& g) {
     const int strips = adjoint_strips(g);
+    const int64_t wave = (int64_t)lg::device_sm_count() * 16;
     int rows = std::max(1, g.N1);
-    while (rows > 16 && g.ninst * strips * ((g.N1 + rows - 1) / rows) < (int64_t)lg::device_sm_count() * 32) rows = (rows + 1) / 2;
+    while (rows > 16 && g.ninst * strips * ((g.N1 + rows - 1) / rows) < wave) rows = (rows + 1) / 2;
     return rows;
 }
 
 cudaError_t launch_adjoint_step(int dtype, int kernel, const void* x, const void* lam_in, void* lam_out,
-                                const void* prm, const Geo& g, double dt, double* acc, cudaStream_t s) {
+                                const void* prm, const Geo& g, double dt, double* acc, unsigned long long* work,
+                                unsigned long long base, cudaStream_t s) {
     if (kernel == kAdjointStrip) {
         if (dtype == 0)
             return launch_adjoint_strip<double>((const double*)x, (const double*)lam_in, (double*)lam_out, prm, g, dt,
-                                                acc, s);
+                                                acc, work, base, s);
         return launch_adjoint_strip<float>((const float*)x, (const float*)lam_in, (float*)lam_out, prm, g, dt, acc,
-                                           s);
+                                           work, base, s);
     }
     if (dtype == 0)
         return launch_adjoint<double, 8>((const double*)x, (const double*)lam_in, (double*)lam_out, prm, g, dt, acc,

@@ -42,9 +42,13 @@ int64_t adjoint_items(int dtype, int kernel, const Geo& g);
 int64_t loss_items(const Geo& g);                // tiles of the loss kernel; one double each
 
 // cotangents of x_n from those of x_{n+1}; acc[3 item + k] += the step's
-// dL/d(lambda, D, eps4) share of each work item
+// dL/d(lambda, D, eps4) share of each work item.  work (strip form; may be
+// null) is a device counter, zero before the first of a run of launches on
+// one stream: each launch advances it by exactly adjoint_items, and base is
+// its value when the launch starts (launches so far x adjoint_items).
 cudaError_t launch_adjoint_step(int dtype, int kernel, const void* x, const void* lam_in, void* lam_out, const void* prm,
-                                const Geo& g, double dt, double* acc, cudaStream_t s);
+                                const Geo& g, double dt, double* acc, unsigned long long* work,
+                                unsigned long long base, cudaStream_t s);
 // lam = (2 (phi - target), 0), loss[tile] = that tile's sum of squares
 cudaError_t launch_loss_seed(int dtype, const void* x, const double* target, void* lam, Geo g, double* loss,
                              cudaStream_t s);

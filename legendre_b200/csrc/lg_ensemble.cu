@@ -488,15 +488,22 @@ int lg_ensemble_value_and_grad(lg_ensemble* e, double dt, int64_t nsteps, int64_
         ENS_CUDA(e, cudaMalloc(&e->d_target, cells * sizeof(double)));
         ENS_CUDA(e, cudaMalloc(&e->d_usum, e->ninst * sizeof(double)));
     }
-    if (e->acc_cap < acc_n) {
+    // the accumulator slots, then the strip form's work-list counter
+    if (e->acc_cap < acc_n + 1) {
         cudaFree(e->d_acc);
         e->d_acc = nullptr;
         e->acc_cap = 0;
-        ENS_CUDA(e, cudaMalloc(&e->d_acc, acc_n * sizeof(double)));
-        e->acc_cap = acc_n;
+        ENS_CUDA(e, cudaMalloc(&e->d_acc, (acc_n + 1) * sizeof(double)));
+        e->acc_cap = acc_n + 1;
     }
+    const bool listed = e->adj_kernel == lg::adj::kAdjointStrip;
+    unsigned long long* work = listed ? reinterpret_cast<unsigned long long*>(e->d_acc + acc_n) : nullptr;
+    // each strip launch advances the counter by its number of units, so the
+    // base of a launch is the units of the launches before it in this call
+    const unsigned long long per_launch = (unsigned long long)(acc_n / 3);
+    unsigned long long ticket = 0;
     ENS_CUDA(e, cudaMemcpyAsync(e->d_target, target, cells * sizeof(double), cudaMemcpyHostToDevice, st));
-    ENS_CUDA(e, cudaMemsetAsync(e->d_acc, 0, acc_n * sizeof(double), st));
+    ENS_CUDA(e, cudaMemsetAsync(e->d_acc, 0, (acc_n + 1) * sizeof(double), st));
     for (void* q : e->adj) ENS_CUDA(e, cudaMemsetAsync(q, 0, state_bytes(e), st));
 
     // forward pass: checkpoints of the recomputed segments; the resident
@@ -539,8 +546,9 @@ int lg_ensemble_value_and_grad(lg_ensemble* e, double dt, int64_t nsteps, int64_
             for (int64_t i = len - 1; i >= 0; --i) {
                 const void* x = e->res[(size_t)(s * K + i - n_res0)];
                 ENS_CUDA(e, lg::adj::launch_adjoint_step(kind, e->adj_kernel, x, e->adj[a], e->adj[a ^ 1],
-                                                         e->d_adj_params, geo, dt, e->d_acc, st));
+                                                         e->d_adj_params, geo, dt, e->d_acc, work, ticket, st));
                 lg::abi_count_launch(e->ctx, 1);
+                ticket += per_launch;
                 a ^= 1;
             }
             continue;
@@ -558,8 +566,9 @@ int lg_ensemble_value_and_grad(lg_ensemble* e, double dt, int64_t nsteps, int64_
         for (int64_t i = len - 1; i >= 0; --i) {
             const void* x = i == 0 ? e->ckpt[(size_t)s] : e->seg[(size_t)(i - 1)];
             ENS_CUDA(e, lg::adj::launch_adjoint_step(kind, e->adj_kernel, x, e->adj[a], e->adj[a ^ 1],
-                                                     e->d_adj_params, geo, dt, e->d_acc, st));
+                                                     e->d_adj_params, geo, dt, e->d_acc, work, ticket, st));
             lg::abi_count_launch(e->ctx, 1);
+            ticket += per_launch;
             a ^= 1;
         }
     }

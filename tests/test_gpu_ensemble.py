@@ -11,13 +11,17 @@
   checks run twice: on the continuous form (tolerance 0) with h = 1e-4, and
   on the reference's tolerance with h = 1e-5, small enough that no face of
   these runs changes branch.
-* The FP32 ensemble's gradients (FP32 forward and adjoint, FP64 parameter
-  accumulation) stay close to the FP64 ones.
+* The FP32 ensemble's gradients (FP32 forward and adjoint; parameter
+  partials summed in FP32 within a strip unit, in FP64 across units and
+  steps) stay close to the FP64 ones.
+* The strip form agrees with the tile form also where it hands units out
+  from its work list (more units than one wave of resident warps).
 """
 import math
 
 import numpy as np
 import pytest
+import torch
 
 import legendre_b200 as L
 import oracle_bind as orc_mod
@@ -219,6 +223,46 @@ def test_strip_and_tile_adjoints_agree(sched, dtype, rel, cells, block, ninst):
         assert np.allclose(b[k], a[k], rtol=rel, atol=rel * np.abs(a[k]).max()), k
     for k in ("phi0", "u0"):
         assert np.linalg.norm(b[k] - a[k]) <= rel * np.linalg.norm(a[k]), k
+
+
+@pytest.mark.parametrize("dtype,rel", [("f64", 1e-10), ("f32", 2e-4)])
+def test_strip_work_list_past_the_first_wave(sched, dtype, rel):
+    # 96 instances of 128^2 in 16-row strip units: 96 x 5 strips x 8 row runs
+    # = 3840 units, more than one wave of resident warps (148 SMs x 16 warps
+    # in FP32, x 8 in FP64), so the strip form hands most units out from its
+    # work list; it must still agree with the tile form, and its resident
+    # tail must give the same bits
+    n, block, ninst = 128, 64, 96
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    assert ninst * 5 * 8 > sms * 16
+    grid = L.CartesianGrid([n, n], [block, block], [0.0, 0.0], [H, H])
+    ys, xs = np.meshgrid((np.arange(n) + 0.5) * H, (np.arange(n) + 0.5) * H, indexing="ij")
+    phi0 = np.empty((ninst, n, n))
+    for i in range(ninst):
+        r = np.hypot(xs - n * H * (0.3 + 0.1 * (i % 5)), ys - n * H * (0.35 + 0.07 * (i % 4)))
+        phi0[i] = np.maximum(-1.0, -np.tanh((r - 3.0 - (i % 3)) / math.sqrt(2.0)))
+    eps4, seeds = [0.02 + 0.01 * (i % 4) for i in range(ninst)], [40 + i for i in range(ninst)]
+    target = np.tanh(phi0 * 0.8)
+    steps, ckpt = 7, 3
+    state_bytes = 2 * ninst * (block + 2) ** 2 * (n // block) ** 2 * (8 if dtype == "f64" else 4)  # phi and u
+    out = {}
+    for kernel, resident in (("tile", 0), ("strip", 0), ("strip", steps)):
+        model = L.ModelC(0.05, LAM, 0.01)
+        model.d_thermal = D
+        ens = L.Ensemble(grid, model, eps4, seeds, sched, dtype=dtype)
+        ens.set("phi", phi0)
+        ens.set("u", -0.5)
+        out[kernel, resident] = ens.value_and_grad(DT, steps, ckpt, target, kernel=kernel,
+                                                   resident_bytes=resident * state_bytes)
+        ens._destroy()
+    a, b, c = out["tile", 0], out["strip", 0], out["strip", steps]
+    assert np.array_equal(a["loss"], b["loss"])
+    for k in ("lambda", "d_thermal", "eps4", "delta"):
+        assert np.allclose(b[k], a[k], rtol=rel, atol=rel * np.abs(a[k]).max()), k
+    for k in ("phi0", "u0"):
+        assert np.linalg.norm(b[k] - a[k]) <= rel * np.linalg.norm(a[k]), k
+    for k in ("loss", "lambda", "d_thermal", "eps4", "delta", "phi0", "u0"):
+        assert np.array_equal(c[k], b[k]), k
 
 
 @pytest.mark.parametrize("dtype", ["f64", "f32"])
