@@ -50,6 +50,9 @@ __device__ __forceinline__ float recip(float x) {
     return r;
 }
 
+template <class T>
+__device__ __forceinline__ T fma_(T a, T b, T c) { return fma(a, b, c); }
+
 // a(x, y), da(x, y) of KarmaRappelFlux::face and their partial derivatives
 // in x, y and eps4; x and y are the face's (derx, dery).
 template <class T>
@@ -72,20 +75,22 @@ __device__ __forceinline__ FaceDer<T> face_der(T x, T y, T a_bar, T ae, T a12, T
         return f;
     }
     const T is = recip(s);
-    const T is2 = is * is, is3 = is2 * is;
+    const T is2 = is * is;
+    const T d = x2 - y2;
     const T R = (x2 * x2 + y2 * y2) * is2;
     f.a = a_bar + ae * R;  // a_bar (1 + eps' R)
-    const T Rx = T(4) * x * y2 * (x2 - y2) * is3;
-    const T Ry = T(4) * y * x2 * (y2 - x2) * is3;
-    f.ax = ae * Rx;
-    f.ay = ae * Ry;
-    const T G = x * y * (x2 - y2);
-    f.da = -a12 * G * is2;
-    const T Gx = y * (T(3) * x2 - y2), Gy = x * (x2 - T(3) * y2);
-    f.dax = -a12 * (Gx * is2 - T(4) * x * G * is3);
-    f.day = -a12 * (Gy * is2 - T(4) * y * G * is3);
-    f.ae = T(-3) + T(3) * R;   // a = (1 - 3 eps4) + 3 eps4 R
-    f.dae = T(-12) * G * is2;  // a12 = 12 eps4
+    // Rx = 4 x y^2 d / s^3, Ry = -4 y x^2 d / s^3: one shared factor
+    const T k = ae * (T(4) * d) * (is2 * is);
+    f.ax = k * (x * y2);
+    f.ay = -k * (y * x2);
+    const T G = x * y * d, Gs = G * is2;  // G / s^2
+    f.da = -a12 * Gs;
+    // dax = -a12 (Gx - 4 x G / s) / s^2, day likewise
+    const T m4 = T(-4) * G * is, na = -a12 * is2;
+    f.dax = na * fma_(m4, x, y * (T(3) * x2 - y2));
+    f.day = na * fma_(m4, y, x * (x2 - T(3) * y2));
+    f.ae = T(-3) + T(3) * R;  // a = (1 - 3 eps4) + 3 eps4 R
+    f.dae = T(-12) * Gs;      // a12 = 12 eps4
     return f;
 }
 
