@@ -825,14 +825,15 @@ int adjoint_tile_rows(int dtype) { return dtype == 0 ? 8 : 16; }
 int adjoint_strips(const Geo& g) { return (g.N0 + SW - 1) / SW; }
 
 // rows per strip unit: the whole instance height, halved while the launch
-// would hold fewer units than one wave of 16 warps per SM (down to 16 rows).
-// Each unit completes two rows beyond the ones it gathers, so tall units
-// waste least; the work list evens out the rest (on 256 instances of 256^2,
-// 128-row units ran the step 2.5 % faster than 64-row ones, 32-row units
-// 2 % slower)
+// would hold fewer units than 15 warps per SM, most of one wave of 16 (down
+// to 16 rows).  Each unit completes two rows beyond the ones it gathers, so
+// tall units waste least; the work list evens out the rest (on 256
+// instances of 256^2, 9 x 256 = 2304 units of the whole height, 97 % of a
+// wave, ran the gradient 0.5 % faster than 128-row units, which ran it
+// 1.6 % faster than 64-row ones)
 int adjoint_strip_rows(const Geo& g) {
     const int strips = adjoint_strips(g);
-    const int64_t wave = (int64_t)lg::device_sm_count() * 16;
+    const int64_t wave = (int64_t)lg::device_sm_count() * 15;
     int rows = std::max(1, g.N1);
     while (rows > 16 && g.ninst * strips * ((g.N1 + rows - 1) / rows) < wave) rows = (rows + 1) / 2;
     return rows;
