@@ -60,6 +60,8 @@ struct lg_ensemble {
     double* d_target = nullptr;
     double* d_usum = nullptr;  // per instance: the sum of the u cotangents (the Delta gradient's)
     int adj_kernel = lg::adj::kAdjointStrip;
+    cudaStream_t aux = nullptr;          // the target's upload, beside the forward pass
+    cudaEvent_t target_ready = nullptr;  // ... and its completion, awaited by the loss kernel
 };
 
 namespace {
@@ -183,6 +185,10 @@ void free_workspace(lg_ensemble* e) {
 }
 
 void free_all(lg_ensemble* e) {
+    if (e->target_ready) cudaEventDestroy(e->target_ready);
+    if (e->aux) cudaStreamDestroy(e->aux);
+    e->target_ready = nullptr;
+    e->aux = nullptr;
     for (auto& kv : e->graphs) cudaGraphExecDestroy(kv.second.first);
     e->graphs.clear();
     free_workspace(e);
@@ -502,7 +508,6 @@ int lg_ensemble_value_and_grad(lg_ensemble* e, double dt, int64_t nsteps, int64_
     // base of a launch is the units of the launches before it in this call
     const unsigned long long per_launch = (unsigned long long)(acc_n / 3);
     unsigned long long ticket = 0;
-    ENS_CUDA(e, cudaMemcpyAsync(e->d_target, target, cells * sizeof(double), cudaMemcpyHostToDevice, st));
     ENS_CUDA(e, cudaMemsetAsync(e->d_acc, 0, (acc_n + 1) * sizeof(double), st));
     for (void* q : e->adj) ENS_CUDA(e, cudaMemsetAsync(q, 0, state_bytes(e), st));
 
@@ -534,6 +539,18 @@ int lg_ensemble_value_and_grad(lg_ensemble* e, double dt, int64_t nsteps, int64_
         e->t += dt;
         e->step_index += 1;
     }
+    // the target crosses from the host while the queued forward steps run:
+    // its copy goes on a second stream (from pageable memory it holds this
+    // thread until the bytes are staged), and the loss kernel, its first
+    // reader, waits for it.  The previous call's reads of d_target ended at
+    // that call's closing synchronisation.
+    if (!e->aux) {
+        ENS_CUDA(e, cudaStreamCreateWithFlags(&e->aux, cudaStreamNonBlocking));
+        ENS_CUDA(e, cudaEventCreateWithFlags(&e->target_ready, cudaEventDisableTiming));
+    }
+    ENS_CUDA(e, cudaMemcpyAsync(e->d_target, target, cells * sizeof(double), cudaMemcpyHostToDevice, e->aux));
+    ENS_CUDA(e, cudaEventRecord(e->target_ready, e->aux));
+    ENS_CUDA(e, cudaStreamWaitEvent(st, e->target_ready, 0));
     // terminal loss and the seed of the backward sweep
     int a = 0;
     ENS_CUDA(e, lg::adj::launch_loss_seed(kind, e->state[e->cur], e->d_target, e->adj[a], geo, e->d_loss, st));
